@@ -1,0 +1,462 @@
+#!/usr/bin/env python3
+"""Throughput benchmark of the zb3d BM3D path on B200.
+
+Workload (the metric's configuration): plain two-pass BM3Dv2 on YUV420PS
+1920x1080 luma / 960x540 chroma, sigma=[10,10,10], block_step=4, bm_range=12,
+radius=0, dct/dct, extractor_exp=3.  Pass 1 (hard threshold) makes the basic
+estimate, pass 2 (Wiener) uses it as `ref`; all three planes, every frame.
+Frames are seeded synthetic (gradient + 20 rectangles + sinusoidal texture +
+N(0, 10/255) noise), 64 per GPU.  A step is that two-pass job over 8 frames.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is luma megapixels per second of the whole job with inputs resident in
+HBM (CUDA events on the launching streams, max over ranks).  `e2e` is the same
+job through the public API (zb3d.BM3Dv2 on host frames: pinned staging, H2D,
+kernels, D2H inside the timed region).  Multi-GPU runs shard frames across
+ranks (no collective on the data path) and report weak scaling.
+
+`--impl reference` times the CPU restatement of the path (the reference ships
+no CPU BM3D) on the host's cores over a bounded frame sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "vapoursynth-zipcu_b200"))
+
+import numpy as np  # noqa: E402
+
+W, H = 1920, 1080
+SIGMA = 10.0
+BLOCK_STEP, BM_RANGE, EXTRACTOR_EXP = 4, 12, 3
+FRAMES_PER_GPU = 64
+BATCH = 8
+DISTINCT = 8            # distinct synthetic frames, replicated into FRAMES_PER_GPU device buffers
+METRIC = "BM3Dv2 1080p Mpix/s: plain vs BF16+learned-pilot form at ΔPSNR≤0.05 dB"
+WORKLOAD = ("plain two-pass BM3Dv2, YUV420PS 1920x1080 / 960x540, sigma [10,10,10], block_step 4, "
+            "bm_range 12, radius 0, dct/dct, extractor_exp 3")
+KW = dict(sigma=[SIGMA] * 3, block_step=BLOCK_STEP, bm_range=BM_RANGE, extractor_exp=EXTRACTOR_EXP)
+
+
+def plane_dims():
+    return [(W, H), (W // 2, H // 2), (W // 2, H // 2)]
+
+
+def synth_frames(clip: int, count: int):
+    from zb3d import synth
+    out = []
+    for f in range(count):
+        out.append([synth.noisy_plane(w, h, SIGMA, clip=clip, frame=f, plane=p)
+                    for p, (w, h) in enumerate(plane_dims())])
+    return out
+
+
+def match_flops(w, h, bs, rng):
+    """Algorithmic FLOPs of one block-matching launch: 192 per candidate (64 sub,
+    64 mul, 64 add per 8x8 distance) over every reference block's clipped window."""
+    xs = [min(bs * k, w - 8) for k in range((w - 8 + bs - 1) // bs + 1)]
+    ys = [min(bs * k, h - 8) for k in range((h - 8 + bs - 1) // bs + 1)]
+    cols = sum(min(x + rng, w - 8) - max(x - rng, 0) + 1 for x in xs)
+    rows = sum(min(y + rng, h - 8) - max(y - rng, 0) + 1 for y in ys)
+    return 192.0 * cols * rows
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our implementation, device-resident
+# ---------------------------------------------------------------------------
+class DevicePipeline:
+    """Two-pass BM3Dv2 on device buffers.  Per frame and plane one buffer holds
+    [basic | noisy]: pass 1 reads the noisy half and writes the basic half, pass 2
+    reads both (ref = basic) and writes the output plane; nothing is copied."""
+
+    def __init__(self, torch, nstreams: int = 2):
+        from zb3d import _native as N
+        from zb3d.device import DeviceFilter
+        self.torch = torch
+        self.ns = nstreams
+        self.basic = [DeviceFilter(W, H, family=N.YUV, subsampling=(1, 1), num_streams=1, **KW)
+                      for _ in range(nstreams)]
+        self.final = [DeviceFilter(W, H, family=N.YUV, subsampling=(1, 1), num_streams=1, ref=True, **KW)
+                      for _ in range(nstreams)]
+        self.lay = self.basic[0].entries
+        self.streams = [torch.cuda.Stream() for _ in range(nstreams)]
+
+    def upload(self, frames, count: int):
+        t = self.torch
+        self.bufs, self.outs = [], []
+        for i in range(count):
+            src = frames[i % len(frames)]
+            fb, fo = [], []
+            for e, lay in enumerate(self.lay):
+                pe = lay.height * lay.pitch
+                b = t.zeros(2 * pe, dtype=t.float32, device="cuda")
+                host = np.zeros((lay.height, lay.pitch), np.float32)
+                host[:, :lay.width] = src[lay.plane[0]]
+                b[pe:].copy_(t.from_numpy(host.reshape(-1)))
+                fb.append(b)
+                fo.append(t.empty(pe, dtype=t.float32, device="cuda"))
+            self.bufs.append(fb)
+            self.outs.append(fo)
+        t.cuda.synchronize()
+
+    def run_frame(self, j: int, fidx: int):
+        k = j % self.ns
+        st = self.streams[k].cuda_stream
+        for e, lay in enumerate(self.lay):
+            b = self.bufs[fidx][e]
+            pe4 = lay.height * lay.pitch * 4
+            self.basic[k].run_entry(e, b.data_ptr() + pe4, b.data_ptr(), st)
+            self.final[k].run_entry(e, b.data_ptr(), self.outs[fidx][e].data_ptr(), st)
+
+    def profile(self, on: bool):
+        for f in self.basic + self.final:
+            f.profile(on)
+
+    def collect(self):
+        mm = mn = fm = fn = 0
+        for f in self.basic + self.final:
+            a, b, c, d = f.profile_collect()
+            mm, mn, fm, fn = mm + a, mn + b, fm + c, fn + d
+        return mm, mn, fm, fn
+
+    def timed(self, steps: int, start_frame: int = 0) -> float:
+        t = self.torch
+        s0 = self.streams[0]
+        start, end = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
+        start.record(s0)
+        for s in self.streams[1:]:
+            s.wait_event(start)
+        n = len(self.bufs)
+        for step in range(steps):
+            for j in range(BATCH):
+                self.run_frame(j, (start_frame + step * BATCH + j) % n)
+        for s in self.streams[1:]:
+            ev = t.cuda.Event()
+            ev.record(s)
+            s0.wait_event(ev)
+        end.record(s0)
+        end.synchronize()
+        return start.elapsed_time(end)
+
+    def launches_per_frame(self) -> int:
+        # match + filter + finish per plane and pass (1920/960 widths need no clamped-column launch)
+        return 2 * len(self.lay) * 3
+
+    def close(self):
+        for f in self.basic + self.final:
+            f.close()
+
+
+def run_e2e(frames, steps: int, warmup: int, num_streams: int = 4):
+    """Same job through the public API on host frames (zb3d.BM3Dv2)."""
+    import zb3d
+    from zb3d import _native as N
+    nfr = BATCH * (steps + warmup)
+    host = [frames[i % len(frames)] for i in range(nfr)]
+    clip = zb3d.Clip.from_frames(host, family=N.YUV, subsampling=(1, 1))
+    basic = zb3d.BM3Dv2(clip, num_streams=num_streams, **KW)
+    final = zb3d.BM3Dv2(clip, ref=basic, num_streams=num_streams, **KW)
+    pool = ThreadPoolExecutor(num_streams)
+
+    def step(s):
+        list(pool.map(final.get_frame, range(s * BATCH, (s + 1) * BATCH)))
+
+    for s in range(warmup):
+        step(s)
+    t0 = time.perf_counter()
+    for s in range(warmup, warmup + steps):
+        step(s)
+    dt = time.perf_counter() - t0
+    pool.shutdown()
+    # bytes per step: pass 1 uploads the clip, pass 2 the ref and the clip; both download their output
+    px = sum(((w + 31) // 32 * 32) * h for w, h in plane_dims())
+    h2d = 3 * px * 4 * BATCH
+    d2h = 2 * px * 4 * BATCH
+    return dt, h2d, d2h
+
+
+# ---------------------------------------------------------------------------
+# the reference's own kernels on the same GPU (drop-in comparison)
+# ---------------------------------------------------------------------------
+def run_ref_cuda(torch, frames, steps: int, warmup: int):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        import ref_configs as rc
+        import refh
+    except Exception:
+        return None
+    specs = {}
+    for final in (0, 1):
+        for (w, h) in ((W, H), (W // 2, H // 2)):
+            s = rc.RefSpec(w=w, h=h, stride=w, sigma=(SIGMA,) * 3, block_step=BLOCK_STEP, bm_range=BM_RANGE,
+                           final=final, extractor_exp=EXTRACTOR_EXP)
+            if not (refh.available() and refh.has_cubin(s)):
+                return None
+            specs[(final, w)] = s
+    ns = 2
+    kernels = [{k: refh.RefKernel(s) for k, s in specs.items()} for _ in range(ns)]
+    streams = [torch.cuda.Stream() for _ in range(ns)]
+    dims = plane_dims()
+    bufs, res = [], []
+    for i in range(FRAMES_PER_GPU):
+        src = frames[i % len(frames)]
+        fb = []
+        for p, (w, h) in enumerate(dims):
+            b = torch.zeros(2 * w * h, dtype=torch.float32, device="cuda")
+            b[w * h:].copy_(torch.from_numpy(np.ascontiguousarray(src[p]).reshape(-1)))
+            fb.append((b, torch.empty(w * h, dtype=torch.float32, device="cuda")))
+        bufs.append(fb)
+    for k in range(ns):
+        res.append({w: torch.empty(2 * w * h, dtype=torch.float32, device="cuda") for (w, h) in dims})
+
+    def frame(j, fidx):
+        k = j % ns
+        st = streams[k].cuda_stream
+        for p, (w, h) in enumerate(dims):
+            b, out = bufs[fidx][p]
+            r = res[k][w]
+            kernels[k][(0, w)].run(r.data_ptr(), b.data_ptr() + w * h * 4, b.data_ptr(), r.numel() * 4, st)
+            kernels[k][(1, w)].run(r.data_ptr(), b.data_ptr(), out.data_ptr(), r.numel() * 4, st)
+
+    def timed(nsteps, first):
+        s0 = streams[0]
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s0)
+        streams[1].wait_event(a)
+        for s in range(nsteps):
+            for j in range(BATCH):
+                frame(j, (first + s * BATCH + j) % FRAMES_PER_GPU)
+        ev = torch.cuda.Event()
+        ev.record(streams[1])
+        s0.wait_event(ev)
+        z.record(s0)
+        z.synchronize()
+        return a.elapsed_time(z)
+
+    timed(warmup, 0)
+    ms = timed(steps, warmup * BATCH)
+    for d in kernels:
+        for kk in d.values():
+            kk.close()
+    return ms
+
+
+# ---------------------------------------------------------------------------
+# CPU restatement (FP64 oracle) on the host cores
+# ---------------------------------------------------------------------------
+def cpu_two_pass_frame(frame, nthreads):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    import ref_configs as rc
+    for p, (w, h) in enumerate(plane_dims()):
+        noisy = np.ascontiguousarray(frame[p], np.float32)
+        c1 = orc.make_cfg(w, h, w, [rc.scaled_sigma(SIGMA, False)], BLOCK_STEP, BM_RANGE, 0,
+                          nthreads=nthreads, extractor_exp=EXTRACTOR_EXP)
+        num, den, _ = orc.bm3d_pass(c1, noisy[None, None, None], want_matches=False)
+        basic = (num[0, 0] / den[0, 0]).astype(np.float32)
+        c2 = orc.make_cfg(w, h, w, [rc.scaled_sigma(SIGMA, True)], BLOCK_STEP, BM_RANGE, 0, final=1,
+                          nthreads=nthreads, extractor_exp=EXTRACTOR_EXP)
+        src = np.stack([basic, noisy])[:, None, None]
+        orc.bm3d_pass(c2, src, want_matches=False)
+
+
+def cpu_baseline(frames, budget_s: float = 20.0, max_frames: int = 4):
+    nthreads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    done = 0
+    while done < max_frames and (done == 0 or time.perf_counter() - t0 < budget_s):
+        cpu_two_pass_frame(frames[done % len(frames)], nthreads)
+        done += 1
+    dt = time.perf_counter() - t0
+    return {"value": W * H * done / dt / 1e6, "unit": "Mpix/s", "cores": nthreads, "kind": "port",
+            "sample": f"{done} full 1080p YUV420 frame(s), both passes, all planes, FP64 oracle "
+                      f"(FP32 exact-order matching), {dt:.1f} s"}
+
+
+def reference_arm(args, rank: int, world: int):
+    if rank != 0:
+        return 0
+    nthreads = os.cpu_count() or 1
+    frames = synth_frames(0, 2)
+    for i in range(args.warmup):
+        cpu_two_pass_frame(frames[i % 2], nthreads)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        cpu_two_pass_frame(frames[i % 2], nthreads)
+    dt = time.perf_counter() - t0
+    v = W * H * args.steps / dt / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpix/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "step": "one frame (both passes, all planes) on the CPU"},
+            "cpu_baseline": {"value": v, "unit": "Mpix/s", "cores": nthreads, "kind": "port",
+                             "sample": f"{args.steps} 1080p YUV420 frames, FP64 restatement of the path "
+                                       "(the reference has no CPU BM3D)"},
+            "e2e": {"value": v, "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-cuda", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from zb3d import _native as N
+    N.lib()
+    frames = synth_frames(rank, DISTINCT)
+    pipe = DevicePipeline(torch)
+    pipe.upload(frames, FRAMES_PER_GPU)
+    pipe.timed(args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    pipe.profile(True)
+    ms = pipe.timed(args.steps, start_frame=args.warmup * BATCH)
+    pipe.profile(False)
+    clk = clocks.stop()
+    match_ms, match_n, filt_ms, filt_n = pipe.collect()
+    torch.cuda.synchronize()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    frames_done = args.steps * BATCH * world
+    value = W * H * frames_done / (ms / 1e3) / 1e6
+
+    # dominant kernel: block matching; algorithmic FLOPs per frame (both passes, three planes)
+    flops_frame = 2 * sum(match_flops(w, h, BLOCK_STEP, BM_RANGE) for (w, h) in plane_dims())
+    match_flops_total = flops_frame * args.steps * BATCH
+    sm_max = (clk or {}).get("sm_max_mhz") or 1965.0
+    props = torch.cuda.get_device_properties(local)
+    peak_fp32 = props.multi_processor_count * 128 * 2 * sm_max * 1e6 / 1e12
+    achieved = match_flops_total / (match_ms / 1e3) / 1e12 if match_ms > 0 else None
+
+    out = {"metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic: seeded gradient + 20 rectangles + sinusoidal texture, N(0, 10/255) noise",
+           "config": {"workload": WORKLOAD, "form": "plain FP32, match indices bit-exact with the reference",
+                      "frames_per_gpu": FRAMES_PER_GPU, "batch_frames_per_step": BATCH,
+                      "l2": f"inputs larger than L2: {FRAMES_PER_GPU} distinct frame buffers "
+                            f"({FRAMES_PER_GPU * 2 * 12.4:.0f} MB) cycled",
+                      "parallelism": f"frame shards over {world} GPU(s), no collective",
+                      "streams": pipe.ns},
+           "gpu_launches": pipe.launches_per_frame() * args.steps * BATCH,
+           "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
+                        "frac": (achieved / peak_fp32) if achieved else None, "traffic": None,
+                        "kernel": "zb_match_tiled<ssd, shared, bs4> (block matching)",
+                        "per_launch_ms": match_ms / max(match_n, 1), "launches": match_n,
+                        "peak_source": f"nominal FP32: {props.multi_processor_count} SMs x 128 lanes x 2 x "
+                                       f"{sm_max:.0f} MHz (MEASURED_PEAKS.json has no FP32 figure)",
+                        "filter_ms_per_launch": filt_ms / max(filt_n, 1)},
+           "clocks": clk}
+    if rank == 0 and not args.no_ref_cuda:
+        rms = run_ref_cuda(torch, frames, args.steps, args.warmup)
+        if rms:
+            rv = W * H * args.steps * BATCH / (rms / 1e3) / 1e6
+            out["ref_cuda"] = {"value": rv, "unit": "Mpix/s", "ms_per_step": rms / args.steps,
+                               "what": "the reference's own bm3d.cu kernels (NVRTC-built, -use_fast_math) on "
+                                       "this GPU, same frames, same two-pass chaining, device-resident",
+                               "speedup_ours": value / world / rv}
+    pipe.close()
+    if not args.no_e2e:
+        dt, h2d, d2h = run_e2e(frames, args.steps, args.warmup)
+        out["e2e"] = {"value": W * H * args.steps * BATCH * world / dt / 1e6, "unit": "Mpix/s",
+                      "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                      "how": "zb3d.BM3Dv2 twice (basic, then ref=basic) on host numpy frames, 4 request "
+                             "threads, wall clock"}
+    if rank == 0 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(frames)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,208 @@
+/*
+ * zb3d — B200-native BM3D / BM3Dv2 / VAggregate behind a plain C ABI.
+ *
+ * Drop-in replacement for the BM3D path of the vszipcu VapourSynth plugin.
+ * Each entry point states the reference interface it replaces (paths inside the
+ * vszipcu project).  No CUDA or torch types cross this boundary: frames are
+ * plain float pointers with byte strides, device buffers are pointers, streams
+ * are opaque `void *` (a cudaStream_t, or NULL for the default stream).
+ *
+ * Threading: a filter may be called from several threads at once (VapourSynth's
+ * fmParallel): up to `num_streams` frames are in flight, each on its own pair of
+ * CUDA streams; further callers wait for a free slot.
+ */
+#ifndef ZB3D_H
+#define ZB3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* "argument not given" for the optional int arguments of zb3d_args. */
+#define ZB3D_UNSET (-2147483647 - 1)
+
+/* VapourSynth colour families (cfGray, cfRGB, cfYUV) and sample types. */
+enum { ZB3D_GRAY = 1, ZB3D_RGB = 2, ZB3D_YUV = 3 };
+enum { ZB3D_INTEGER = 0, ZB3D_FLOAT = 1 };
+
+/* The part of VSVideoInfo / VSVideoFormat the filters read
+ * (vszipcu src/bm3d.zig:990-1011, 1090-1092). */
+typedef struct zb3d_video_info {
+    int color_family;
+    int sample_type;
+    int bits_per_sample;
+    int subsampling_w, subsampling_h;
+    int num_planes;
+    int width, height;
+    int num_frames;
+} zb3d_video_info;
+
+/* The BM3D / BM3Dv2 argument map (vszipcu src/plugin.zig:84-90, defaults in
+ * src/bm3d.zig:1013-1081).  Per-plane arrays hold n_* elements (0 = not given);
+ * a missing element i falls back to element i-1, as the reference does.
+ * Optional ints use ZB3D_UNSET for "not given".  Strings are case-insensitive. */
+typedef struct zb3d_args {
+    const zb3d_video_info *ref;            /* "ref" clip, or NULL */
+    const float *sigma;            int n_sigma;
+    const int *block_step;         int n_block_step;
+    const int *bm_range;           int n_bm_range;
+    int radius;
+    const int *ps_num;             int n_ps_num;
+    const int *ps_range;           int n_ps_range;
+    int chroma;
+    int device_id;
+    int num_streams;
+    int extractor_exp;
+    const char *const *bm_error_s;      int n_bm_error_s;
+    const char *const *transform_2d_s;  int n_transform_2d_s;
+    const char *const *transform_1d_s;  int n_transform_1d_s;
+    int zero_init;
+    int fast_fused;
+} zb3d_args;
+
+/* Fills `a` with "nothing given" (all defaults). */
+void zb3d_args_init(zb3d_args *a);
+
+/* One frame: up to three float planes, strides in bytes. */
+typedef struct zb3d_frame {
+    const float *ptr[3];
+    ptrdiff_t stride[3];
+} zb3d_frame;
+
+typedef struct zb3d_frame_out {
+    float *ptr[3];
+    ptrdiff_t stride[3];
+} zb3d_frame_out;
+
+typedef struct zb3d_filter zb3d_filter;
+
+/*
+ * Creates a BM3D (v2 = 0) or BM3Dv2 (v2 = 1) filter for `clip`.
+ * Replaces: vszipcu src/bm3d.zig:965 `create` / :1432 `createV2` (validation and
+ * error strings :990-1256).  Returns NULL and writes the reference's error text
+ * ("BM3D: ...") into err on failure.  BM3Dv2 with every plane's sigma below
+ * FLT_EPSILON returns a pass-through filter (src/bm3d.zig:1449-1456).
+ */
+zb3d_filter *zb3d_create(const zb3d_video_info *clip, const zb3d_args *args, int v2, char *err, size_t errlen);
+
+/* Output clip info: BM3D with radius > 0 emits the stacked accumulator clip of
+ * height h*2*(2r+1) (src/bm3d.zig:1224-1231). */
+void zb3d_output_info(const zb3d_filter *f, zb3d_video_info *out);
+
+/* Source frames [*first, *last] that frame n needs from clip (and from ref),
+ * the request pattern of src/bm3d.zig:643-650. */
+void zb3d_frame_range(const zb3d_filter *f, int n, int *first, int *last);
+
+/* Frame properties of the stacked output (BM3D_V_radius, BM3D_V_process), src/bm3d.zig:716-720. */
+void zb3d_output_props(const zb3d_filter *f, int *radius, int process[3]);
+
+/*
+ * Produces frame n into dst.  clip_frames / ref_frames hold the frames
+ * [first, last] of zb3d_frame_range (ref_frames NULL when there is no ref).
+ * Replaces: vszipcu src/bm3d.zig:635 `getFrame` (process :274, processFused :481,
+ * download :427).  Planes whose sigma is below FLT_EPSILON are not written
+ * (the caller copies them, as newVideoFrame2 does), except that the stacked
+ * output zeroes them when zero_init is set (src/bm3d.zig:708-715).
+ * Returns 0, or -1 with "BM3D: process frame failed." style text in err.
+ */
+int zb3d_get_frame(zb3d_filter *f, int n, const zb3d_frame *clip_frames, const zb3d_frame *ref_frames,
+                   zb3d_frame_out *dst, char *err, size_t errlen);
+
+/* Releases the filter and its device memory (src/bm3d.zig:739 `free`). */
+void zb3d_free(zb3d_filter *f);
+
+/* ---- device-resident path (inputs already in HBM) ----------------------- */
+
+/* One plane entry of a filter: a processed plane, or Y+U+V when chroma. */
+typedef struct zb3d_entry_layout {
+    int nplanes;              /* 1, or 3 for CBM3D */
+    int plane[3];             /* clip plane index of each entry plane */
+    int width, height, pitch; /* pitch in floats */
+    int tw;                   /* temporal window 2r+1 of one frame's window */
+    int nclips;               /* 2 when a ref clip drives matching */
+    size_t src_offset, src_elems;  /* [clips][planes][tw][height][pitch] floats */
+    size_t dst_offset, dst_elems;  /* [planes][height][pitch] (stacked: [planes][tw][2][height][pitch]) */
+} zb3d_entry_layout;
+
+int zb3d_num_entries(const zb3d_filter *f);
+int zb3d_entry_layout_get(const zb3d_filter *f, int e, zb3d_entry_layout *out);
+size_t zb3d_src_elems(const zb3d_filter *f);
+size_t zb3d_dst_elems(const zb3d_filter *f);
+
+/*
+ * Runs one frame window entirely on the device: d_src holds zb3d_src_elems floats
+ * in the entry layout, d_dst receives zb3d_dst_elems floats (the denoised planes,
+ * or the stacked accumulators of BM3D radius > 0).  Enqueued on `stream`; uses
+ * the filter's slot 0 workspace, so concurrent calls on one filter must not overlap.
+ * Replaces the device half of src/bm3d.zig:375-401.
+ */
+int zb3d_process_device(zb3d_filter *f, const float *d_src, float *d_dst, void *stream, char *err, size_t errlen);
+
+/*
+ * One entry of one window on the device, with caller-placed buffers: d_src is the
+ * entry's [clips][planes][tw][height][pitch] block, d_dst its
+ * [planes][height][pitch] output (stacked [planes][tw][2][height][pitch] when
+ * radius > 0).  Lets a two-pass pipeline write the basic estimate straight into
+ * the ref slot of the second pass.  Same slot-0 workspace rule as above.
+ */
+int zb3d_process_entry_device(zb3d_filter *f, int e, const float *d_src, float *d_dst, void *stream, char *err,
+                              size_t errlen);
+
+/*
+ * Launch timing: with `on`, every block-matching launch of this filter is
+ * bracketed by CUDA events on its stream; zb3d_profile_collect waits for them
+ * and returns the summed milliseconds and launch count since the last collect.
+ */
+void zb3d_profile_enable(zb3d_filter *f, int on);
+int zb3d_profile_collect(zb3d_filter *f, double *match_ms, int *match_launches, double *filter_ms,
+                         int *filter_launches);
+
+/*
+ * Block matching only, for entry e of one window already on the device: writes
+ * the 8-entry match list of every reference block to d_list
+ * (int32 pairs [nby][nbx][8][2]: x, then y | z << 24, in list order; z is the
+ * window frame).  Blocks sit at x = min(bs*kx, w-8), y = min(bs*ky, h-8).
+ * Replaces the matching half of vszipcu src/bm3d.cu:571-788 (its index8_x/y/z).
+ */
+int zb3d_match_device(zb3d_filter *f, int e, const float *d_src, int32_t *d_list, void *stream, char *err,
+                      size_t errlen);
+
+/*
+ * Temporal aggregation on the device over float accumulator stacks (the
+ * stacked BM3D output): dst = sum_t num[t] / sum_t den[t] in ascending t, IEEE
+ * division.  stacks[t] points to the stacked entry buffer of frame clamp(n-r+t),
+ * z[t] is the slot aggZ(t, n, nframes, r).  Replaces src/bm3d_vagg.cu:18-48.
+ */
+int zb3d_vaggregate_device(const float *const *stacks, const int *z, int tw, int width, int height, int pitch,
+                           int nplanes, unsigned proc_mask, float *d_dst, void *stream);
+
+/* ---- VAggregate -------------------------------------------------------- */
+
+typedef struct zb3d_vagg zb3d_vagg;
+
+/* Replaces: vszipcu src/bm3d.zig:1372 `createVAggregate` (errors :1391-1417). */
+zb3d_vagg *zb3d_vaggregate_create(const zb3d_video_info *clip, const zb3d_video_info *src, const int *planes,
+                                  int n_planes, char *err, size_t errlen);
+void zb3d_vaggregate_output_info(const zb3d_vagg *v, zb3d_video_info *out);
+/* Stacked frames [*first, *last] of `clip` that output frame n needs (src/bm3d.zig:1327-1331). */
+void zb3d_vaggregate_frame_range(const zb3d_vagg *v, int n, int *first, int *last);
+/* stacks = the stacked frames [first, last]; planes not listed are left to the caller.
+ * Replaces src/bm3d.zig:1319 `aggGetFrame` / :1284 `aggPlane`. */
+int zb3d_vaggregate_get_frame(zb3d_vagg *v, int n, const zb3d_frame *stacks, zb3d_frame_out *dst, char *err,
+                              size_t errlen);
+void zb3d_vaggregate_free(zb3d_vagg *v);
+
+/* aggZ of src/bm3d.zig:46-48: the slot of stacked frame clamp(n-r+i) that belongs to frame n. */
+int zb3d_agg_z(int i, int n, int nframes, int radius);
+
+/* Library version string. */
+const char *zb3d_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZB3D_H */

@@ -1,0 +1,46 @@
+// Kernel argument blocks shared by the CUDA kernels and the C++ host.
+#pragma once
+#include <cstdint>
+
+namespace zb {
+
+enum Metric { M_SSD = 0, M_SAD = 1, M_ZSSD = 2, M_ZSAD = 3, M_SSD_NORM = 4 };
+
+// Block matching of one plane entry.  Reference blocks sit at
+// x = min(bs*kx, w-8), y = min(bs*ky, h-8) (vszipcu src/bm3d.cu:585-595).
+struct MatchArgs {
+    const float *frames;   // matching plane of window frame t at frames + t*fstride
+    long long fstride;
+    int w, h, pitch;
+    int bs, range;
+    int radius, ps_num, ps_range;
+    int nbx, nby;          // reference blocks per row / column
+    int nbx_al;            // blocks whose x = bs*kx needs no clamp
+    int tile_pitch;        // shared tile row pitch in floats (tiled kernel)
+    int chunks;            // ceil((2*range+1)/4)
+    int2 *list;            // [nby*nbx][8]: (x, y | z << 24)
+    float *errs;           // [nby*nbx][8]: distances of the spatial list (radius > 0)
+    int self_incl;         // 1: insert the block itself here (radius 0)
+    int gen_mode;          // generic kernel: 0 = every block, 1 = clamped last column only
+};
+
+// Collaborative filtering + aggregation of one plane entry.
+struct FilterArgs {
+    const float *src;                 // [clips][planes][tw][h][pitch]
+    long long clip_stride, plane_stride, frame_stride;
+    int w, h, pitch;
+    int nplanes, chroma;
+    const int2 *list;                 // [nblocks][8]
+    int nblocks;
+    float sigma[3];                   // already scaled (hard or Wiener factor)
+    float extractor;                  // 2^extractor_exp, or 0
+    unsigned long long *num;          // [planes][tw][h][pitch]  fixed point, 2^32 = 1.0
+    unsigned long long *den;          // [planes][tw][h][pitch]  weights at patch origins
+    long long acc_plane_stride, acc_frame_stride;
+};
+
+// Fixed-point scale of the accumulators: value * 2^32 held in a signed 64-bit sum.
+constexpr float kFixScale = 4294967296.0f;
+constexpr float kFixInv = 2.3283064365386962890625e-10f;
+
+}  // namespace zb

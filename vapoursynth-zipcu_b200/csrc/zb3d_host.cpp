@@ -1,0 +1,1294 @@
+// zb3d host: argument validation, plane entries, stream-slot pool, device frame
+// caches, host<->device staging, and the C ABI of include/zb3d.h.
+//
+// Mirrors the filter host of vszipcu (src/bm3d.zig, src/pool.zig,
+// src/framecache.zig) in C++ over the CUDA runtime: the kernels are compiled
+// ahead of time for sm_100a, so there is no NVRTC step and one kernel serves
+// every frame size and option set.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cctype>
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <condition_variable>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/zb3d.h"
+#include "zb3d_args.h"
+
+namespace zb {
+
+cudaError_t launch_match(MatchArgs a, int metric, int rows_per_cta, bool use_tiled, cudaStream_t st);
+size_t match_tile_bytes(const MatchArgs &a, int rows_per_cta);
+cudaError_t launch_filter(const FilterArgs &a, bool final_, int t2d, int t1d, cudaStream_t st);
+cudaError_t launch_finish(const unsigned long long *num, const unsigned long long *den, long long acc_plane_stride,
+                          long long acc_frame_stride, int w, int h, int pitch, int nplanes, int tw,
+                          unsigned proc_mask, float *dst, int dst_pitch, long long dst_plane_stride, int mode,
+                          cudaStream_t st);
+cudaError_t launch_vagg(const float *const *stacks, const int *z, int tw, int w, int h, int pitch, int nplanes,
+                        unsigned proc_mask, float *dst, int dst_pitch, long long dst_plane_stride, cudaStream_t st);
+
+namespace {
+
+constexpr float kFltEpsilon = 1.19209290e-7f;
+constexpr int kMaxRadius = 16;
+constexpr int kMaxTw = 2 * kMaxRadius + 1;
+
+void set_err(char *err, size_t n, const char *fmt, ...) {
+    if (!err || n == 0) return;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(err, n, fmt, ap);
+    va_end(ap);
+}
+
+bool eq_lower(const char *s, const char *lit) {
+    size_t n = strlen(lit);
+    if (strlen(s) != n) return false;
+    for (size_t i = 0; i < n; ++i)
+        if (std::tolower((unsigned char)s[i]) != lit[i]) return false;
+    return true;
+}
+
+int parse_metric(const char *s) {
+    if (eq_lower(s, "ssd")) return M_SSD;
+    if (eq_lower(s, "sad")) return M_SAD;
+    if (eq_lower(s, "zssd")) return M_ZSSD;
+    if (eq_lower(s, "zsad")) return M_ZSAD;
+    if (eq_lower(s, "ssd/norm")) return M_SSD_NORM;
+    return -1;
+}
+
+int parse_transform(const char *s) {
+    if (eq_lower(s, "dct")) return 0;
+    if (eq_lower(s, "haar")) return 1;
+    if (eq_lower(s, "wht")) return 2;
+    if (eq_lower(s, "bior1.5")) return 3;
+    return -1;
+}
+
+float f32_from_bits(uint32_t b) {
+    float f;
+    memcpy(&f, &b, 4);
+    return f;
+}
+
+// per-plane array with the reference's fallback rule (src/bm3d.zig:953-963)
+template <class T>
+void per_plane(const T *given, int n, T base, T out[3]) {
+    for (int i = 0; i < 3; ++i) out[i] = i < n ? given[i] : (i == 0 ? base : out[i - 1]);
+}
+
+int pick(int v, int dflt) { return v == ZB3D_UNSET ? dflt : v; }
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// ---------------------------------------------------------------------------
+// Device LRU cache with all-or-nothing claims.  A request claims every key it
+// needs at once or waits without holding anything, so requests never deadlock
+// while the capacity covers one request per concurrent caller.
+// ---------------------------------------------------------------------------
+class DevCache {
+  public:
+    struct Slot {
+        long long key = -1;
+        void *buf = nullptr;
+        cudaEvent_t ev = nullptr;
+        int refs = 0;
+        unsigned long long stamp = 0;
+        bool ready = false;
+    };
+
+    ~DevCache() { clear(); }
+
+    bool init(size_t bytes, int n) {
+        slots_.resize(n);
+        for (auto &s : slots_) {
+            if (cudaMalloc(&s.buf, bytes) != cudaSuccess) return false;
+            if (cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming) != cudaSuccess) return false;
+        }
+        return true;
+    }
+
+    void clear() {
+        for (auto &s : slots_) {
+            if (s.buf) cudaFree(s.buf);
+            if (s.ev) cudaEventDestroy(s.ev);
+        }
+        slots_.clear();
+    }
+
+    void *buf(int i) { return slots_[i].buf; }
+    cudaEvent_t ev(int i) { return slots_[i].ev; }
+
+    // keys must be distinct; load[i] tells the caller to fill and publish slot idx[i]
+    void acquire(const long long *keys, int n, int *idx, bool *load) {
+        std::unique_lock<std::mutex> lk(mu_);
+        for (;;) {
+            bool busy = false;
+            for (int k = 0; k < n && !busy; ++k)
+                for (auto &s : slots_)
+                    if (s.key == keys[k] && !s.ready) {
+                        busy = true;
+                        break;
+                    }
+            if (busy) {
+                cv_.wait(lk);
+                continue;
+            }
+            int claimed = 0;
+            for (; claimed < n; ++claimed) {
+                int found = -1;
+                load[claimed] = false;
+                for (int i = 0; i < (int)slots_.size(); ++i)
+                    if (slots_[i].key == keys[claimed]) {
+                        found = i;
+                        break;
+                    }
+                if (found < 0) {
+                    for (int i = 0; i < (int)slots_.size(); ++i) {
+                        if (slots_[i].refs) continue;
+                        bool mine = false;
+                        for (int j = 0; j < claimed; ++j) mine |= idx[j] == i;
+                        if (mine) continue;
+                        if (found < 0 || slots_[i].stamp < slots_[found].stamp) found = i;
+                    }
+                    if (found < 0) break;
+                    slots_[found].key = keys[claimed];
+                    slots_[found].ready = false;
+                    load[claimed] = true;
+                }
+                idx[claimed] = found;
+                slots_[found].refs += 1;
+                slots_[found].stamp = ++clock_;
+            }
+            if (claimed == n) return;
+            for (int j = 0; j < claimed; ++j) {
+                slots_[idx[j]].refs -= 1;
+                if (load[j]) slots_[idx[j]].key = -1;
+            }
+            cv_.notify_all();
+            cv_.wait(lk);
+        }
+    }
+
+    void publish(int i) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            slots_[i].ready = true;
+        }
+        cv_.notify_all();
+    }
+
+    void abandon(int i) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            if (!slots_[i].ready) slots_[i].key = -1;
+        }
+        cv_.notify_all();
+    }
+
+    void release(const int *idx, int n) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            for (int k = 0; k < n; ++k) slots_[idx[k]].refs -= 1;
+        }
+        cv_.notify_all();
+    }
+
+  private:
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::vector<Slot> slots_;
+    unsigned long long clock_ = 0;
+};
+
+}  // namespace
+
+struct Entry {
+    int w, h, pitch;
+    int nplanes;
+    int planes[3];
+    float sigma[3];  // scaled
+    int bs, range, ps_num, ps_range;
+    unsigned proc_mask;
+    int metric, t2d, t1d;
+    int nbx, nby, nbx_al;
+    long long nblocks;
+    size_t plane_elems;            // h * pitch
+    size_t src_off, src_elems;     // window layout [clips][planes][tw][h][pitch]
+    size_t dst_off, dst_elems;     // window output: [planes][h][pitch], stacked [planes][tw][2][h][pitch] if r > 0
+    size_t out_off;                // BM3Dv2 temporal frame output [planes][h][pitch]
+    size_t frame_off;              // offset inside one cached source frame [clips][entry planes][h][pitch]
+};
+
+// Device scratch of one in-flight frame (the reference's per-stream slot).
+struct Slot {
+    cudaStream_t st = nullptr, cst = nullptr;
+    cudaEvent_t ev_up = nullptr;
+    float *d_src = nullptr, *d_dst = nullptr;
+    unsigned long long *num = nullptr, *den = nullptr;
+    int2 *list = nullptr;
+    float *errs = nullptr;
+    float *h_stage = nullptr;
+    size_t stage_up = 0, stage_down = 0;
+
+    void destroy() {
+        if (st) cudaStreamDestroy(st);
+        if (cst) cudaStreamDestroy(cst);
+        if (ev_up) cudaEventDestroy(ev_up);
+        cudaFree(d_src);
+        cudaFree(d_dst);
+        cudaFree(num);
+        cudaFree(den);
+        cudaFree(list);
+        cudaFree(errs);
+        if (h_stage) cudaFreeHost(h_stage);
+        *this = Slot();
+    }
+};
+
+struct Filter {
+    // configuration
+    zb3d_video_info vi{};
+    zb3d_video_info vi_out{};
+    bool v2 = false, passthrough = false;
+    bool final_ = false, chroma = false, fused = false, zero_init = true;
+    int radius = 0, tw = 1;
+    int nclips = 1;
+    float extractor = 0.0f;
+    bool process[3] = {false, false, false};
+    int device = 0;
+    int num_streams = 4;
+    std::vector<Entry> entries;
+    size_t sum_src = 0, sum_dst = 0, sum_out = 0, frame_elems = 0;
+    size_t acc_elems = 0;          // largest entry accumulator (planes * tw * h * pitch)
+    long long max_blocks = 0;
+
+    // slot pool (src/pool.zig)
+    std::vector<Slot> slots;
+    std::vector<int> free_slots;
+    std::mutex pool_mu;
+    std::condition_variable pool_cv;
+
+    // temporal caches (src/framecache.zig): source frames and accumulator stacks
+    DevCache src_cache, acc_cache;
+
+    // optional launch timing (zb3d_profile_enable)
+    bool profile = false;
+    std::mutex prof_mu;
+    std::vector<cudaEvent_t> prof_match, prof_filter;  // start/stop pairs
+
+    bool stacked_out() const { return radius > 0 && !v2; }
+    // output of one window (one centre): stacked accumulators when radius > 0
+    size_t dst_entry_elems(const Entry &e) const {
+        return radius > 0 ? (size_t)e.nplanes * tw * 2 * e.plane_elems : (size_t)e.nplanes * e.plane_elems;
+    }
+};
+
+namespace {
+
+int acquire_slot(Filter *f) {
+    std::unique_lock<std::mutex> lk(f->pool_mu);
+    f->pool_cv.wait(lk, [&] { return !f->free_slots.empty(); });
+    int s = f->free_slots.back();
+    f->free_slots.pop_back();
+    return s;
+}
+
+void release_slot(Filter *f, int s) {
+    {
+        std::lock_guard<std::mutex> lk(f->pool_mu);
+        f->free_slots.push_back(s);
+    }
+    f->pool_cv.notify_one();
+}
+
+bool alloc_slot(Filter *f, Slot &s) {
+    auto ok = [](cudaError_t e) { return e == cudaSuccess; };
+    const size_t src = f->sum_src;
+    const size_t dst = std::max(f->sum_dst, f->sum_out);
+    if (!ok(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking))) return false;
+    if (!ok(cudaStreamCreateWithFlags(&s.cst, cudaStreamNonBlocking))) return false;
+    if (!ok(cudaEventCreateWithFlags(&s.ev_up, cudaEventDisableTiming))) return false;
+    if (!ok(cudaMalloc(&s.d_src, src * sizeof(float)))) return false;
+    if (!ok(cudaMalloc(&s.d_dst, dst * sizeof(float)))) return false;
+    if (!ok(cudaMalloc(&s.num, f->acc_elems * 8))) return false;
+    if (!ok(cudaMalloc(&s.den, f->acc_elems * 8))) return false;
+    if (!ok(cudaMalloc(&s.list, f->max_blocks * 8 * sizeof(int2)))) return false;
+    if (f->radius > 0 && !ok(cudaMalloc(&s.errs, f->max_blocks * 8 * sizeof(float)))) return false;
+    s.stage_up = f->v2 && f->radius > 0 ? f->frame_elems : src;
+    s.stage_down = dst;
+    if (!ok(cudaHostAlloc((void **)&s.h_stage, (s.stage_up + s.stage_down) * sizeof(float), cudaHostAllocDefault)))
+        return false;
+    return true;
+}
+
+// Block matching of one entry into the slot's match list.
+cudaError_t run_match(Filter *f, Slot &s, const Entry &en, const float *src) {
+        MatchArgs ma{};
+        ma.frames = src;  // clip 0, plane 0: the matching plane of every window frame
+        ma.fstride = (long long)en.plane_elems;
+        ma.w = en.w;
+        ma.h = en.h;
+        ma.pitch = en.pitch;
+        ma.bs = en.bs;
+        ma.range = en.range;
+        ma.radius = f->radius;
+        ma.ps_num = en.ps_num;
+        ma.ps_range = en.ps_range;
+        ma.nbx = en.nbx;
+        ma.nby = en.nby;
+        ma.nbx_al = en.nbx_al;
+        ma.list = s.list;
+        ma.errs = f->radius > 0 ? s.errs : nullptr;
+        const int rows = 4;
+        bool tiled = (en.bs == 4 || en.bs == 8);
+        if (tiled) {
+            MatchArgs t = ma;
+            t.chunks = (2 * en.range + 1 + 3) / 4;
+            t.tile_pitch = 128 + 4 * t.chunks;
+            tiled = match_tile_bytes(t, rows) <= 200 * 1024;
+        }
+        return launch_match(ma, en.metric, rows, tiled, s.st);
+}
+
+cudaEvent_t prof_event(Filter *f, std::vector<cudaEvent_t> &v, cudaStream_t st) {
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreate(&ev) != cudaSuccess) return nullptr;
+    cudaEventRecord(ev, st);
+    std::lock_guard<std::mutex> lk(f->prof_mu);
+    v.push_back(ev);
+    return ev;
+}
+
+// Runs every entry of one window (d_src, entry layout) into d_dst on the slot's stream.
+cudaError_t run_entry(Filter *f, Slot &s, const Entry &en, const float *src, float *dst);
+
+cudaError_t run_window(Filter *f, Slot &s, const float *d_src, float *d_dst) {
+    for (const Entry &en : f->entries) {
+        cudaError_t e = run_entry(f, s, en, d_src + en.src_off, d_dst + en.dst_off);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// One entry: src = its [clips][planes][tw][h][pitch] block, dst = its output block.
+cudaError_t run_entry(Filter *f, Slot &s, const Entry &en, const float *src, float *dst) {
+    cudaError_t e = cudaSuccess;
+    {
+        const size_t acc = (size_t)en.nplanes * f->tw * en.plane_elems;
+        if ((e = cudaMemsetAsync(s.num, 0, acc * 8, s.st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(s.den, 0, acc * 8, s.st)) != cudaSuccess) return e;
+        if (f->profile) prof_event(f, f->prof_match, s.st);
+        if ((e = run_match(f, s, en, src)) != cudaSuccess) return e;
+        if (f->profile) prof_event(f, f->prof_match, s.st);
+        FilterArgs fa{};
+        fa.src = src;
+        fa.plane_stride = (long long)f->tw * en.plane_elems;
+        fa.clip_stride = (long long)en.nplanes * fa.plane_stride;
+        fa.frame_stride = (long long)en.plane_elems;
+        fa.w = en.w;
+        fa.h = en.h;
+        fa.pitch = en.pitch;
+        fa.nplanes = en.nplanes;
+        fa.chroma = f->chroma;
+        fa.list = s.list;
+        fa.nblocks = (int)en.nblocks;
+        for (int i = 0; i < 3; ++i) fa.sigma[i] = en.sigma[i];
+        fa.extractor = f->extractor;
+        fa.num = s.num;
+        fa.den = s.den;
+        fa.acc_frame_stride = (long long)en.plane_elems;
+        fa.acc_plane_stride = (long long)f->tw * en.plane_elems;
+        if (f->profile) prof_event(f, f->prof_filter, s.st);
+        if ((e = launch_filter(fa, f->final_, en.t2d, en.t1d, s.st)) != cudaSuccess) return e;
+        if (f->profile) prof_event(f, f->prof_filter, s.st);
+        if (f->radius == 0) {
+            e = launch_finish(s.num, s.den, fa.acc_plane_stride, fa.acc_frame_stride, en.w, en.h, en.pitch,
+                              en.nplanes, 1, en.proc_mask, dst, en.pitch, (long long)en.plane_elems, 0, s.st);
+        } else {
+            e = launch_finish(s.num, s.den, fa.acc_plane_stride, fa.acc_frame_stride, en.w, en.h, en.pitch,
+                              en.nplanes, f->tw, en.proc_mask, dst, en.pitch,
+                              (long long)f->tw * 2 * en.plane_elems, 1, s.st);
+        }
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+void copy_plane_in(float *dst, int pitch, const float *src, ptrdiff_t stride_bytes, int w, int h) {
+    for (int y = 0; y < h; ++y)
+        memcpy(dst + (size_t)y * pitch, (const char *)src + (ptrdiff_t)y * stride_bytes, (size_t)w * sizeof(float));
+}
+
+void copy_plane_out(float *dst, ptrdiff_t stride_bytes, const float *src, int pitch, int w, int h) {
+    for (int y = 0; y < h; ++y)
+        memcpy((char *)dst + (ptrdiff_t)y * stride_bytes, src + (size_t)y * pitch, (size_t)w * sizeof(float));
+}
+
+int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+}  // namespace
+
+}  // namespace zb
+
+using zb::Entry;
+using zb::Filter;
+
+extern "C" {
+
+void zb3d_args_init(zb3d_args *a) {
+    memset(a, 0, sizeof *a);
+    a->radius = a->chroma = a->device_id = a->num_streams = a->extractor_exp = ZB3D_UNSET;
+    a->zero_init = a->fast_fused = ZB3D_UNSET;
+}
+
+const char *zb3d_version(void) { return "zb3d 0.1.0 (sm_100a)"; }
+
+int zb3d_agg_z(int i, int n, int nframes, int radius) {
+    return std::min(std::max(2 * radius - i, n - nframes + 1 + radius), n + radius);
+}
+
+static Filter *create_impl(const zb3d_video_info *clip, const zb3d_args *a, int v2, char *err, size_t errlen) {
+    using namespace zb;
+    zb3d_args dflt;
+    if (!a) {
+        zb3d_args_init(&dflt);
+        a = &dflt;
+    }
+    std::unique_ptr<Filter> f(new Filter());
+    f->vi = *clip;
+    f->v2 = v2 != 0;
+    const zb3d_video_info &vi = *clip;
+
+    if (f->v2) {
+        // BM3Dv2: planes whose sigma is below FLT_EPSILON pass through; all of them -> the clip itself
+        bool proc[3] = {true, true, true};
+        for (int i = 0; i < 3; ++i) {
+            if (i < a->n_sigma)
+                proc[i] = !(a->sigma[i] < kFltEpsilon);
+            else if (i > 0)
+                proc[i] = proc[i - 1];
+        }
+        bool skip = true;
+        for (int i = 0; i < std::min(vi.num_planes, 3); ++i)
+            if (proc[i]) skip = false;
+        if (skip) {
+            f->passthrough = true;
+            f->vi_out = vi;
+            return f.release();
+        }
+    }
+    if (vi.width <= 0 || vi.height <= 0 || vi.sample_type != ZB3D_FLOAT || vi.bits_per_sample != 32) {
+        set_err(err, errlen, "BM3D: only constant format 32 bit float input supported.");
+        return nullptr;
+    }
+    if (a->ref) {
+        const zb3d_video_info &r = *a->ref;
+        if (r.color_family != vi.color_family || r.sample_type != vi.sample_type ||
+            r.bits_per_sample != vi.bits_per_sample || r.subsampling_w != vi.subsampling_w ||
+            r.subsampling_h != vi.subsampling_h) {
+            set_err(err, errlen, "BM3D: \"ref\" must be of the same format as \"clip\".");
+            return nullptr;
+        }
+        if (r.width != vi.width || r.height != vi.height) {
+            set_err(err, errlen, "BM3D: \"ref\" must be of the same dimensions as \"clip\".");
+            return nullptr;
+        }
+        if (r.num_frames != vi.num_frames) {
+            set_err(err, errlen, "BM3D: \"ref\" must be of the same number of frames as \"clip\".");
+            return nullptr;
+        }
+        f->final_ = true;
+    }
+    float sigma[3];
+    per_plane<float>(a->sigma, a->n_sigma, 3.0f, sigma);
+    for (float s : sigma)
+        if (!(s >= 0)) {
+            set_err(err, errlen, "BM3D: \"sigma\" must be non-negative.");
+            return nullptr;
+        }
+    for (int i = 0; i < 3; ++i) f->process[i] = !(sigma[i] < kFltEpsilon);
+    // f32(2.7*0.75*64/255) / f32(0.75*64/255) as the reference stores them (src/bm3d.zig:1019-1024)
+    const float factor = f->final_ ? f32_from_bits(0x3e40c0c1u) : f32_from_bits(0x3f021bb6u);
+    for (float &s : sigma) s *= factor;
+
+    int block_step[3], bm_range[3], ps_num[3], ps_range[3];
+    per_plane<int>(a->block_step, a->n_block_step, 8, block_step);
+    for (int v : block_step)
+        if (v <= 0 || v > 8) {
+            set_err(err, errlen, "BM3D: \"block_step\" must be in range [1, 8].");
+            return nullptr;
+        }
+    per_plane<int>(a->bm_range, a->n_bm_range, 9, bm_range);
+    for (int v : bm_range)
+        if (v <= 0) {
+            set_err(err, errlen, "BM3D: \"bm_range\" must be positive.");
+            return nullptr;
+        }
+    per_plane<int>(a->ps_num, a->n_ps_num, 2, ps_num);
+    for (int v : ps_num)
+        if (v <= 0 || v > 8) {
+            set_err(err, errlen, "BM3D: \"ps_num\" must be in range [1, 8].");
+            return nullptr;
+        }
+    per_plane<int>(a->ps_range, a->n_ps_range, 4, ps_range);
+    for (int v : ps_range)
+        if (v <= 0) {
+            set_err(err, errlen, "BM3D: \"ps_range\" must be positive.");
+            return nullptr;
+        }
+    f->radius = pick(a->radius, 0);
+    if (f->radius < 0) {
+        set_err(err, errlen, "BM3D: \"radius\" must be non-negative.");
+        return nullptr;
+    }
+    if (f->radius > kMaxRadius) {
+        set_err(err, errlen, "BM3D: \"radius\" must be <= 16.");
+        return nullptr;
+    }
+    f->tw = 2 * f->radius + 1;
+    f->fused = f->v2 && pick(a->fast_fused, 0) != 0 && f->radius > 0;
+    f->chroma = pick(a->chroma, 0) != 0;
+    if (f->chroma && (vi.color_family != ZB3D_YUV || vi.subsampling_w != 0 || vi.subsampling_h != 0)) {
+        set_err(err, errlen, "BM3D: clip format must be YUV444 when \"chroma\" is true.");
+        return nullptr;
+    }
+    f->zero_init = pick(a->zero_init, 1) != 0;
+    const int extractor_exp = pick(a->extractor_exp, 0);
+    f->extractor = extractor_exp != 0 ? std::ldexp(1.0f, extractor_exp) : 0.0f;
+
+    int metric[3] = {M_SSD, M_SSD, M_SSD}, t2d[3] = {0, 0, 0}, t1d[3] = {0, 0, 0};
+    for (int i = 0; i < 3; ++i) {
+        if (i < a->n_bm_error_s) {
+            metric[i] = parse_metric(a->bm_error_s[i]);
+            if (metric[i] < 0) {
+                set_err(err, errlen, "BM3D: invalid \"bm_error_s\".");
+                return nullptr;
+            }
+        } else if (i > 0) {
+            metric[i] = metric[i - 1];
+        }
+        if (i < a->n_transform_2d_s) {
+            t2d[i] = parse_transform(a->transform_2d_s[i]);
+            if (t2d[i] < 0) {
+                set_err(err, errlen, "BM3D: invalid \"transform_2d_s\".");
+                return nullptr;
+            }
+        } else if (i > 0) {
+            t2d[i] = t2d[i - 1];
+        }
+        if (i < a->n_transform_1d_s) {
+            t1d[i] = parse_transform(a->transform_1d_s[i]);
+            if (t1d[i] < 0) {
+                set_err(err, errlen, "BM3D: invalid \"transform_1d_s\".");
+                return nullptr;
+            }
+        } else if (i > 0) {
+            t1d[i] = t1d[i - 1];
+        }
+    }
+    f->device = pick(a->device_id, 0);
+    if (f->device < 0) {
+        set_err(err, errlen, "BM3D: invalid device ID.");
+        return nullptr;
+    }
+    if (a->num_streams != ZB3D_UNSET && (a->num_streams < 1 || a->num_streams > 32)) {
+        set_err(err, errlen, "BM3D: num_streams must be 1..32.");
+        return nullptr;
+    }
+    f->num_streams = pick(a->num_streams, 4);
+
+    bool any = false;
+    for (int i = 0; i < vi.num_planes && i < 3; ++i) any |= f->process[i];
+    if (!any) {
+        set_err(err, errlen, "BM3D: all planes have sigma < FLT_EPSILON (nothing to process).");
+        return nullptr;
+    }
+    f->nclips = f->final_ ? 2 : 1;
+
+    auto fill_geom = [&](Entry &e) {
+        e.pitch = round_up(e.w, 32);
+        e.plane_elems = (size_t)e.h * e.pitch;
+        e.nbx = (e.w - 8 + e.bs - 1) / e.bs + 1;
+        e.nby = (e.h - 8 + e.bs - 1) / e.bs + 1;
+        e.nbx_al = (e.w - 8) / e.bs + 1;
+        e.nblocks = (long long)e.nbx * e.nby;
+    };
+    if (f->chroma) {
+        Entry e{};
+        e.w = vi.width;
+        e.h = vi.height;
+        e.nplanes = 3;
+        for (int i = 0; i < 3; ++i) {
+            e.planes[i] = i;
+            e.sigma[i] = sigma[i];
+        }
+        e.bs = block_step[0];
+        e.range = bm_range[0];
+        e.ps_num = ps_num[0];
+        e.ps_range = ps_range[0];
+        e.proc_mask = 0;
+        for (int i = 0; i < 3; ++i) e.proc_mask |= (unsigned)f->process[i] << i;
+        e.metric = metric[0];
+        e.t2d = t2d[0];
+        e.t1d = t1d[0];
+        if (vi.width < 8 || vi.height < 8) {
+            set_err(err, errlen, "BM3D: every processed plane must be at least 8x8.");
+            return nullptr;
+        }
+        fill_geom(e);
+        f->entries.push_back(e);
+    } else {
+        for (int p = 0; p < vi.num_planes && p < 3; ++p) {
+            if (!f->process[p]) continue;
+            Entry e{};
+            e.w = p == 0 ? vi.width : vi.width >> vi.subsampling_w;
+            e.h = p == 0 ? vi.height : vi.height >> vi.subsampling_h;
+            if (e.w < 8 || e.h < 8) {
+                set_err(err, errlen, "BM3D: every processed plane must be at least 8x8.");
+                return nullptr;
+            }
+            e.nplanes = 1;
+            e.planes[0] = p;
+            e.sigma[0] = e.sigma[1] = e.sigma[2] = sigma[p];
+            e.bs = block_step[p];
+            e.range = bm_range[p];
+            e.ps_num = ps_num[p];
+            e.ps_range = ps_range[p];
+            e.proc_mask = 1;
+            e.metric = metric[p];
+            e.t2d = t2d[p];
+            e.t1d = t1d[p];
+            fill_geom(e);
+            f->entries.push_back(e);
+        }
+    }
+    size_t src_off = 0, dst_off = 0, out_off = 0, frame_off = 0;
+    for (Entry &e : f->entries) {
+        if (e.w > 65535 || e.h > 65535) {
+            set_err(err, errlen, "BM3D: frame too large (planes are limited to 65535x65535).");
+            return nullptr;
+        }
+        e.src_off = src_off;
+        e.src_elems = (size_t)f->nclips * e.nplanes * f->tw * e.plane_elems;
+        e.dst_off = dst_off;
+        e.dst_elems = f->dst_entry_elems(e);
+        e.out_off = out_off;
+        e.frame_off = frame_off;
+        src_off += e.src_elems;
+        dst_off += e.dst_elems;
+        out_off += (size_t)e.nplanes * e.plane_elems;
+        frame_off += (size_t)f->nclips * e.nplanes * e.plane_elems;
+        f->acc_elems = std::max(f->acc_elems, (size_t)e.nplanes * f->tw * e.plane_elems);
+        f->max_blocks = std::max(f->max_blocks, e.nblocks);
+        // int32 index limits of the reference (src/bm3d.zig:1190-1201)
+        if (e.src_elems >= (1ull << 31) || (size_t)e.nplanes * f->tw * 2 * e.plane_elems >= (1ull << 31)) {
+            set_err(err, errlen, "BM3D: frame/radius too large (a device region exceeds 2^31 samples).");
+            return nullptr;
+        }
+        if (e.plane_elems * f->tw * 2 * 4 >= (1ull << 32)) {
+            set_err(err, errlen, "BM3D: stacked output plane too large (exceeds 4 GiB).");
+            return nullptr;
+        }
+    }
+    f->sum_src = src_off;
+    f->sum_dst = dst_off;
+    f->sum_out = out_off;
+    f->frame_elems = frame_off;
+
+    f->vi_out = vi;
+    if (f->stacked_out()) {
+        const long long mult = 2LL * (2LL * f->radius + 1);
+        if ((long long)vi.height * mult > INT_MAX) {
+            set_err(err, errlen, "BM3D: clip too tall for the stacked output.");
+            return nullptr;
+        }
+        f->vi_out.height = (int)(vi.height * mult);
+    }
+
+    // ---- CUDA resources (src/bm3d.zig:772-951) ----
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || f->device >= ndev) {
+        set_err(err, errlen, "BM3D: invalid device ID.");
+        return nullptr;
+    }
+    cudaSetDevice(f->device);
+    f->slots.resize(f->num_streams);
+    int made = 0;
+    for (auto &s : f->slots) {
+        if (!alloc_slot(f.get(), s)) {
+            s.destroy();
+            cudaGetLastError();
+            if (made > 0) break;  // keep the slots that fit (src/pool.zig:31-49)
+            set_err(err, errlen, "BM3D: out of device memory.");
+            return nullptr;
+        }
+        ++made;
+    }
+    f->slots.resize(made);
+    for (int i = made - 1; i >= 0; --i) f->free_slots.push_back(i);
+    if (f->v2 && f->radius > 0) {
+        // source frames: one request spans 4r+1 frames; accumulator stacks: 2r+1 centres
+        const int span = 4 * f->radius + 1;
+        const int n_src = span * (made + 1);
+        const int n_acc = f->tw * (made + 1);
+        const size_t stack_bytes = f->sum_dst * sizeof(float);
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const size_t need = (size_t)f->frame_elems * 4 * n_src + stack_bytes * (size_t)n_acc;
+        if (need + (256u << 20) > free_b || !f->src_cache.init(f->frame_elems * sizeof(float), n_src) ||
+            !f->acc_cache.init(stack_bytes, n_acc)) {
+            cudaGetLastError();
+            if (!f->fused) {
+                set_err(err, errlen, "BM3D: out of device memory.");
+                for (auto &s : f->slots) s.destroy();
+                return nullptr;
+            }
+            set_err(err, errlen,
+                    "BM3Dv2: fast_fused needs at least %zu MiB of accumulator cache (%d slots x %zu MiB) but only "
+                    "%zu MiB of device memory is free. Use fast_fused=False (composed BM3D + VAggregate, much less "
+                    "VRAM), or lower num_streams/radius.",
+                    (stack_bytes * f->tw) >> 20, f->tw, stack_bytes >> 20, free_b >> 20);
+            for (auto &s : f->slots) s.destroy();
+            return nullptr;
+        }
+    }
+    return f.release();
+}
+
+zb3d_filter *zb3d_create(const zb3d_video_info *clip, const zb3d_args *args, int v2, char *err, size_t errlen) {
+    if (!clip) {
+        zb::set_err(err, errlen, "BM3D: clip is required.");
+        return nullptr;
+    }
+    return reinterpret_cast<zb3d_filter *>(create_impl(clip, args, v2, err, errlen));
+}
+
+void zb3d_output_info(const zb3d_filter *fp, zb3d_video_info *out) {
+    *out = reinterpret_cast<const Filter *>(fp)->vi_out;
+}
+
+void zb3d_frame_range(const zb3d_filter *fp, int n, int *first, int *last) {
+    const Filter *f = reinterpret_cast<const Filter *>(fp);
+    const int req = f->passthrough ? 0 : (f->v2 ? 2 * f->radius : f->radius);
+    *first = std::max(n - req, 0);
+    *last = std::min(n + req, f->vi.num_frames - 1);
+}
+
+void zb3d_output_props(const zb3d_filter *fp, int *radius, int process[3]) {
+    const Filter *f = reinterpret_cast<const Filter *>(fp);
+    *radius = f->radius;
+    for (int i = 0; i < 3; ++i) process[i] = f->process[i];
+}
+
+int zb3d_num_entries(const zb3d_filter *fp) { return (int)reinterpret_cast<const Filter *>(fp)->entries.size(); }
+
+int zb3d_entry_layout_get(const zb3d_filter *fp, int e, zb3d_entry_layout *o) {
+    const Filter *f = reinterpret_cast<const Filter *>(fp);
+    if (e < 0 || e >= (int)f->entries.size()) return -1;
+    const Entry &en = f->entries[e];
+    o->nplanes = en.nplanes;
+    for (int i = 0; i < 3; ++i) o->plane[i] = en.planes[i];
+    o->width = en.w;
+    o->height = en.h;
+    o->pitch = en.pitch;
+    o->tw = f->tw;
+    o->nclips = f->nclips;
+    o->src_offset = en.src_off;
+    o->src_elems = en.src_elems;
+    o->dst_offset = en.dst_off;
+    o->dst_elems = en.dst_elems;
+    return 0;
+}
+
+size_t zb3d_src_elems(const zb3d_filter *fp) { return reinterpret_cast<const Filter *>(fp)->sum_src; }
+size_t zb3d_dst_elems(const zb3d_filter *fp) { return reinterpret_cast<const Filter *>(fp)->sum_dst; }
+
+int zb3d_process_device(zb3d_filter *fp, const float *d_src, float *d_dst, void *stream, char *err, size_t errlen) {
+    Filter *f = reinterpret_cast<Filter *>(fp);
+    if (f->passthrough || f->slots.empty()) {
+        zb::set_err(err, errlen, "BM3D: nothing to process on the device.");
+        return -1;
+    }
+    cudaSetDevice(f->device);
+    zb::Slot s = f->slots[0];
+    s.st = stream ? (cudaStream_t)stream : f->slots[0].st;
+    cudaError_t e = zb::run_window(f, s, d_src, d_dst);
+    if (e != cudaSuccess) {
+        zb::set_err(err, errlen, "BM3D: process frame failed (%s).", cudaGetErrorString(e));
+        return -1;
+    }
+    return 0;
+}
+
+int zb3d_process_entry_device(zb3d_filter *fp, int e, const float *d_src, float *d_dst, void *stream, char *err,
+                              size_t errlen) {
+    Filter *f = reinterpret_cast<Filter *>(fp);
+    if (f->passthrough || e < 0 || e >= (int)f->entries.size()) {
+        zb::set_err(err, errlen, "BM3D: no such entry.");
+        return -1;
+    }
+    cudaSetDevice(f->device);
+    zb::Slot s = f->slots[0];
+    s.st = stream ? (cudaStream_t)stream : f->slots[0].st;
+    cudaError_t ce = zb::run_entry(f, s, f->entries[e], d_src, d_dst);
+    if (ce != cudaSuccess) {
+        zb::set_err(err, errlen, "BM3D: process frame failed (%s).", cudaGetErrorString(ce));
+        return -1;
+    }
+    return 0;
+}
+
+void zb3d_profile_enable(zb3d_filter *fp, int on) { reinterpret_cast<Filter *>(fp)->profile = on != 0; }
+
+int zb3d_profile_collect(zb3d_filter *fp, double *match_ms, int *match_launches, double *filter_ms,
+                         int *filter_launches) {
+    Filter *f = reinterpret_cast<Filter *>(fp);
+    std::lock_guard<std::mutex> lk(f->prof_mu);
+    auto sum = [](std::vector<cudaEvent_t> &v, double *ms, int *n) {
+        double t = 0.0;
+        int k = 0;
+        for (size_t i = 0; i + 1 < v.size(); i += 2) {
+            cudaEventSynchronize(v[i + 1]);
+            float x = 0.0f;
+            if (cudaEventElapsedTime(&x, v[i], v[i + 1]) == cudaSuccess) {
+                t += x;
+                ++k;
+            }
+        }
+        for (cudaEvent_t ev : v) cudaEventDestroy(ev);
+        v.clear();
+        if (ms) *ms = t;
+        if (n) *n = k;
+    };
+    sum(f->prof_match, match_ms, match_launches);
+    sum(f->prof_filter, filter_ms, filter_launches);
+    return 0;
+}
+
+int zb3d_match_device(zb3d_filter *fp, int e, const float *d_src, int32_t *d_list, void *stream, char *err,
+                      size_t errlen) {
+    Filter *f = reinterpret_cast<Filter *>(fp);
+    if (f->passthrough || e < 0 || e >= (int)f->entries.size()) {
+        zb::set_err(err, errlen, "BM3D: no such entry.");
+        return -1;
+    }
+    cudaSetDevice(f->device);
+    zb::Slot s = f->slots[0];
+    s.st = stream ? (cudaStream_t)stream : f->slots[0].st;
+    const Entry &en = f->entries[e];
+    cudaError_t ce = zb::run_match(f, s, en, d_src + en.src_off);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(d_list, s.list, (size_t)en.nblocks * 8 * sizeof(int2), cudaMemcpyDeviceToDevice, s.st);
+    if (ce != cudaSuccess) {
+        zb::set_err(err, errlen, "BM3D: matching failed (%s).", cudaGetErrorString(ce));
+        return -1;
+    }
+    return 0;
+}
+
+int zb3d_vaggregate_device(const float *const *stacks, const int *z, int tw, int width, int height, int pitch,
+                           int nplanes, unsigned proc_mask, float *d_dst, void *stream) {
+    return zb::launch_vagg(stacks, z, tw, width, height, pitch, nplanes, proc_mask, d_dst, pitch,
+                           (long long)height * pitch, (cudaStream_t)stream) == cudaSuccess
+               ? 0
+               : -1;
+}
+
+// ---- host-frame path ------------------------------------------------------
+
+static int get_frame_window(Filter *f, int n, const zb3d_frame *clip_frames, const zb3d_frame *ref_frames,
+                            zb3d_frame_out *dst, char *err, size_t errlen) {
+    using namespace zb;
+    int first, last;
+    zb3d_frame_range(reinterpret_cast<zb3d_filter *>(f), n, &first, &last);
+    const int nf = f->vi.num_frames;
+    const int slot = acquire_slot(f);
+    Slot &s = f->slots[slot];
+    cudaSetDevice(f->device);
+    // stage the window [clips][planes][t][h][pitch] per entry
+    for (const Entry &e : f->entries) {
+        for (int c = 0; c < f->nclips; ++c) {
+            const zb3d_frame *frames = (f->final_ && c == 0) ? ref_frames : clip_frames;
+            for (int i = 0; i < e.nplanes; ++i)
+                for (int t = 0; t < f->tw; ++t) {
+                    const int idx = clampi(n - f->radius + t, 0, nf - 1);
+                    const zb3d_frame &fr = frames[idx - first];
+                    const int p = e.planes[i];
+                    float *d = s.h_stage + e.src_off + ((size_t)(c * e.nplanes + i) * f->tw + t) * e.plane_elems;
+                    copy_plane_in(d, e.pitch, fr.ptr[p], fr.stride[p], e.w, e.h);
+                }
+        }
+    }
+    cudaError_t ce = cudaMemcpyAsync(s.d_src, s.h_stage, f->sum_src * sizeof(float), cudaMemcpyHostToDevice, s.cst);
+    if (ce == cudaSuccess) ce = cudaEventRecord(s.ev_up, s.cst);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s.st, s.ev_up, 0);
+    if (ce == cudaSuccess) ce = run_window(f, s, s.d_src, s.d_dst);
+    float *down = s.h_stage + s.stage_up;
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(down, s.d_dst, f->sum_dst * sizeof(float), cudaMemcpyDeviceToHost, s.st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s.st);
+    if (ce != cudaSuccess) {
+        cudaStreamSynchronize(s.cst);
+        cudaStreamSynchronize(s.st);
+        release_slot(f, slot);
+        set_err(err, errlen, "BM3D: process frame failed. (%s)", cudaGetErrorString(ce));
+        return -1;
+    }
+    for (const Entry &e : f->entries) {
+        for (int i = 0; i < e.nplanes; ++i) {
+            if (!((e.proc_mask >> i) & 1)) continue;
+            const int p = e.planes[i];
+            if (f->stacked_out()) {
+                const float *src = down + e.dst_off + (size_t)i * f->tw * 2 * e.plane_elems;
+                copy_plane_out(dst->ptr[p], dst->stride[p], src, e.pitch, e.w, e.h * 2 * f->tw);
+            } else {
+                copy_plane_out(dst->ptr[p], dst->stride[p], down + e.dst_off + (size_t)i * e.plane_elems, e.pitch,
+                               e.w, e.h);
+            }
+        }
+    }
+    if (f->stacked_out() && f->zero_init) {
+        for (int p = 0; p < f->vi.num_planes && p < 3; ++p) {
+            if (f->process[p]) continue;
+            const int w = p == 0 ? f->vi.width : f->vi.width >> f->vi.subsampling_w;
+            const int h = (p == 0 ? f->vi_out.height : f->vi_out.height >> f->vi.subsampling_h);
+            for (int y = 0; y < h; ++y) memset((char *)dst->ptr[p] + (ptrdiff_t)y * dst->stride[p], 0, (size_t)w * 4);
+        }
+    }
+    release_slot(f, slot);
+    return 0;
+}
+
+// BM3Dv2 radius > 0: accumulator stacks of the 2r+1 centres around n (cached on
+// the device by centre), then the temporal aggregation.  The stacks and the
+// aggregation are those of the composed BM3D + VAggregate chain, so the output
+// is the same byte for byte (src/bm3d.zig:481-633).
+static int get_frame_temporal(Filter *f, int n, const zb3d_frame *clip_frames, const zb3d_frame *ref_frames,
+                              zb3d_frame_out *dst, char *err, size_t errlen) {
+    using namespace zb;
+    const int r = f->radius, tw = f->tw, nf = f->vi.num_frames;
+    int first, last;
+    zb3d_frame_range(reinterpret_cast<zb3d_filter *>(f), n, &first, &last);
+    const int slot = acquire_slot(f);
+    Slot &s = f->slots[slot];
+    cudaSetDevice(f->device);
+    cudaError_t ce = cudaSuccess;
+
+    // centres and their accumulator stacks
+    long long ckeys[kMaxTw];
+    int centres[kMaxTw], nc = 0;
+    for (int i = 0; i < tw; ++i) {
+        const int m = clampi(n - r + i, 0, nf - 1);
+        bool dup = false;
+        for (int k = 0; k < nc; ++k) dup |= centres[k] == m;
+        if (!dup) {
+            centres[nc] = m;
+            ckeys[nc] = m;
+            ++nc;
+        }
+    }
+    int aidx[kMaxTw];
+    bool aload[kMaxTw];
+    f->acc_cache.acquire(ckeys, nc, aidx, aload);
+
+    // source frames the missing centres need
+    long long skeys[4 * kMaxRadius + 1];
+    int sframes[4 * kMaxRadius + 1], ns = 0;
+    for (int k = 0; k < nc; ++k) {
+        if (!aload[k]) continue;
+        for (int t = 0; t < tw; ++t) {
+            const int idx = clampi(centres[k] - r + t, 0, nf - 1);
+            bool dup = false;
+            for (int q = 0; q < ns; ++q) dup |= sframes[q] == idx;
+            if (!dup) {
+                sframes[ns] = idx;
+                skeys[ns] = idx;
+                ++ns;
+            }
+        }
+    }
+    int sidx[4 * kMaxRadius + 1];
+    bool sload[4 * kMaxRadius + 1];
+    if (ns) f->src_cache.acquire(skeys, ns, sidx, sload);
+    for (int q = 0; q < ns && ce == cudaSuccess; ++q) {
+        if (!sload[q]) continue;
+        const int idx = sframes[q];
+        float *stage = s.h_stage;  // one frame at a time through the up-stage
+        for (const Entry &e : f->entries)
+            for (int c = 0; c < f->nclips; ++c) {
+                const zb3d_frame *frames = (f->final_ && c == 0) ? ref_frames : clip_frames;
+                const zb3d_frame &fr = frames[idx - first];
+                for (int i = 0; i < e.nplanes; ++i) {
+                    const int p = e.planes[i];
+                    copy_plane_in(stage + e.frame_off + (size_t)(c * e.nplanes + i) * e.plane_elems, e.pitch,
+                                  fr.ptr[p], fr.stride[p], e.w, e.h);
+                }
+            }
+        ce = cudaMemcpyAsync(f->src_cache.buf(sidx[q]), stage, f->frame_elems * sizeof(float), cudaMemcpyHostToDevice,
+                             s.cst);
+        if (ce == cudaSuccess) ce = cudaEventRecord(f->src_cache.ev(sidx[q]), s.cst);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(s.cst);  // the stage is reused by the next frame
+        if (ce == cudaSuccess) f->src_cache.publish(sidx[q]);
+    }
+    for (int q = 0; q < ns && ce == cudaSuccess; ++q) ce = cudaStreamWaitEvent(s.st, f->src_cache.ev(sidx[q]), 0);
+
+    // compute the missing stacks
+    for (int k = 0; k < nc && ce == cudaSuccess; ++k) {
+        if (!aload[k]) continue;
+        const int m = centres[k];
+        for (const Entry &e : f->entries)
+            for (int c = 0; c < f->nclips; ++c)
+                for (int i = 0; i < e.nplanes; ++i)
+                    for (int t = 0; t < tw && ce == cudaSuccess; ++t) {
+                        const int idx = clampi(m - r + t, 0, nf - 1);
+                        int q = 0;
+                        while (sframes[q] != idx) ++q;
+                        const float *from = (const float *)f->src_cache.buf(sidx[q]) + e.frame_off +
+                                            (size_t)(c * e.nplanes + i) * e.plane_elems;
+                        float *to = s.d_src + e.src_off + ((size_t)(c * e.nplanes + i) * tw + t) * e.plane_elems;
+                        ce = cudaMemcpyAsync(to, from, e.plane_elems * sizeof(float), cudaMemcpyDeviceToDevice, s.st);
+                    }
+        if (ce != cudaSuccess) break;
+        // the window's stacked accumulators go straight into the cache slot
+        float *stack = (float *)f->acc_cache.buf(aidx[k]);
+        ce = run_window(f, s, s.d_src, stack);
+        if (ce == cudaSuccess) ce = cudaEventRecord(f->acc_cache.ev(aidx[k]), s.st);
+        if (ce == cudaSuccess) f->acc_cache.publish(aidx[k]);
+    }
+    for (int k = 0; k < nc && ce == cudaSuccess; ++k) ce = cudaStreamWaitEvent(s.st, f->acc_cache.ev(aidx[k]), 0);
+
+    // temporal aggregation of frame n
+    float *down = s.h_stage + s.stage_up;
+    for (const Entry &e : f->entries) {
+        if (ce != cudaSuccess) break;
+        const float *ptrs[kMaxTw];
+        int zs[kMaxTw];
+        for (int i = 0; i < tw; ++i) {
+            const int m = clampi(n - r + i, 0, nf - 1);
+            int k = 0;
+            while (centres[k] != m) ++k;
+            ptrs[i] = (const float *)f->acc_cache.buf(aidx[k]) + e.dst_off;
+            zs[i] = zb3d_agg_z(i, n, nf, r);
+        }
+        ce = launch_vagg(ptrs, zs, tw, e.w, e.h, e.pitch, e.nplanes, e.proc_mask, s.d_dst + e.out_off, e.pitch,
+                         (long long)e.plane_elems, s.st);
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(down, s.d_dst, f->sum_out * sizeof(float), cudaMemcpyDeviceToHost, s.st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s.st);
+    // claims are dropped only after the streams drained (released slots may be reloaded at once)
+    if (ce != cudaSuccess) {
+        cudaStreamSynchronize(s.cst);
+        cudaStreamSynchronize(s.st);
+        for (int q = 0; q < ns; ++q)
+            if (sload[q]) f->src_cache.abandon(sidx[q]);
+        if (ns) f->src_cache.release(sidx, ns);
+        for (int k = 0; k < nc; ++k)
+            if (aload[k]) f->acc_cache.abandon(aidx[k]);
+        f->acc_cache.release(aidx, nc);
+        release_slot(f, slot);
+        set_err(err, errlen, "BM3Dv2: process frame failed. (%s)", cudaGetErrorString(ce));
+        return -1;
+    }
+    if (ns) f->src_cache.release(sidx, ns);
+    f->acc_cache.release(aidx, nc);
+    for (const Entry &e : f->entries)
+        for (int i = 0; i < e.nplanes; ++i) {
+            if (!((e.proc_mask >> i) & 1)) continue;
+            const int p = e.planes[i];
+            copy_plane_out(dst->ptr[p], dst->stride[p], down + e.out_off + (size_t)i * e.plane_elems, e.pitch, e.w,
+                           e.h);
+        }
+    release_slot(f, slot);
+    return 0;
+}
+
+int zb3d_get_frame(zb3d_filter *fp, int n, const zb3d_frame *clip_frames, const zb3d_frame *ref_frames,
+                   zb3d_frame_out *dst, char *err, size_t errlen) {
+    Filter *f = reinterpret_cast<Filter *>(fp);
+    if (n < 0 || n >= f->vi.num_frames) {
+        zb::set_err(err, errlen, "BM3D: frame %d out of range.", n);
+        return -1;
+    }
+    if (f->passthrough) {
+        int first, last;
+        zb3d_frame_range(fp, n, &first, &last);
+        const zb3d_frame &fr = clip_frames[n - first];
+        for (int p = 0; p < f->vi.num_planes && p < 3; ++p) {
+            const int w = p == 0 ? f->vi.width : f->vi.width >> f->vi.subsampling_w;
+            const int h = p == 0 ? f->vi.height : f->vi.height >> f->vi.subsampling_h;
+            for (int y = 0; y < h; ++y)
+                memcpy((char *)dst->ptr[p] + (ptrdiff_t)y * dst->stride[p],
+                       (const char *)fr.ptr[p] + (ptrdiff_t)y * fr.stride[p], (size_t)w * 4);
+        }
+        return 0;
+    }
+    if (f->final_ && !ref_frames) {
+        zb::set_err(err, errlen, "BM3D: ref frames are required.");
+        return -1;
+    }
+    if (f->v2 && f->radius > 0) return get_frame_temporal(f, n, clip_frames, ref_frames, dst, err, errlen);
+    return get_frame_window(f, n, clip_frames, ref_frames, dst, err, errlen);
+}
+
+void zb3d_free(zb3d_filter *fp) {
+    Filter *f = reinterpret_cast<Filter *>(fp);
+    if (!f) return;
+    if (!f->passthrough) {
+        cudaSetDevice(f->device);
+        for (auto &s : f->slots) {
+            if (s.st) cudaStreamSynchronize(s.st);
+            if (s.cst) cudaStreamSynchronize(s.cst);
+            s.destroy();
+        }
+        f->src_cache.clear();
+        f->acc_cache.clear();
+    }
+    delete f;
+}
+
+// ---- VAggregate -----------------------------------------------------------
+
+struct zb3d_vagg {
+    zb3d_video_info vi;       // src
+    int radius;
+    bool process[3];
+    int device;
+    std::mutex mu;
+    float *d_in = nullptr, *d_out = nullptr, *h_stage = nullptr;
+    size_t in_elems = 0, out_elems = 0;
+    cudaStream_t st = nullptr;
+};
+
+zb3d_vagg *zb3d_vaggregate_create(const zb3d_video_info *clip, const zb3d_video_info *src, const int *planes,
+                                  int n_planes, char *err, size_t errlen) {
+    using namespace zb;
+    if (src->height <= 0 || src->sample_type != ZB3D_FLOAT || src->bits_per_sample != 32) {
+        set_err(err, errlen, "VAggregate: \"src\" must be 32 bit float.");
+        return nullptr;
+    }
+    if (clip->color_family != src->color_family || clip->sample_type != src->sample_type ||
+        clip->bits_per_sample != src->bits_per_sample || clip->subsampling_w != src->subsampling_w ||
+        clip->subsampling_h != src->subsampling_h || clip->num_frames != src->num_frames) {
+        set_err(err, errlen, "VAggregate: \"clip\" must have the same format and frame count as \"src\".");
+        return nullptr;
+    }
+    const int ratio = clip->height / src->height;
+    if (ratio < 6 || (ratio - 2) % 4 != 0 || clip->height % src->height != 0 || clip->width != src->width) {
+        set_err(err, errlen, "VAggregate: \"clip\" is not a BM3D stacked clip of \"src\" (radius >= 1).");
+        return nullptr;
+    }
+    const int radius = (ratio - 2) / 4;
+    if (radius > kMaxRadius) {
+        set_err(err, errlen, "VAggregate: radius too large.");
+        return nullptr;
+    }
+    bool proc[3] = {false, false, false};
+    for (int i = 0; i < n_planes; ++i) {
+        if (planes[i] < 0 || planes[i] > 2) {
+            set_err(err, errlen, "VAggregate: \"planes\" must be 0..2.");
+            return nullptr;
+        }
+        proc[planes[i]] = true;
+    }
+    if (n_planes == 0) {
+        set_err(err, errlen, "VAggregate: \"planes\" is required.");
+        return nullptr;
+    }
+    zb3d_vagg *v = new zb3d_vagg();
+    v->vi = *src;
+    v->radius = radius;
+    for (int i = 0; i < 3; ++i) v->process[i] = proc[i];
+    cudaGetDevice(&v->device);
+    return v;
+}
+
+void zb3d_vaggregate_output_info(const zb3d_vagg *v, zb3d_video_info *out) { *out = v->vi; }
+
+void zb3d_vaggregate_frame_range(const zb3d_vagg *v, int n, int *first, int *last) {
+    *first = std::max(n - v->radius, 0);
+    *last = std::min(n + v->radius, v->vi.num_frames - 1);
+}
+
+int zb3d_vaggregate_get_frame(zb3d_vagg *v, int n, const zb3d_frame *stacks, zb3d_frame_out *dst, char *err,
+                              size_t errlen) {
+    using namespace zb;
+    std::lock_guard<std::mutex> lk(v->mu);
+    const int r = v->radius, tw = 2 * r + 1, nf = v->vi.num_frames;
+    int first, last;
+    zb3d_vaggregate_frame_range(v, n, &first, &last);
+    cudaSetDevice(v->device);
+    // device layout per plane: tw stacks of [tw][2][h][pitch] (one plane at a time)
+    const int W = v->vi.width, H = v->vi.height;
+    const int pitch = round_up(W, 32);
+    const size_t stack_elems = (size_t)tw * 2 * H * pitch;
+    if (!v->st && cudaStreamCreateWithFlags(&v->st, cudaStreamNonBlocking) != cudaSuccess) {
+        set_err(err, errlen, "VAggregate: CUDA initialization failed.");
+        return -1;
+    }
+    if (v->in_elems < stack_elems * tw) {
+        cudaFree(v->d_in);
+        cudaFree(v->d_out);
+        if (v->h_stage) cudaFreeHost(v->h_stage);
+        v->in_elems = stack_elems * tw;
+        v->out_elems = (size_t)H * pitch;
+        if (cudaMalloc(&v->d_in, v->in_elems * 4) != cudaSuccess ||
+            cudaMalloc(&v->d_out, v->out_elems * 4) != cudaSuccess ||
+            cudaHostAlloc((void **)&v->h_stage, (v->in_elems + v->out_elems) * 4, cudaHostAllocDefault) != cudaSuccess) {
+            v->in_elems = 0;
+            set_err(err, errlen, "VAggregate: out of device memory.");
+            return -1;
+        }
+    }
+    for (int p = 0; p < v->vi.num_planes && p < 3; ++p) {
+        if (!v->process[p]) continue;
+        const int w = p == 0 ? W : W >> v->vi.subsampling_w;
+        const int h = p == 0 ? H : H >> v->vi.subsampling_h;
+        const int pp = round_up(w, 32);
+        const size_t se = (size_t)tw * 2 * h * pp;
+        const float *ptrs[kMaxTw];
+        int zs[kMaxTw];
+        for (int i = 0; i < tw; ++i) {
+            const int idx = clampi(n - r + i, 0, nf - 1);
+            const zb3d_frame &fr = stacks[idx - first];
+            copy_plane_in(v->h_stage + i * se, pp, fr.ptr[p], fr.stride[p], w, h * 2 * tw);
+            ptrs[i] = v->d_in + i * se;
+            zs[i] = zb3d_agg_z(i, n, nf, r);
+        }
+        cudaError_t ce = cudaMemcpyAsync(v->d_in, v->h_stage, se * tw * 4, cudaMemcpyHostToDevice, v->st);
+        if (ce == cudaSuccess)
+            ce = launch_vagg(ptrs, zs, tw, w, h, pp, 1, 1u, v->d_out, pp, (long long)h * pp, v->st);
+        float *down = v->h_stage + v->in_elems;
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(down, v->d_out, (size_t)h * pp * 4, cudaMemcpyDeviceToHost, v->st);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(v->st);
+        if (ce != cudaSuccess) {
+            set_err(err, errlen, "VAggregate: process frame failed. (%s)", cudaGetErrorString(ce));
+            return -1;
+        }
+        copy_plane_out(dst->ptr[p], dst->stride[p], down, pp, w, h);
+    }
+    return 0;
+}
+
+void zb3d_vaggregate_free(zb3d_vagg *v) {
+    if (!v) return;
+    cudaSetDevice(v->device);
+    if (v->st) cudaStreamSynchronize(v->st), cudaStreamDestroy(v->st);
+    cudaFree(v->d_in);
+    cudaFree(v->d_out);
+    if (v->h_stage) cudaFreeHost(v->h_stage);
+    delete v;
+}
+
+}  // extern "C"

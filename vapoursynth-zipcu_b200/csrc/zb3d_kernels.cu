@@ -1,0 +1,879 @@
+// zb3d device kernels: block matching, collaborative filtering, aggregation.
+//
+// Compiled for sm_100a with -use_fast_math, the same floating-point mode as the
+// reference kernel (vszipcu src/bm3d.zig:20-24): flush-to-zero, approximate
+// division / square root, FMA contraction.  Where bit-exact agreement with the
+// reference matters (patch distances, transforms, shrinkage) the operation order
+// is the reference's; the distance chains are written with explicit
+// __fmul_rn/__fmaf_rn so the contraction is fixed by the source, not the compiler.
+//
+// Design (B200):
+//  * Matching: one lane owns 4 columns ("half block") of a reference block and
+//    slides a 4x8 candidate window along each candidate row.  With block_step 4,
+//    lane k's half is the first half of block k and the second half of block
+//    k-1, so every column distance is computed once for two blocks.  Candidate
+//    rows of a whole warp-row of blocks are staged in a shared-memory tile and
+//    read as float4 (bank-conflict free, no shuffles in the inner loop except one
+//    to join the two halves).  The top-8 list lives in registers and follows the
+//    reference's insertion rule in scan order, so the lists are bit-identical.
+//  * Filtering: 8 lanes per group, the reference's transform order, FP32.
+//  * Aggregation: signed 64-bit fixed point (2^32 = 1.0) with integer atomics,
+//    which is exact and order independent; the weight sum is accumulated once
+//    per patch at its origin and expanded by an 8x8 box sum in the finish pass.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "zb3d_args.h"
+#include "zb3d_transforms.cuh"
+
+namespace zb {
+
+#define ZB_FLT_MAX 3.402823466e+38f
+#define ZB_FLT_EPS 1.192092896e-07f
+
+static constexpr unsigned kFull = 0xffffffffu;
+
+// ---------------------------------------------------------------------------
+// Top-8 list: sorted by distance; a candidate enters before the first strictly
+// larger entry (vszipcu src/bm3d.cu:641-653), so ties keep scan order.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void top8_insert(float (&e)[8], int (&q)[8], float err, int pos) {
+#pragma unroll
+    for (int i = 7; i > 0; --i) {
+        const bool ci = err < e[i];
+        const bool cp = err < e[i - 1];
+        e[i] = cp ? e[i - 1] : (ci ? err : e[i]);
+        q[i] = cp ? q[i - 1] : (ci ? pos : q[i]);
+    }
+    if (err < e[0]) {
+        e[0] = err;
+        q[0] = pos;
+    }
+}
+
+__device__ __forceinline__ void top8_insert_z(float (&e)[8], int (&q)[8], int (&z)[8], float err, int pos, int zz) {
+#pragma unroll
+    for (int i = 7; i > 0; --i) {
+        const bool ci = err < e[i];
+        const bool cp = err < e[i - 1];
+        e[i] = cp ? e[i - 1] : (ci ? err : e[i]);
+        q[i] = cp ? q[i - 1] : (ci ? pos : q[i]);
+        z[i] = cp ? z[i - 1] : (ci ? zz : z[i]);
+    }
+    if (err < e[0]) {
+        e[0] = err;
+        q[0] = pos;
+        z[0] = zz;
+    }
+}
+
+__device__ __forceinline__ int pack_pos(int x, int y) { return x | (y << 16); }
+__device__ __forceinline__ int pos_x(int p) { return p & 0xffff; }
+__device__ __forceinline__ int pos_y(int p) { return (int)((unsigned)p >> 16); }
+
+// ---------------------------------------------------------------------------
+// Patch distances, per half block (4 columns x 8 rows), vszipcu src/bm3d.cu:282-390.
+// Column j: even rows and odd rows accumulate separately, column = e0 + e1; the
+// 8 columns join as ((s0+s1)+(s2+s3)) + ((s4+s5)+(s6+s7)): each half returns its
+// bracket, the caller adds the two halves.  `st` is the reference patch's
+// statistic (mean for zssd/zsad, norm for ssd/norm); `pm` the lane-pair mask.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float colsum8(const float (&n)[8][4], int j) {
+    return ((n[0][j] + n[1][j]) + (n[2][j] + n[3][j])) + ((n[4][j] + n[5][j]) + (n[6][j] + n[7][j]));
+}
+
+template <int M>
+__device__ __forceinline__ float half_distance(const float (&c)[8][4], const float (&n)[8][4], float st, unsigned pm) {
+    float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if constexpr (M == M_SSD) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float d[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) d[i] = c[i][j] - n[i][j];
+            float e0 = __fmul_rn(d[0], d[0]);
+            float e1 = __fmul_rn(d[1], d[1]);
+            e0 = __fmaf_rn(d[2], d[2], e0);
+            e1 = __fmaf_rn(d[3], d[3], e1);
+            e0 = __fmaf_rn(d[4], d[4], e0);
+            e1 = __fmaf_rn(d[5], d[5], e1);
+            e0 = __fmaf_rn(d[6], d[6], e0);
+            e1 = __fmaf_rn(d[7], d[7], e1);
+            s[j] = e0 + e1;
+        }
+    } else if constexpr (M == M_SAD) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float e0 = 0.0f, e1 = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 8; i += 2) {
+                e0 += fabsf(c[i][j] - n[i][j]);
+                e1 += fabsf(c[i + 1][j] - n[i + 1][j]);
+            }
+            s[j] = e0 + e1;
+        }
+    } else if constexpr (M == M_ZSSD || M == M_ZSAD) {
+        float hsum = (colsum8(n, 0) + colsum8(n, 1)) + (colsum8(n, 2) + colsum8(n, 3));
+        float tot = hsum + __shfl_xor_sync(pm, hsum, 1);
+        const float dm = st - tot * (1.0f / 64.f);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = (c[i][j] - n[i][j]) - dm;
+            if constexpr (M == M_ZSSD) {
+                float e0 = __fmul_rn(v[0], v[0]);
+                float e1 = __fmul_rn(v[1], v[1]);
+                e0 = __fmaf_rn(v[2], v[2], e0);
+                e1 = __fmaf_rn(v[3], v[3], e1);
+                e0 = __fmaf_rn(v[4], v[4], e0);
+                e1 = __fmaf_rn(v[5], v[5], e1);
+                e0 = __fmaf_rn(v[6], v[6], e0);
+                e1 = __fmaf_rn(v[7], v[7], e1);
+                s[j] = e0 + e1;
+            } else {
+                float e0 = 0.0f, e1 = 0.0f;
+#pragma unroll
+                for (int i = 0; i < 8; i += 2) {
+                    e0 += fabsf(v[i]);
+                    e1 += fabsf(v[i + 1]);
+                }
+                s[j] = e0 + e1;
+            }
+        }
+    } else {  // M_SSD_NORM: 2 - 2 <a,b> / (|a| |b| + eps)
+        float q[4], x[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float e0 = __fmul_rn(n[0][j], n[0][j]);
+            float e1 = __fmul_rn(n[1][j], n[1][j]);
+            float f0 = __fmul_rn(c[0][j], n[0][j]);
+            float f1 = __fmul_rn(c[1][j], n[1][j]);
+#pragma unroll
+            for (int i = 2; i < 8; i += 2) {
+                e0 = __fmaf_rn(n[i][j], n[i][j], e0);
+                e1 = __fmaf_rn(n[i + 1][j], n[i + 1][j], e1);
+                f0 = __fmaf_rn(c[i][j], n[i][j], f0);
+                f1 = __fmaf_rn(c[i + 1][j], n[i + 1][j], f1);
+            }
+            q[j] = e0 + e1;
+            x[j] = f0 + f1;
+        }
+        float hq = (q[0] + q[1]) + (q[2] + q[3]);
+        float hx = (x[0] + x[1]) + (x[2] + x[3]);
+        float nn = sqrtf(hq + __shfl_xor_sync(pm, hq, 1));
+        float dot = hx + __shfl_xor_sync(pm, hx, 1);
+        // full distance; the caller's half join is skipped for this metric
+        return 2.0f - 2.0f * dot / __fmaf_rn(st, nn, ZB_FLT_EPS);
+    }
+    return (s[0] + s[1]) + (s[2] + s[3]);
+}
+
+// Joins the two half distances (pair lanes) into the block distance.
+template <int M>
+__device__ __forceinline__ float join_pair(float hd, unsigned pm) {
+    if constexpr (M == M_SSD_NORM) return hd;
+    return hd + __shfl_xor_sync(pm, hd, 1);
+}
+
+// Statistic of the reference patch needed by the mean- or norm-based metrics.
+template <int M>
+__device__ __forceinline__ float ref_stat(const float (&c)[8][4], unsigned pm) {
+    if constexpr (M == M_ZSSD || M == M_ZSAD) {
+        float h = (colsum8(c, 0) + colsum8(c, 1)) + (colsum8(c, 2) + colsum8(c, 3));
+        return (h + __shfl_xor_sync(pm, h, 1)) * (1.0f / 64.f);
+    } else if constexpr (M == M_SSD_NORM) {
+        float q[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float e0 = __fmul_rn(c[0][j], c[0][j]);
+            float e1 = __fmul_rn(c[1][j], c[1][j]);
+#pragma unroll
+            for (int i = 2; i < 8; i += 2) {
+                e0 = __fmaf_rn(c[i][j], c[i][j], e0);
+                e1 = __fmaf_rn(c[i + 1][j], c[i + 1][j], e1);
+            }
+            q[j] = e0 + e1;
+        }
+        float h = (q[0] + q[1]) + (q[2] + q[3]);
+        return sqrtf(h + __shfl_xor_sync(pm, h, 1));
+    }
+    return 0.0f;
+}
+
+// metrics whose column terms can be shared between neighbouring blocks
+template <int M> struct Shareable { static constexpr bool value = (M == M_SSD || M == M_SAD); };
+
+__device__ __forceinline__ float f4c(const float4 &v, int k) {
+    return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
+}
+
+// ---------------------------------------------------------------------------
+// Spatial matching, block_step 4 or 8, from a shared-memory tile.
+// A warp covers one row of reference blocks; lane k's half starts at column
+// x0 + 4k (SHARED: block k = lanes k, k+1) or, in PAIR mode, block b = lanes
+// 2b, 2b+1.  The CTA's warps take consecutive block rows and share the tile.
+// ---------------------------------------------------------------------------
+template <int M, bool SHARED, int BS>
+__global__ void __launch_bounds__(128) zb_match_tiled(MatchArgs a) {
+    extern __shared__ __align__(16) float tile[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    constexpr int NBW = SHARED ? 31 : 16;
+    const int R = a.range, W = a.w, H = a.h, tp = a.tile_pitch;
+    const int kx0 = blockIdx.x * NBW;
+    const int x0 = kx0 * BS;
+    const int by0 = blockIdx.y * nw;
+    const int by_last = min(by0 + nw - 1, a.nby - 1);
+    const int y_first = min(BS * by0, H - 8);
+    const int y_last = min(BS * by_last, H - 8);
+    const int r0 = max(y_first - R, 0);
+    const int nrows = min(y_last + R, H - 8) + 8 - r0;
+    const int c0 = x0 - R;
+    const float *plane = a.frames + (long long)a.radius * a.fstride;
+
+    for (int idx = threadIdx.x; idx < nrows * tp; idx += blockDim.x) {
+        const int r = idx / tp, c = idx - r * tp;
+        const int gx = c0 + c;
+        tile[idx] = (gx >= 0 && gx < W) ? plane[(long long)(r0 + r) * a.pitch + gx] : 0.0f;
+    }
+    __syncthreads();
+
+    const int by = by0 + warp;
+    if (by >= a.nby) return;
+    const int y = min(BS * by, H - 8);
+    const int b = SHARED ? lane : (lane >> 1);
+    const int hh = SHARED ? 0 : (lane & 1);
+    const int kx = kx0 + b;
+    const int xb = BS * kx;
+    const int uo = BS * b + 4 * hh;  // tile column of this half at dx = -R
+    const bool blk = (SHARED ? lane < 31 : true) && kx < a.nbx_al;
+
+    float c[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) c[i][j] = tile[(y - r0 + i) * tp + uo + R + j];
+    const float st = ref_stat<M>(c, kFull);
+
+    float e[8];
+    int q[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        e[i] = ZB_FLT_MAX;
+        q[i] = 0;
+    }
+    const int top = max(y - R, 0), bottom = min(y + R, H - 8);
+    const int lo = -xb, hi = W - 8 - xb;
+    const int chunks = a.chunks;
+
+    for (int row = top; row <= bottom; ++row) {
+        const float *tr = tile + (row - r0) * tp + uo;
+        float4 A[8], B[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) A[i] = *reinterpret_cast<const float4 *>(tr + i * tp);
+        for (int m = 0; m < chunks; ++m) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) B[i] = *reinterpret_cast<const float4 *>(tr + i * tp + 4 * (m + 1));
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const int dx = -R + 4 * m + s;
+                if (dx > R) break;
+                float n[8][4];
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) n[i][j] = (j + s < 4) ? f4c(A[i], j + s) : f4c(B[i], j + s - 4);
+                const float hd = half_distance<M>(c, n, st, kFull);
+                float err;
+                if constexpr (SHARED)
+                    err = hd + __shfl_down_sync(kFull, hd, 1);
+                else
+                    err = join_pair<M>(hd, kFull);
+                if (blk && dx >= lo && dx <= hi && err < e[7]) top8_insert(e, q, err, pack_pos(xb + dx, row));
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) A[i] = B[i];
+        }
+    }
+
+    if (!blk || (!SHARED && hh)) return;
+    const long long bi = (long long)by * a.nbx + kx;
+    const int self = pack_pos(xb, y);
+    if (a.self_incl) {
+        bool found = false;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) found |= (q[i] == self);
+        if (!found) {
+#pragma unroll
+            for (int i = 7; i > 0; --i) {
+                e[i] = e[i - 1];
+                q[i] = q[i - 1];
+            }
+            e[0] = 0.0f;
+            q[0] = self;
+        }
+    }
+    int2 *out = a.list + bi * 8;
+    const int zr = a.radius << 24;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) out[i] = make_int2(pos_x(q[i]), pos_y(q[i]) | zr);
+    if (a.errs) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a.errs[bi * 8 + i] = e[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Scan of one rectangular candidate window from global memory by a lane pair
+// (row-major, the reference's order).  `plane` is already offset by this
+// lane's half (4*hh columns).  A 4-column ring holds the sliding window.
+// ---------------------------------------------------------------------------
+template <int M>
+__device__ __forceinline__ void scan_window(const float *__restrict__ plane, int pitch, int left, int right, int top,
+                                            int bottom, const float (&c)[8][4], float st, unsigned pm,
+                                            float (&e)[8], int (&q)[8]) {
+    for (int row = top; row <= bottom; ++row) {
+        const float *rp = plane + (long long)row * pitch;
+        float w[8][4];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) w[i][j] = __ldg(rp + i * pitch + left + j);
+        for (int col = left; col <= right; col += 4) {
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const int cc = col + s;
+                if (cc > right) break;
+                float n[8][4];
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) n[i][j] = w[i][(s + j) & 3];
+                const float hd = half_distance<M>(c, n, st, pm);
+                const float err = join_pair<M>(hd, pm);
+                if (err < e[7]) top8_insert(e, q, err, pack_pos(cc, row));
+                if (cc + 1 <= right) {
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) w[i][s] = __ldg(rp + i * pitch + cc + 4);
+                }
+            }
+        }
+    }
+}
+
+// Spatial matching for any block_step (and for the clamped last block column of
+// the tiled kernel), reading candidates through the L1/L2 path.  Lane pair per block.
+template <int M>
+__global__ void __launch_bounds__(128) zb_match_global(MatchArgs a) {
+    const int lane = threadIdx.x & 31;
+    const long long pair = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 1;
+    const int hh = lane & 1;
+    const long long nb = a.gen_mode ? a.nby : (long long)a.nby * a.nbx;
+    if (pair >= nb) return;
+    int kx, by;
+    if (a.gen_mode) {
+        kx = a.nbx - 1;
+        by = (int)pair;
+    } else {
+        by = (int)(pair / a.nbx);
+        kx = (int)(pair - (long long)by * a.nbx);
+    }
+    const int W = a.w, H = a.h, R = a.range;
+    const int x = min(a.bs * kx, W - 8), y = min(a.bs * by, H - 8);
+    const unsigned pm = 3u << (lane & 30);
+    const float *plane = a.frames + (long long)a.radius * a.fstride + 4 * hh;
+
+    float c[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) c[i][j] = __ldg(plane + (long long)(y + i) * a.pitch + x + j);
+    const float st = ref_stat<M>(c, pm);
+    float e[8];
+    int q[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        e[i] = ZB_FLT_MAX;
+        q[i] = 0;
+    }
+    scan_window<M>(plane, a.pitch, max(x - R, 0), min(x + R, W - 8), max(y - R, 0), min(y + R, H - 8), c, st, pm, e, q);
+    if (hh) return;
+    const long long bi = (long long)by * a.nbx + kx;
+    const int self = pack_pos(x, y);
+    if (a.self_incl) {
+        bool found = false;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) found |= (q[i] == self);
+        if (!found) {
+#pragma unroll
+            for (int i = 7; i > 0; --i) {
+                e[i] = e[i - 1];
+                q[i] = q[i - 1];
+            }
+            e[0] = 0.0f;
+            q[0] = self;
+        }
+    }
+    const int zr = a.radius << 24;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a.list[bi * 8 + i] = make_int2(pos_x(q[i]), pos_y(q[i]) | zr);
+    if (a.errs) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a.errs[bi * 8 + i] = e[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Temporal predictive search (vszipcu src/bm3d.cu:663-756) and self inclusion
+// (:758-788).  Starts from the spatial list; for direction -1 then +1 and
+// t = 1..r a per-frame list is built from ps_range windows around the first
+// ps_num entries of the previous list (t = 1: the spatial list), and its first
+// ps_num entries are merged into the block's list.
+// ---------------------------------------------------------------------------
+template <int M>
+__global__ void __launch_bounds__(128) zb_match_temporal(MatchArgs a) {
+    const int lane = threadIdx.x & 31;
+    const long long pair = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 1;
+    const int hh = lane & 1;
+    const long long nb = (long long)a.nby * a.nbx;
+    if (pair >= nb) return;
+    const int by = (int)(pair / a.nbx), kx = (int)(pair - (long long)by * a.nbx);
+    const int W = a.w, H = a.h, r = a.radius, P = a.ps_range;
+    const int x = min(a.bs * kx, W - 8), y = min(a.bs * by, H - 8);
+    const unsigned pm = 3u << (lane & 30);
+    const float *centre = a.frames + (long long)r * a.fstride + 4 * hh;
+
+    float c[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) c[i][j] = __ldg(centre + (long long)(y + i) * a.pitch + x + j);
+    const float st = ref_stat<M>(c, pm);
+
+    float ge[8];
+    int gq[8], gz[8], sq[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int2 v = a.list[pair * 8 + i];
+        ge[i] = a.errs[pair * 8 + i];
+        gq[i] = pack_pos(v.x, v.y & 0xffffff);
+        gz[i] = r;
+        sq[i] = gq[i];
+    }
+#pragma unroll 1
+    for (int dir = -1; dir <= 1; dir += 2) {
+        int lq[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) lq[i] = sq[i];
+#pragma unroll 1
+        for (int t = 1; t <= r; ++t) {
+            const int zt = r + dir * t;
+            const float *fp = a.frames + (long long)zt * a.fstride + 4 * hh;
+            float fe[8];
+            int fq[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                fe[i] = ZB_FLT_MAX;
+                fq[i] = 0;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (i < a.ps_num) {
+                    const int xx = pos_x(lq[i]), yy = pos_y(lq[i]);
+                    scan_window<M>(fp, a.pitch, max(xx - P, 0), min(xx + P, W - 8), max(yy - P, 0),
+                                   min(yy + P, H - 8), c, st, pm, fe, fq);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if (i < a.ps_num && fe[i] < ge[7]) top8_insert_z(ge, gq, gz, fe[i], fq[i], zt);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) lq[i] = fq[i];
+        }
+    }
+    if (hh) return;
+    const int self = pack_pos(x, y);
+    bool found = false;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) found |= (gq[i] == self && gz[i] == r);
+    if (!found) {
+#pragma unroll
+        for (int i = 7; i > 0; --i) {
+            gq[i] = gq[i - 1];
+            gz[i] = gz[i - 1];
+        }
+        gq[0] = self;
+        gz[0] = r;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a.list[pair * 8 + i] = make_int2(pos_x(gq[i]), pos_y(gq[i]) | (gz[i] << 24));
+}
+
+// ---------------------------------------------------------------------------
+// Collaborative filtering (vszipcu src/bm3d.cu:392-546) and aggregation.
+// 8 lanes per group, lane j holds column j of every patch (64 values).  The
+// forward 3D transform runs vertical, horizontal (between two transposes), then
+// across the 8 patches; the inverse runs in the reference's order too, so every
+// coefficient and every keep/drop decision equals the reference's.
+// ---------------------------------------------------------------------------
+static constexpr int kFilterWarps = 4;
+static constexpr int kTransStride = 72;  // 8 rows x 9 (padded) floats per group and patch
+
+// 8x8 transpose of each patch inside the lane group, through shared memory.
+// Lane j's value i moves to lane i, value j.  Bank-conflict free: a group is 8
+// consecutive banks at a stride of 8 per group, rows padded to 9.
+__device__ __forceinline__ void group_transpose(float (&d)[64], float *buf, int g, int j, unsigned gm) {
+    __syncwarp(gm);
+#pragma unroll
+    for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) buf[(p * 4 + g) * kTransStride + i * 9 + j] = d[p * 8 + i];
+    __syncwarp(gm);
+#pragma unroll
+    for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) d[p * 8 + i] = buf[(p * 4 + g) * kTransStride + j * 9 + i];
+}
+
+template <class T2, class T1>
+__device__ __forceinline__ void forward3(float (&d)[64], float *buf, int g, int j, unsigned gm) {
+#pragma unroll
+    for (int p = 0; p < 8; ++p) T2::fwd(&d[p * 8]);
+    group_transpose(d, buf, g, j, gm);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) T2::fwd(&d[p * 8]);
+    group_transpose(d, buf, g, j, gm);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+        float t[8];
+#pragma unroll
+        for (int p = 0; p < 8; ++p) t[p] = d[p * 8 + v];
+        T1::fwd(t);
+#pragma unroll
+        for (int p = 0; p < 8; ++p) d[p * 8 + v] = t[p];
+    }
+}
+
+template <class T2, class T1>
+__device__ __forceinline__ void inverse3(float (&d)[64], float *buf, int g, int j, unsigned gm) {
+#pragma unroll
+    for (int p = 0; p < 8; ++p) T2::inv(&d[p * 8]);
+    group_transpose(d, buf, g, j, gm);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) T2::inv(&d[p * 8]);
+    group_transpose(d, buf, g, j, gm);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+        float t[8];
+#pragma unroll
+        for (int p = 0; p < 8; ++p) t[p] = d[p * 8 + v];
+        T1::inv(t);
+#pragma unroll
+        for (int p = 0; p < 8; ++p) d[p * 8 + v] = t[p];
+    }
+}
+
+__device__ __forceinline__ float group_sum(float k, unsigned gm) {
+    k += __shfl_xor_sync(gm, k, 1, 8);
+    k += __shfl_xor_sync(gm, k, 2, 8);
+    k += __shfl_xor_sync(gm, k, 4, 8);
+    return k;
+}
+
+__device__ __forceinline__ unsigned long long to_fix(float v) {
+    return (unsigned long long)__float2ll_rn(v * kFixScale);
+}
+
+template <bool FINAL, int T2D, int T1D>
+__global__ void __launch_bounds__(kFilterWarps * 32) zb_filter(FilterArgs a) {
+    using T2 = typename TransformOf<T2D>::type;
+    using T1 = typename TransformOf<T1D>::type;
+    __shared__ float tbuf[kFilterWarps][8 * 4 * kTransStride];
+    const int lane = threadIdx.x & 31;
+    const int j = lane & 7, g = lane >> 3;
+    const unsigned gm = 0xffu << (lane & 24);
+    const long long grp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+    if (grp >= a.nblocks) return;
+    float *buf = tbuf[threadIdx.x >> 5];
+
+    int px[8], py[8], pz[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int2 v = a.list[grp * 8 + i];
+        px[i] = v.x;
+        py[i] = v.y & 0xffffff;
+        pz[i] = (unsigned)v.y >> 24;
+    }
+    const float E = a.extractor;
+
+    for (int p = 0; p < a.nplanes; ++p) {
+        const float sigma = p == 0 ? a.sigma[0] : (p == 1 ? a.sigma[1] : a.sigma[2]);
+        if (a.chroma && sigma < ZB_FLT_EPS) continue;
+        const float *sp = a.src + (FINAL ? a.clip_stride : 0) + p * a.plane_stride;
+        float d[64];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float *q = sp + pz[i] * a.frame_stride + (long long)py[i] * a.pitch + px[i] + j;
+#pragma unroll
+            for (int r = 0; r < 8; ++r) d[i * 8 + r] = __ldg(q + r * a.pitch);
+        }
+        forward3<T2, T1>(d, buf, g, j, gm);
+        float k = 0.0f;
+        if constexpr (!FINAL) {
+#pragma unroll
+            for (int i = 0; i < 64; ++i) {
+                const float val = d[i];
+                const float thr = (i == 0 && j == 0) ? 0.0f : sigma;
+                const float flag = fabsf(val) >= thr;
+                k += flag;
+                d[i] = flag ? (val * (1.0f / 4096.0f)) : 0.0f;
+            }
+        } else {
+            float rf[64];
+            const float *rp = a.src + p * a.plane_stride;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const float *q = rp + pz[i] * a.frame_stride + (long long)py[i] * a.pitch + px[i] + j;
+#pragma unroll
+                for (int r = 0; r < 8; ++r) rf[i * 8 + r] = __ldg(q + r * a.pitch);
+            }
+            forward3<T2, T1>(rf, buf, g, j, gm);
+            const float s2 = sigma * sigma;
+#pragma unroll
+            for (int i = 0; i < 64; ++i) {
+                float val = d[i];
+                const float rv = rf[i];
+                float coeff = (rv * rv) / __fmaf_rn(rv, rv, s2);
+                if (i == 0) coeff = j ? coeff : 1.0f;
+                val *= coeff;
+                k = __fmaf_rn(coeff, coeff, k);
+                d[i] = val * (1.0f / 4096.0f);
+            }
+        }
+        k = group_sum(k, gm);
+        const float w = 1.0f / k;
+        inverse3<T2, T1>(d, buf, g, j, gm);
+
+        unsigned long long *num = a.num + p * a.acc_plane_stride;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            unsigned long long *q = num + pz[i] * a.acc_frame_stride + (long long)py[i] * a.pitch + px[i] + j;
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const float v = __fmaf_rn(w, d[i * 8 + r], E) - E;
+                atomicAdd(q + r * a.pitch, to_fix(v));
+            }
+        }
+        const float wq = (w + E) - E;
+        // lane j books the weight of patch j once, at its origin
+        int zx = px[0], zy = py[0], zz = pz[0];
+#pragma unroll
+        for (int i = 1; i < 8; ++i)
+            if (i == j) {
+                zx = px[i];
+                zy = py[i];
+                zz = pz[i];
+            }
+        atomicAdd(a.den + p * a.acc_plane_stride + zz * a.acc_frame_stride + (long long)zy * a.pitch + zx, to_fix(wq));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Finish: fixed point -> float.  The weight at a pixel is the 8x8 box sum of the
+// origin weights whose patch covers it.  mode 0 writes num/den (radius 0,
+// src/bm3d.cu:898-922, IEEE division); mode 1 writes the stacked accumulator
+// planes [plane][t][2][h][pitch] of the temporal path (src/bm3d.zig:1224-1231).
+// ---------------------------------------------------------------------------
+struct FinishArgs {
+    const unsigned long long *num, *den;
+    long long acc_plane_stride, acc_frame_stride;
+    int w, h, pitch;
+    int tw;
+    unsigned proc_mask;       // planes written (bit p)
+    float *dst;               // mode 0: [planes][h][dst_pitch]; mode 1: stacked
+    int dst_pitch;
+    long long dst_plane_stride;
+    int mode;
+};
+
+__global__ void __launch_bounds__(256) zb_finish(FinishArgs a) {
+    __shared__ long long t[15][40];
+    __shared__ long long hs[15][32];
+    const int plane = blockIdx.z / a.tw, slot = blockIdx.z - plane * a.tw;
+    if (!((a.proc_mask >> plane) & 1)) return;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
+    const long long base = plane * a.acc_plane_stride + slot * a.acc_frame_stride;
+    const unsigned long long *den = a.den + base;
+    for (int i = threadIdx.y * 32 + threadIdx.x; i < 15 * 39; i += 256) {
+        const int r = i / 39, c = i - r * 39;
+        const int gy = y0 - 7 + r, gx = x0 - 7 + c;
+        t[r][c] = (gy >= 0 && gy < a.h && gx >= 0 && gx < a.w) ? (long long)den[(long long)gy * a.pitch + gx] : 0;
+    }
+    __syncthreads();
+    for (int i = threadIdx.y * 32 + threadIdx.x; i < 15 * 32; i += 256) {
+        const int r = i >> 5, c = i & 31;
+        long long s = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s += t[r][c + k];
+        hs[r][c] = s;
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    if (x >= a.w || y >= a.h) return;
+    long long ds = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) ds += hs[threadIdx.y + k][threadIdx.x];
+    const long long ns = (long long)a.num[base + (long long)y * a.pitch + x];
+    const float nf = __ll2float_rn(ns) * kFixInv;
+    const float df = __ll2float_rn(ds) * kFixInv;
+    if (a.mode == 0) {
+        a.dst[plane * a.dst_plane_stride + (long long)y * a.dst_pitch + x] = __fdiv_rn(nf, df);
+    } else {
+        float *o = a.dst + plane * a.dst_plane_stride + (long long)slot * 2 * a.h * a.dst_pitch;
+        o[(long long)y * a.dst_pitch + x] = nf;
+        o[(long long)(a.h + y) * a.dst_pitch + x] = df;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launchers.
+// ---------------------------------------------------------------------------
+template <int M, bool SHARED, int BS>
+static cudaError_t launch_tiled_t(const MatchArgs &a, int rows_per_cta, cudaStream_t st) {
+    constexpr int NBW = SHARED ? 31 : 16;
+    const int gx = (a.nbx_al + NBW - 1) / NBW;
+    const int gy = (a.nby + rows_per_cta - 1) / rows_per_cta;
+    const int rows = (rows_per_cta - 1) * BS + 2 * a.range + 8;
+    const size_t smem = (size_t)rows * a.tile_pitch * sizeof(float);
+    auto k = zb_match_tiled<M, SHARED, BS>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<dim3(gx, gy), rows_per_cta * 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int M>
+static cudaError_t launch_tiled_m(const MatchArgs &a, int rows_per_cta, cudaStream_t st) {
+    if (a.bs == 8) return launch_tiled_t<M, false, 8>(a, rows_per_cta, st);
+    if constexpr (Shareable<M>::value) return launch_tiled_t<M, true, 4>(a, rows_per_cta, st);
+    return launch_tiled_t<M, false, 4>(a, rows_per_cta, st);
+}
+
+template <int M>
+static cudaError_t launch_global_m(const MatchArgs &a, cudaStream_t st) {
+    const long long nb = a.gen_mode ? a.nby : (long long)a.nby * a.nbx;
+    const long long threads = nb * 2;
+    zb_match_global<M><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int M>
+static cudaError_t launch_temporal_m(const MatchArgs &a, cudaStream_t st) {
+    const long long threads = (long long)a.nby * a.nbx * 2;
+    zb_match_temporal<M><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// Shared-memory bytes the tiled kernel needs for `rows_per_cta` block rows.
+size_t match_tile_bytes(const MatchArgs &a, int rows_per_cta) {
+    return (size_t)((rows_per_cta - 1) * a.bs + 2 * a.range + 8) * a.tile_pitch * sizeof(float);
+}
+
+cudaError_t launch_match(MatchArgs a, int metric, int rows_per_cta, bool use_tiled, cudaStream_t st) {
+    cudaError_t e = cudaSuccess;
+    const bool tiled = use_tiled && (a.bs == 4 || a.bs == 8);
+    a.self_incl = a.radius == 0;
+    if (tiled) {
+        a.chunks = (2 * a.range + 1 + 3) / 4;
+        a.tile_pitch = 128 + 4 * a.chunks;
+        switch (metric) {
+        case M_SSD: e = launch_tiled_m<M_SSD>(a, rows_per_cta, st); break;
+        case M_SAD: e = launch_tiled_m<M_SAD>(a, rows_per_cta, st); break;
+        case M_ZSSD: e = launch_tiled_m<M_ZSSD>(a, rows_per_cta, st); break;
+        case M_ZSAD: e = launch_tiled_m<M_ZSAD>(a, rows_per_cta, st); break;
+        default: e = launch_tiled_m<M_SSD_NORM>(a, rows_per_cta, st); break;
+        }
+        if (e != cudaSuccess) return e;
+        if (a.nbx_al == a.nbx) goto temporal;
+        a.gen_mode = 1;  // clamped last column
+    } else {
+        a.gen_mode = 0;
+    }
+    switch (metric) {
+    case M_SSD: e = launch_global_m<M_SSD>(a, st); break;
+    case M_SAD: e = launch_global_m<M_SAD>(a, st); break;
+    case M_ZSSD: e = launch_global_m<M_ZSSD>(a, st); break;
+    case M_ZSAD: e = launch_global_m<M_ZSAD>(a, st); break;
+    default: e = launch_global_m<M_SSD_NORM>(a, st); break;
+    }
+    if (e != cudaSuccess) return e;
+temporal:
+    if (a.radius > 0) {
+        switch (metric) {
+        case M_SSD: e = launch_temporal_m<M_SSD>(a, st); break;
+        case M_SAD: e = launch_temporal_m<M_SAD>(a, st); break;
+        case M_ZSSD: e = launch_temporal_m<M_ZSSD>(a, st); break;
+        case M_ZSAD: e = launch_temporal_m<M_ZSAD>(a, st); break;
+        default: e = launch_temporal_m<M_SSD_NORM>(a, st); break;
+        }
+    }
+    return e;
+}
+
+template <bool FINAL, int T2D, int T1D>
+static cudaError_t launch_filter_t(const FilterArgs &a, cudaStream_t st) {
+    const long long threads = (long long)a.nblocks * 8;
+    const int tpb = kFilterWarps * 32;
+    zb_filter<FINAL, T2D, T1D><<<(unsigned)((threads + tpb - 1) / tpb), tpb, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <bool FINAL, int T2D>
+static cudaError_t launch_filter_f2(const FilterArgs &a, int t1d, cudaStream_t st) {
+    switch (t1d) {
+    case T_DCT: return launch_filter_t<FINAL, T2D, T_DCT>(a, st);
+    case T_HAAR: return launch_filter_t<FINAL, T2D, T_HAAR>(a, st);
+    case T_WHT: return launch_filter_t<FINAL, T2D, T_WHT>(a, st);
+    default: return launch_filter_t<FINAL, T2D, T_BIOR15>(a, st);
+    }
+}
+
+template <bool FINAL>
+static cudaError_t launch_filter_f(const FilterArgs &a, int t2d, int t1d, cudaStream_t st) {
+    switch (t2d) {
+    case T_DCT: return launch_filter_f2<FINAL, T_DCT>(a, t1d, st);
+    case T_HAAR: return launch_filter_f2<FINAL, T_HAAR>(a, t1d, st);
+    case T_WHT: return launch_filter_f2<FINAL, T_WHT>(a, t1d, st);
+    default: return launch_filter_f2<FINAL, T_BIOR15>(a, t1d, st);
+    }
+}
+
+cudaError_t launch_filter(const FilterArgs &a, bool final_, int t2d, int t1d, cudaStream_t st) {
+    return final_ ? launch_filter_f<true>(a, t2d, t1d, st) : launch_filter_f<false>(a, t2d, t1d, st);
+}
+
+cudaError_t launch_finish(const unsigned long long *num, const unsigned long long *den, long long acc_plane_stride,
+                          long long acc_frame_stride, int w, int h, int pitch, int nplanes, int tw,
+                          unsigned proc_mask, float *dst, int dst_pitch, long long dst_plane_stride, int mode,
+                          cudaStream_t st) {
+    FinishArgs a;
+    a.num = num;
+    a.den = den;
+    a.acc_plane_stride = acc_plane_stride;
+    a.acc_frame_stride = acc_frame_stride;
+    a.w = w;
+    a.h = h;
+    a.pitch = pitch;
+    a.tw = mode == 0 ? 1 : tw;
+    a.proc_mask = proc_mask;
+    a.dst = dst;
+    a.dst_pitch = dst_pitch;
+    a.dst_plane_stride = dst_plane_stride;
+    a.mode = mode;
+    dim3 grid((w + 31) / 32, (h + 7) / 8, nplanes * a.tw);
+    zb_finish<<<grid, dim3(32, 8), 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace zb

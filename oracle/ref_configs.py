@@ -179,6 +179,15 @@ def workload_specs():
     return out
 
 
+def api_specs():
+    """Whole-plane cases of the public-API tests (YUV420 two-pass planes)."""
+    out = []
+    for final in (0, 1):
+        for (w, h) in ((96, 64), (48, 32)):
+            out.append(RefSpec(w=w, h=h, stride=w, sigma=(10.0,) * 3, block_step=4, bm_range=12, final=final))
+    return out
+
+
 def vagg_specs():
     out = []
     for s in parity_specs() + workload_specs():
@@ -189,7 +198,7 @@ def vagg_specs():
 
 def all_specs():
     seen, out = set(), []
-    for s in parity_specs() + workload_specs():
+    for s in parity_specs() + workload_specs() + api_specs():
         if s not in seen:
             seen.add(s)
             out.append(s)

@@ -1,0 +1,145 @@
+"""The public API (zb3d.BM3D / BM3Dv2 / VAggregate on host frames, through the
+C ABI's get_frame) against the reference's own kernels on the same GPU.
+
+* two-pass BM3Dv2 on YUV420 equals, plane by plane, the reference kernel run
+  as basic then final pass (bitwise, deterministic mode);
+* BM3D with radius > 0 emits the reference's stacked accumulators for the
+  clamped window of every frame (src/bm3d.zig:684-699), bitwise;
+* BM3Dv2 radius > 0 equals the reference's vaggregate over those stacks, and
+  the fused and composed forms are byte-identical (README.md:77-79);
+* CBM3D (YUV444, chroma=1); concurrent get_frame calls; frame-range errors.
+"""
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+import pytest
+
+import oracle as orc  # noqa: F401  (keeps the oracle importable in this module's process)
+import ref_configs as rc
+import refh
+import zb3d
+from zb3d import _native as N
+from zb3d import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref_window(spec, src_np, dump=False):
+    from test_ref_pin import _run_ref
+    return _run_ref(spec, src_np, dump=dump)
+
+
+def _need(spec):
+    if not refh.available() or not refh.has_cubin(spec):
+        pytest.skip("reference kernels not built")
+
+
+def _gray_clip(w, h, n, sigma, motion=False):
+    return zb3d.Clip.from_frames([[synth.noisy_plane(w, h, sigma, frame=f, motion=motion)[:, :w]] for f in range(n)])
+
+
+def test_host_path_equals_device_path():
+    from gpu_common import run_product
+    from common import make_src
+    spec = rc.parity_specs()[1]
+    src = make_src(spec)
+    (dev,), _ = run_product(spec, src)
+    clip = zb3d.Clip.from_frames([[src[0, 0, 0, :, :spec.w]]])
+    out = zb3d.BM3D(clip, sigma=10.0, block_step=4, bm_range=12, extractor_exp=3).get_frame(0)[0]
+    assert np.array_equal(out, dev[0])
+
+
+def test_two_pass_yuv420_equals_reference_kernels():
+    w, h, sigma = 96, 64, 10.0
+    frames = [[synth.noisy_plane(w >> (p > 0), h >> (p > 0), sigma, frame=f, plane=p)[:, :w >> (p > 0)]
+               for p in range(3)] for f in range(2)]
+    clip = zb3d.Clip.from_frames(frames, family=N.YUV, subsampling=(1, 1))
+    kw = dict(sigma=[sigma] * 3, block_step=4, bm_range=12, extractor_exp=3)
+    basic = zb3d.BM3Dv2(clip, **kw)
+    final = zb3d.BM3Dv2(clip, ref=basic, **kw)
+    for n in range(2):
+        got_b, got_f = basic.get_frame(n), final.get_frame(n)
+        for p in range(3):
+            pw, ph = w >> (p > 0), h >> (p > 0)
+            sb = rc.RefSpec(w=pw, h=ph, stride=pw, sigma=(sigma,) * 3, block_step=4, bm_range=12)
+            sf = rc.RefSpec(w=pw, h=ph, stride=pw, sigma=(sigma,) * 3, block_step=4, bm_range=12, final=1)
+            _need(sb)
+            _need(sf)
+            noisy = frames[n][p]
+            _, rb, _ = _ref_window(sb, noisy[None, None, None])
+            assert np.array_equal(rb[0], got_b[p]), (n, p)
+            _, rf, _ = _ref_window(sf, np.stack([got_b[p], noisy])[:, None, None])
+            assert np.array_equal(rf[0], got_f[p]), (n, p)
+
+
+@pytest.mark.parametrize("final", [0, 1])
+def test_temporal_stacks_vaggregate_and_fused(final):
+    import torch
+    w, h, r, nf, sigma = 64, 48, 1, 5, 15.0
+    clip = _gray_clip(w, h, nf, sigma, motion=True)
+    ref = _gray_clip(w, h, nf, sigma / 4, motion=True) if final else None
+    kw = dict(sigma=sigma, radius=r, extractor_exp=3)
+    spec = rc.RefSpec(w=w, h=h, stride=w, sigma=(sigma,) * 3, radius=r, final=final)
+    _need(spec)
+    stacked = zb3d.BM3D(clip, ref=ref, **kw)
+    assert stacked.height == h * 2 * (2 * r + 1)
+    # sigma falls back plane to plane, so all three planes count as processed (src/bm3d.zig:1013-1017)
+    assert stacked.get_props(0) == {"BM3D_V_radius": r, "BM3D_V_process": [1, 1, 1]}
+    ref_stacks = {}
+    for n in range(nf):
+        idx = [min(max(n - r + t, 0), nf - 1) for t in range(2 * r + 1)]
+        win = np.stack([clip.get_frame(i)[0] for i in idx])[None, None]
+        if final:
+            win = np.concatenate([np.stack([ref.get_frame(i)[0] for i in idx])[None, None], win])
+        res, _, _ = _ref_window(spec, win)
+        ref_stacks[n] = res[0]
+        got = stacked.get_frame(n)[0].reshape(2 * r + 1, 2, h, w)
+        assert np.array_equal(got, res[0]), n
+    composed = zb3d.BM3Dv2(clip, ref=ref, **kw)
+    fused = zb3d.BM3Dv2(clip, ref=ref, fast_fused=1, **kw)
+    vagg = refh.RefVagg(w, h, w, r, 1)
+    for n in range(nf):
+        a, b = composed.get_frame(n)[0], fused.get_frame(n)[0]
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), n
+        stacks = [torch.from_numpy(ref_stacks[min(max(n - r + i, 0), nf - 1)]).cuda() for i in range(2 * r + 1)]
+        zs = [orc.agg_z(i, n, nf, r) for i in range(2 * r + 1)]
+        dst = torch.zeros((h, w), dtype=torch.float32, device="cuda")
+        vagg.run(dst.data_ptr(), [s.data_ptr() for s in stacks], zs, 1)
+        torch.cuda.synchronize()
+        assert np.array_equal(dst.cpu().numpy(), a), n
+    vagg.close()
+
+
+def test_cbm3d_yuv444_equals_reference():
+    w, h, sig = 48, 40, (8.0, 6.0, 6.0)
+    frames = [[synth.noisy_plane(w, h, 8.0, frame=0, plane=p)[:, :w] for p in range(3)]]
+    clip = zb3d.Clip.from_frames(frames, family=N.YUV)
+    out = zb3d.BM3D(clip, sigma=list(sig), chroma=1, extractor_exp=3).get_frame(0)
+    spec = rc.RefSpec(w=w, h=h, stride=w, sigma=sig, chroma=1, proc_mask=7)
+    _need(spec)
+    _, dst, _ = _ref_window(spec, np.stack(frames[0])[None, :, None])
+    for p in range(3):
+        assert np.array_equal(out[p], dst[p]), p
+
+
+def test_concurrent_get_frame_matches_serial():
+    clip = _gray_clip(80, 64, 8, 10.0)
+    f = zb3d.BM3D(clip, sigma=10.0, block_step=4, num_streams=4, extractor_exp=3)
+    serial = [f.get_frame(n)[0].copy() for n in range(8)]
+    g = zb3d.BM3D(clip, sigma=10.0, block_step=4, num_streams=4, extractor_exp=3)
+    with ThreadPoolExecutor(6) as ex:
+        par = list(ex.map(lambda n: g.get_frame(n)[0], range(8)))
+    for a, b in zip(serial, par):
+        assert np.array_equal(a, b)
+
+
+def test_unprocessed_planes_are_copied_and_errors_raise():
+    w, h = 64, 48
+    frames = [[synth.noisy_plane(w >> (p > 0), h >> (p > 0), 5.0, frame=0, plane=p)[:, :w >> (p > 0)]
+               for p in range(3)]]
+    clip = zb3d.Clip.from_frames(frames, family=N.YUV, subsampling=(1, 1))
+    out = zb3d.BM3Dv2(clip, sigma=[5.0, 0.0]).get_frame(0)
+    assert not np.array_equal(out[0], frames[0][0])
+    assert np.array_equal(out[1], frames[0][1]) and np.array_equal(out[2], frames[0][2])
+    with pytest.raises(zb3d.Error):
+        zb3d.BM3Dv2(clip, sigma=5.0).get_frame(3)

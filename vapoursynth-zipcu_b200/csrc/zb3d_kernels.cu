@@ -639,12 +639,15 @@ __global__ void __launch_bounds__(kFilterWarps * 32) zb_filter(FilterArgs a) {
                 for (int r = 0; r < 8; ++r) rf[i * 8 + r] = __ldg(q + r * a.pitch);
             }
             forward3<T2, T1>(rf, buf, g, j, gm);
+            // coeff = r^2 / (r^2 + sigma^2): the reference rounds r^2 once and adds
+            // sigma^2 (no fused multiply-add in the denominator); k accumulates by FMA
             const float s2 = sigma * sigma;
 #pragma unroll
             for (int i = 0; i < 64; ++i) {
                 float val = d[i];
                 const float rv = rf[i];
-                float coeff = (rv * rv) / __fmaf_rn(rv, rv, s2);
+                const float r2 = __fmul_rn(rv, rv);
+                float coeff = r2 / __fadd_rn(r2, s2);
                 if (i == 0) coeff = j ? coeff : 1.0f;
                 val *= coeff;
                 k = __fmaf_rn(coeff, coeff, k);

@@ -179,6 +179,27 @@ int zb3d_match_device(zb3d_filter *f, int e, const float *d_src, int32_t *d_list
 int zb3d_vaggregate_device(const float *const *stacks, const int *z, int tw, int width, int height, int pitch,
                            int nplanes, unsigned proc_mask, float *d_dst, void *stream);
 
+/*
+ * One BM3D pass (radius 0, ssd matching, dct transforms) over one float plane that
+ * is already in device memory, without allocating any device memory: the scratch
+ * it needs lives in a fixed 24 MiB array inside the library.  No counterpart in
+ * the reference.  It is for callers that cannot call cudaMalloc while they run: a
+ * host that fixes each plugin's device-memory budget at load time, or one that
+ * cannot afford cudaMalloc's implicit device-wide synchronisation mid-frame.
+ *   d_src   [1 or 2][height][pitch] floats: the noisy plane; with final = 1, the
+ *           basic estimate (matched on, Wiener reference) followed by the noisy plane
+ *   d_dst   [height][pitch] denoised output
+ *   sigma   8-bit-scale sigma as in zb3d_args (scaled internally like BM3D)
+ * Limits: height*pitch <= 1048576 and at most 131072 reference blocks; larger
+ * planes are rejected with an error.  The first call on a device looks up the
+ * array's device address (make that first call before any stream capture).
+ * Every call reuses the same array, so calls that overlap on the GPU race.
+ * Returns 0, or -1 with the reason in err.
+ */
+int zb3d_bm3d_plane_noalloc(const float *d_src, float *d_dst, int width, int height, int pitch, int final_,
+                            float sigma, int block_step, int bm_range, int extractor_exp, void *stream, char *err,
+                            size_t errlen);
+
 /* ---- VAggregate -------------------------------------------------------- */
 
 typedef struct zb3d_vagg zb3d_vagg;

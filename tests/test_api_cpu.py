@@ -16,7 +16,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def test_library_exports_every_declared_symbol():
     hdr = open(os.path.join(ROOT, "include", "zb3d.h")).read()
-    names = set(re.findall(r"\b(zb3d_[a-z0-9_]+)\s*\(", hdr))
+    # declarations: a line that starts with a return type, then the function name
+    names = set(re.findall(r"^[a-z][a-z0-9_ ]*[ *]+(zb3d_[a-z0-9_]+)\s*\(", hdr, re.M))
     lib = N.lib()
     for n in sorted(names):
         assert hasattr(lib, n), n

@@ -73,6 +73,8 @@ EXPORTS = {
     "zb3d_profile_enable": (None, [c_void_p, c_int]),
     "zb3d_profile_collect": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(c_int),
                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(c_int)]),
+    "zb3d_bm3d_plane_noalloc": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_float, c_int, c_int,
+                                        c_int, c_void_p, c_char_p, c_size_t]),
     "zb3d_match_device": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_char_p, c_size_t]),
     "zb3d_vaggregate_device": (c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(c_int), c_int, c_int, c_int,
                                        c_int, c_int, ctypes.c_uint, c_void_p, c_void_p]),

@@ -35,6 +35,34 @@ namespace zb {
 static constexpr unsigned kFull = 0xffffffffu;
 
 // ---------------------------------------------------------------------------
+// Global -> shared staging with cp.async: no register round trip, every copy of
+// the CTA in flight at once, one wait.  Columns outside [0, w) are zero-filled
+// (src-size 0; the source address then stays a valid in-plane address).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async_f32(float *sdst, const float *gsrc, bool valid) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(saddr), "l"(gsrc), "r"(valid ? 4 : 0)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// rows [0, nrows) x cols [0, ncols) of the plane window at (gx0, gy0) -> smem rows of pitch sp
+__device__ __forceinline__ void stage_window(float *smem, int sp, const float *plane, long long pitch, int gx0,
+                                             int gy0, int nrows, int ncols, int w) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int r = warp; r < nrows; r += nw) {
+        const float *srow = plane + (long long)(gy0 + r) * pitch;
+        float *drow = smem + r * sp;
+        for (int c = lane; c < ncols; c += 32) {
+            const int gx = gx0 + c;
+            const bool ok = gx >= 0 && gx < w;
+            cp_async_f32(drow + c, srow + (ok ? gx : 0), ok);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Top-8 list: sorted by distance; a candidate enters before the first strictly
 // larger entry (vszipcu src/bm3d.cu:641-653), so ties keep scan order.
 // ---------------------------------------------------------------------------
@@ -213,8 +241,62 @@ __device__ __forceinline__ float f4c(const float4 &v, int k) {
 // Spatial matching, block_step 4 or 8, from a shared-memory tile.
 // A warp covers one row of reference blocks; lane k's half starts at column
 // x0 + 4k (SHARED: block k = lanes k, k+1) or, in PAIR mode, block b = lanes
-// 2b, 2b+1.  The CTA's warps take consecutive block rows and share the tile.
+// 2b, 2b+1.  The CTA's warps take consecutive block rows and share the tile,
+// which is staged with cp.async.  Each candidate row is scanned in chunks of 4
+// displacements; the two float4 window halves alternate roles between chunks so
+// the sliding window never moves between registers.
 // ---------------------------------------------------------------------------
+template <int M, bool SHARED>
+__device__ __forceinline__ void tiled_chunk(const float4 (&X)[8], const float4 (&Y)[8], int m, int R, int row, int xb,
+                                            int lo, int hi, const float (&c)[8][4], float st, float (&e)[8],
+                                            int (&q)[8]) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const int dx = -R + 4 * m + s;
+        if (dx > R) break;
+        float n[8][4];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) n[i][j] = (j + s < 4) ? f4c(X[i], j + s) : f4c(Y[i], j + s - 4);
+        const float hd = half_distance<M>(c, n, st, kFull);
+        float err;
+        if constexpr (SHARED)
+            err = hd + __shfl_down_sync(kFull, hd, 1);
+        else
+            err = join_pair<M>(hd, kFull);
+        if (dx >= lo && dx <= hi && err < e[7]) top8_insert(e, q, err, pack_pos(xb + dx, row));
+    }
+}
+
+// Writes a finished list (with self inclusion at radius 0) and its distances.
+__device__ __forceinline__ void store_list(const MatchArgs &a, long long bi, int xb, int y, float (&e)[8],
+                                           int (&q)[8]) {
+    const int self = pack_pos(xb, y);
+    if (a.self_incl) {
+        bool found = false;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) found |= (q[i] == self);
+        if (!found) {
+#pragma unroll
+            for (int i = 7; i > 0; --i) {
+                e[i] = e[i - 1];
+                q[i] = q[i - 1];
+            }
+            e[0] = 0.0f;
+            q[0] = self;
+        }
+    }
+    int2 *out = a.list + bi * 8;
+    const int zr = a.radius << 24;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) out[i] = make_int2(pos_x(q[i]), pos_y(q[i]) | zr);
+    if (a.errs) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a.errs[bi * 8 + i] = e[i];
+    }
+}
+
 template <int M, bool SHARED, int BS>
 __global__ void __launch_bounds__(128) zb_match_tiled(MatchArgs a) {
     extern __shared__ __align__(16) float tile[];
@@ -229,14 +311,9 @@ __global__ void __launch_bounds__(128) zb_match_tiled(MatchArgs a) {
     const int y_last = min(BS * by_last, H - 8);
     const int r0 = max(y_first - R, 0);
     const int nrows = min(y_last + R, H - 8) + 8 - r0;
-    const int c0 = x0 - R;
     const float *plane = a.frames + (long long)a.radius * a.fstride;
-
-    for (int idx = threadIdx.x; idx < nrows * tp; idx += blockDim.x) {
-        const int r = idx / tp, c = idx - r * tp;
-        const int gx = c0 + c;
-        tile[idx] = (gx >= 0 && gx < W) ? plane[(long long)(r0 + r) * a.pitch + gx] : 0.0f;
-    }
+    stage_window(tile, tp, plane, a.pitch, x0 - R, r0, nrows, tp, W);
+    cp_async_wait_all();
     __syncthreads();
 
     const int by = by0 + warp;
@@ -264,7 +341,8 @@ __global__ void __launch_bounds__(128) zb_match_tiled(MatchArgs a) {
         q[i] = 0;
     }
     const int top = max(y - R, 0), bottom = min(y + R, H - 8);
-    const int lo = -xb, hi = W - 8 - xb;
+    // valid displacements of this block: 0 <= xb + dx <= W - 8 (none for helper lanes)
+    const int lo = blk ? -xb : 1, hi = blk ? W - 8 - xb : 0;
     const int chunks = a.chunks;
 
     for (int row = top; row <= bottom; ++row) {
@@ -272,56 +350,181 @@ __global__ void __launch_bounds__(128) zb_match_tiled(MatchArgs a) {
         float4 A[8], B[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) A[i] = *reinterpret_cast<const float4 *>(tr + i * tp);
-        for (int m = 0; m < chunks; ++m) {
+        for (int m = 0; m < chunks; m += 2) {
 #pragma unroll
             for (int i = 0; i < 8; ++i) B[i] = *reinterpret_cast<const float4 *>(tr + i * tp + 4 * (m + 1));
+            tiled_chunk<M, SHARED>(A, B, m, R, row, xb, lo, hi, c, st, e, q);
+            if (m + 1 < chunks) {
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                const int dx = -R + 4 * m + s;
-                if (dx > R) break;
-                float n[8][4];
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) n[i][j] = (j + s < 4) ? f4c(A[i], j + s) : f4c(B[i], j + s - 4);
-                const float hd = half_distance<M>(c, n, st, kFull);
-                float err;
-                if constexpr (SHARED)
-                    err = hd + __shfl_down_sync(kFull, hd, 1);
-                else
-                    err = join_pair<M>(hd, kFull);
-                if (blk && dx >= lo && dx <= hi && err < e[7]) top8_insert(e, q, err, pack_pos(xb + dx, row));
+                for (int i = 0; i < 8; ++i) A[i] = *reinterpret_cast<const float4 *>(tr + i * tp + 4 * (m + 2));
+                tiled_chunk<M, SHARED>(B, A, m + 1, R, row, xb, lo, hi, c, st, e, q);
             }
-#pragma unroll
-            for (int i = 0; i < 8; ++i) A[i] = B[i];
         }
     }
 
     if (!blk || (!SHARED && hh)) return;
-    const long long bi = (long long)by * a.nbx + kx;
-    const int self = pack_pos(xb, y);
-    if (a.self_incl) {
-        bool found = false;
+    store_list(a, (long long)by * a.nbx + kx, xb, y, e, q);
+}
+
+// ---------------------------------------------------------------------------
+// SSD matching with packed FP32x2 arithmetic (sm_100 FADD2 / FMUL2 / FFMA2).
+// The tile is stored twice with candidate rows interleaved in pairs, once with
+// pairs starting at even tile rows and once at odd ones; a float2 then holds
+// rows (2k, 2k+1) of one column of a window, exactly the operands of the even-
+// and odd-row partial sums, which advance together: acc = fma2(d, d, acc)
+// computes the reference's e0 and e1 chains in one instruction and acc.x + acc.y
+// is their join.  d = n + (-c) = -(c - n) exactly, so d*d is the reference's
+// square.  Pair rows are padded by 4 floats every 32 so the lanes' float4 loads
+// do not collide on banks.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int pair_off(int col) {  // float offset of column `col` in a pair row
+    const int f = 2 * col;
+    return f + (f >> 5) * 4;
+}
+
+__device__ __forceinline__ float2 f4lo(const float4 &v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 f4hi(const float4 &v) { return make_float2(v.z, v.w); }
+
+// window column `col` (0..7 across the two chunk halves) of pair row k
+__device__ __forceinline__ float2 win_col(const float4 (&X)[8], const float4 (&Y)[8], int k, int col) {
+    const float4 &v = col < 4 ? ((col & 2) ? X[2 * k + 1] : X[2 * k]) : ((col & 2) ? Y[2 * k + 1] : Y[2 * k]);
+    return (col & 1) ? f4hi(v) : f4lo(v);
+}
+
+template <bool SHARED>
+__device__ __forceinline__ void tiled2_chunk(const float4 (&X)[8], const float4 (&Y)[8], int m, int R, int row,
+                                             int xb, int lo, int hi, const float2 (&nc)[4][4], float (&e)[8],
+                                             int (&q)[8]) {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) found |= (q[i] == self);
-        if (!found) {
+    for (int s = 0; s < 4; ++s) {
+        const int dx = -R + 4 * m + s;
+        if (dx > R) break;
+        float sj[4];
 #pragma unroll
-            for (int i = 7; i > 0; --i) {
-                e[i] = e[i - 1];
-                q[i] = q[i - 1];
+        for (int j = 0; j < 4; ++j) {
+            float2 d = __fadd2_rn(win_col(X, Y, 0, j + s), nc[0][j]);
+            float2 acc = __fmul2_rn(d, d);
+#pragma unroll
+            for (int k = 1; k < 4; ++k) {
+                d = __fadd2_rn(win_col(X, Y, k, j + s), nc[k][j]);
+                acc = __ffma2_rn(d, d, acc);
             }
-            e[0] = 0.0f;
-            q[0] = self;
+            sj[j] = acc.x + acc.y;
+        }
+        const float hd = (sj[0] + sj[1]) + (sj[2] + sj[3]);
+        float err;
+        if constexpr (SHARED)
+            err = hd + __shfl_down_sync(kFull, hd, 1);
+        else
+            err = hd + __shfl_xor_sync(kFull, hd, 1);
+        if (dx >= lo && dx <= hi && err < e[7]) top8_insert(e, q, err, pack_pos(xb + dx, row));
+    }
+}
+
+template <bool SHARED, int BS>
+__global__ void __launch_bounds__(128) zb_match_tiled2(MatchArgs a) {
+    extern __shared__ __align__(16) float tile[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    constexpr int NBW = SHARED ? 31 : 16;
+    const int R = a.range, W = a.w, H = a.h, tp = a.tile_pitch;
+    const int pp = pair_off(tp) + 4;  // pair-row pitch in floats (multiple of 4)
+    const int kx0 = blockIdx.x * NBW;
+    const int x0 = kx0 * BS;
+    const int by0 = blockIdx.y * nw;
+    const int by_last = min(by0 + nw - 1, a.nby - 1);
+    const int y_first = min(BS * by0, H - 8);
+    const int y_last = min(BS * by_last, H - 8);
+    const int r0 = max(y_first - R, 0);
+    const int nrows = min(y_last + R, H - 8) + 8 - r0;
+    const int npe = (nrows + 1) >> 1;  // even-start pair rows
+    float *tE = tile;
+    float *tO = tile + npe * pp;
+    const float *plane = a.frames + (long long)a.radius * a.fstride;
+    {
+        const int gx0 = x0 - R;
+        for (int t = warp; t < nrows; t += nw) {
+            const float *srow = plane + (long long)(r0 + t) * a.pitch;
+            float *de = tE + (t >> 1) * pp + (t & 1);
+            float *dq = t > 0 ? tO + ((t - 1) >> 1) * pp + ((t - 1) & 1) : nullptr;
+            for (int c = lane; c < tp; c += 32) {
+                const int gx = gx0 + c;
+                const bool ok = gx >= 0 && gx < W;
+                const float *g = srow + (ok ? gx : 0);
+                cp_async_f32(de + pair_off(c), g, ok);
+                if (dq) cp_async_f32(dq + pair_off(c), g, ok);
+            }
         }
     }
-    int2 *out = a.list + bi * 8;
-    const int zr = a.radius << 24;
+    cp_async_wait_all();
+    __syncthreads();
+
+    const int by = by0 + warp;
+    if (by >= a.nby) return;
+    const int y = min(BS * by, H - 8);
+    const int b = SHARED ? lane : (lane >> 1);
+    const int hh = SHARED ? 0 : (lane & 1);
+    const int kx = kx0 + b;
+    const int xb = BS * kx;
+    const int uo = BS * b + 4 * hh;  // tile column of this half at dx = -R (even)
+    const bool blk = (SHARED ? lane < 31 : true) && kx < a.nbx_al;
+
+    // negated reference half as row pairs (2k, 2k+1) of each of its 4 columns
+    float2 nc[4][4];
+    {
+        const int t0 = y - r0;
+        const float *base = (t0 & 1) ? tO + ((t0 - 1) >> 1) * pp : tE + (t0 >> 1) * pp;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) out[i] = make_int2(pos_x(q[i]), pos_y(q[i]) | zr);
-    if (a.errs) {
+        for (int k = 0; k < 4; ++k)
 #pragma unroll
-        for (int i = 0; i < 8; ++i) a.errs[bi * 8 + i] = e[i];
+            for (int j = 0; j < 4; ++j) {
+                const float2 v = *reinterpret_cast<const float2 *>(base + k * pp + pair_off(uo + R + j));
+                nc[k][j] = make_float2(-v.x, -v.y);
+            }
     }
+
+    float e[8];
+    int q[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        e[i] = ZB_FLT_MAX;
+        q[i] = 0;
+    }
+    const int top = max(y - R, 0), bottom = min(y + R, H - 8);
+    const int lo = blk ? -xb : 1, hi = blk ? W - 8 - xb : 0;
+    const int chunks = a.chunks;
+
+    for (int row = top; row <= bottom; ++row) {
+        const int t0 = row - r0;
+        const float *prow = (t0 & 1) ? tO + ((t0 - 1) >> 1) * pp : tE + (t0 >> 1) * pp;
+        // X[2k] = columns (0,1), X[2k+1] = columns (2,3) of pair row k, for the chunk's 4 columns
+        float4 A[8], B[8];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            A[2 * k] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(uo));
+            A[2 * k + 1] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(uo + 2));
+        }
+        for (int m = 0; m < chunks; m += 2) {
+            const int c1 = uo + 4 * (m + 1);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                B[2 * k] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(c1));
+                B[2 * k + 1] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(c1 + 2));
+            }
+            tiled2_chunk<SHARED>(A, B, m, R, row, xb, lo, hi, nc, e, q);
+            if (m + 1 < chunks) {
+                const int c2 = uo + 4 * (m + 2);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    A[2 * k] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(c2));
+                    A[2 * k + 1] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(c2 + 2));
+                }
+                tiled2_chunk<SHARED>(B, A, m + 1, R, row, xb, lo, hi, nc, e, q);
+            }
+        }
+    }
+
+    if (!blk || (!SHARED && hh)) return;
+    store_list(a, (long long)by * a.nbx + kx, xb, y, e, q);
 }
 
 // ---------------------------------------------------------------------------
@@ -742,14 +945,35 @@ __global__ void __launch_bounds__(256) zb_finish(FinishArgs a) {
 // ---------------------------------------------------------------------------
 // Host-side launchers.
 // ---------------------------------------------------------------------------
+size_t match_tile_bytes(const MatchArgs &a, int rows_per_cta);
+
 template <int M, bool SHARED, int BS>
 static cudaError_t launch_tiled_t(const MatchArgs &a, int rows_per_cta, cudaStream_t st) {
     constexpr int NBW = SHARED ? 31 : 16;
     const int gx = (a.nbx_al + NBW - 1) / NBW;
     const int gy = (a.nby + rows_per_cta - 1) / rows_per_cta;
-    const int rows = (rows_per_cta - 1) * BS + 2 * a.range + 8;
-    const size_t smem = (size_t)rows * a.tile_pitch * sizeof(float);
+    const size_t smem = match_tile_bytes(a, rows_per_cta);
     auto k = zb_match_tiled<M, SHARED, BS>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<dim3(gx, gy), rows_per_cta * 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+// packed FP32x2 SSD kernel: two pair-interleaved copies of the tile
+static size_t match_tile2_bytes(const MatchArgs &a, int rows_per_cta) {
+    const int f = 2 * a.tile_pitch;
+    const int pp = f + (f >> 5) * 4 + 4;
+    return (size_t)((rows_per_cta - 1) * a.bs + 2 * a.range + 8) * pp * sizeof(float);
+}
+
+template <bool SHARED, int BS>
+static cudaError_t launch_tiled2_t(const MatchArgs &a, int rows_per_cta, cudaStream_t st) {
+    constexpr int NBW = SHARED ? 31 : 16;
+    const int gx = (a.nbx_al + NBW - 1) / NBW;
+    const int gy = (a.nby + rows_per_cta - 1) / rows_per_cta;
+    const size_t smem = match_tile2_bytes(a, rows_per_cta);
+    auto k = zb_match_tiled2<SHARED, BS>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<dim3(gx, gy), rows_per_cta * 32, smem, st>>>(a);
@@ -758,6 +982,12 @@ static cudaError_t launch_tiled_t(const MatchArgs &a, int rows_per_cta, cudaStre
 
 template <int M>
 static cudaError_t launch_tiled_m(const MatchArgs &a, int rows_per_cta, cudaStream_t st) {
+    if constexpr (M == M_SSD) {
+        // SSD at block_step 4 / 8: the packed FP32x2 kernel whenever its two tiles fit
+        if (match_tile2_bytes(a, rows_per_cta) <= 200 * 1024)
+            return a.bs == 8 ? launch_tiled2_t<false, 8>(a, rows_per_cta, st)
+                             : launch_tiled2_t<true, 4>(a, rows_per_cta, st);
+    }
     if (a.bs == 8) return launch_tiled_t<M, false, 8>(a, rows_per_cta, st);
     if constexpr (Shareable<M>::value) return launch_tiled_t<M, true, 4>(a, rows_per_cta, st);
     return launch_tiled_t<M, false, 4>(a, rows_per_cta, st);

@@ -61,6 +61,11 @@ typedef struct zb3d_args {
     const char *const *transform_1d_s;  int n_transform_1d_s;
     int zero_init;
     int fast_fused;
+    /* Not in the reference.  Block-matching form for ssd: 0 (default) = the FP32
+     * scan of every candidate; 1 = tensor-core distance bound plus exact FP32
+     * re-rank of the candidates under it, where the tile geometry allows it
+     * (block_step 4 with bm_range <= 13, for example).  Both give the same lists. */
+    int match_form;
 } zb3d_args;
 
 /* Fills `a` with "nothing given" (all defaults). */
@@ -169,6 +174,25 @@ int zb3d_profile_collect(zb3d_filter *f, double *match_ms, int *match_launches, 
  */
 int zb3d_match_device(zb3d_filter *f, int e, const float *d_src, int32_t *d_list, void *stream, char *err,
                       size_t errlen);
+
+/*
+ * Counters of the tensor-core matching form, summed over every call since the
+ * last reset: out[0] tiles, out[1] reference blocks, out[2] candidates given the
+ * exact re-rank, out[3] blocks handed to the FP32 scan.  Waits for slot 0's stream.
+ */
+int zb3d_match_stats(zb3d_filter *f, unsigned long long out[4], int reset);
+
+/*
+ * Diagnostic of the tensor-core form on one device plane (ssd, radius 0): writes
+ * the match lists like zb3d_match_device, and the pass-1 distance matrix of
+ * tile (0, 0) to d_dist: [128][zb3d_tc_probe_cols(...)] floats, row m = block
+ * (m mod 8, m / 8) of the tile, column = flat candidate index of the tile's
+ * union; only the rows and columns the kernel reads are written.
+ * Returns 0, 1 when the geometry is outside the tensor-core form, -1 on error.
+ */
+int zb3d_tc_probe_cols(int width, int height, int block_step, int bm_range);
+int zb3d_tc_probe(const float *d_plane, int width, int height, int pitch, int block_step, int bm_range,
+                  int32_t *d_list, float *d_dist, unsigned long long stats[4], char *err, size_t errlen);
 
 /*
  * Temporal aggregation on the device over float accumulator stacks (the

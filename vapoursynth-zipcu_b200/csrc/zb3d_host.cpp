@@ -28,6 +28,8 @@
 namespace zb {
 
 cudaError_t launch_match(MatchArgs a, int metric, int rows_per_cta, bool use_tiled, cudaStream_t st);
+bool tc_eligible(const MatchArgs &a);
+int tc_debug_cols(const MatchArgs &a);
 size_t match_tile_bytes(const MatchArgs &a, int rows_per_cta);
 cudaError_t launch_filter(const FilterArgs &a, bool final_, int t2d, int t1d, cudaStream_t st);
 cudaError_t launch_finish(const unsigned long long *num, const unsigned long long *den, long long acc_plane_stride,
@@ -239,6 +241,8 @@ struct Slot {
     unsigned long long *num = nullptr, *den = nullptr;
     int2 *list = nullptr;
     float *errs = nullptr;
+    int *tc_ws = nullptr;                    // tensor-core form: fallback list
+    unsigned long long *tc_stats = nullptr;  // tensor-core form: counters
     float *h_stage = nullptr;
     size_t stage_up = 0, stage_down = 0;
 
@@ -252,6 +256,8 @@ struct Slot {
         cudaFree(den);
         cudaFree(list);
         cudaFree(errs);
+        cudaFree(tc_ws);
+        cudaFree(tc_stats);
         if (h_stage) cudaFreeHost(h_stage);
         *this = Slot();
     }
@@ -263,6 +269,7 @@ struct Filter {
     zb3d_video_info vi_out{};
     bool v2 = false, passthrough = false;
     bool final_ = false, chroma = false, fused = false, zero_init = true;
+    int match_form = 0;            // 1: tensor-core bound + exact re-rank where eligible
     int radius = 0, tw = 1;
     int nclips = 1;
     float extractor = 0.0f;
@@ -326,6 +333,11 @@ bool alloc_slot(Filter *f, Slot &s) {
     if (!ok(cudaMalloc(&s.den, f->acc_elems * 8))) return false;
     if (!ok(cudaMalloc(&s.list, f->max_blocks * 8 * sizeof(int2)))) return false;
     if (f->radius > 0 && !ok(cudaMalloc(&s.errs, f->max_blocks * 8 * sizeof(float)))) return false;
+    if (f->match_form == 1) {
+        if (!ok(cudaMalloc(&s.tc_ws, (kTcWsList + f->max_blocks) * sizeof(int)))) return false;
+        if (!ok(cudaMalloc(&s.tc_stats, 4 * sizeof(unsigned long long)))) return false;
+        if (!ok(cudaMemset(s.tc_stats, 0, 4 * sizeof(unsigned long long)))) return false;
+    }
     s.stage_up = f->v2 && f->radius > 0 ? f->frame_elems : src;
     s.stage_down = dst;
     if (!ok(cudaHostAlloc((void **)&s.h_stage, (s.stage_up + s.stage_down) * sizeof(float), cudaHostAllocDefault)))
@@ -351,6 +363,8 @@ cudaError_t run_match(Filter *f, Slot &s, const Entry &en, const float *src) {
         ma.nbx_al = en.nbx_al;
         ma.list = s.list;
         ma.errs = f->radius > 0 ? s.errs : nullptr;
+        ma.tc_ws = s.tc_ws;  // null: the plain form
+        ma.tc_stats = s.tc_stats;
         const int rows = 4;
         bool tiled = (en.bs == 4 || en.bs == 8);
         if (tiled) {
@@ -450,7 +464,7 @@ extern "C" {
 void zb3d_args_init(zb3d_args *a) {
     memset(a, 0, sizeof *a);
     a->radius = a->chroma = a->device_id = a->num_streams = a->extractor_exp = ZB3D_UNSET;
-    a->zero_init = a->fast_fused = ZB3D_UNSET;
+    a->zero_init = a->fast_fused = a->match_form = ZB3D_UNSET;
 }
 
 const char *zb3d_version(void) { return "zb3d 0.1.0 (sm_100a)"; }
@@ -565,6 +579,11 @@ static Filter *create_impl(const zb3d_video_info *clip, const zb3d_args *a, int 
         return nullptr;
     }
     f->zero_init = pick(a->zero_init, 1) != 0;
+    f->match_form = pick(a->match_form, 0);
+    if (f->match_form != 0 && f->match_form != 1) {
+        set_err(err, errlen, "BM3D: \"match_form\" must be 0 or 1.");
+        return nullptr;
+    }
     const int extractor_exp = pick(a->extractor_exp, 0);
     f->extractor = extractor_exp != 0 ? std::ldexp(1.0f, extractor_exp) : 0.0f;
 
@@ -893,6 +912,82 @@ int zb3d_match_device(zb3d_filter *fp, int e, const float *d_src, int32_t *d_lis
         ce = cudaMemcpyAsync(d_list, s.list, (size_t)en.nblocks * 8 * sizeof(int2), cudaMemcpyDeviceToDevice, s.st);
     if (ce != cudaSuccess) {
         zb::set_err(err, errlen, "BM3D: matching failed (%s).", cudaGetErrorString(ce));
+        return -1;
+    }
+    return 0;
+}
+
+int zb3d_match_stats(zb3d_filter *fp, unsigned long long out[4], int reset) {
+    Filter *f = reinterpret_cast<Filter *>(fp);
+    for (int i = 0; i < 4; ++i) out[i] = 0;
+    if (f->passthrough || f->match_form != 1) return 0;
+    cudaSetDevice(f->device);
+    for (zb::Slot &s : f->slots) {
+        if (!s.tc_stats) continue;
+        unsigned long long v[4];
+        if (cudaStreamSynchronize(s.st) != cudaSuccess ||
+            cudaMemcpy(v, s.tc_stats, sizeof v, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return -1;
+        for (int i = 0; i < 4; ++i) out[i] += v[i];
+        if (reset && cudaMemset(s.tc_stats, 0, sizeof v) != cudaSuccess) return -1;
+    }
+    return 0;
+}
+
+static zb::MatchArgs probe_args(int width, int height, int pitch, int bs, int range) {
+    zb::MatchArgs a{};
+    a.w = width;
+    a.h = height;
+    a.pitch = pitch;
+    a.bs = bs;
+    a.range = range;
+    a.nbx = (width - 8 + bs - 1) / bs + 1;
+    a.nby = (height - 8 + bs - 1) / bs + 1;
+    a.nbx_al = (width - 8) / bs + 1;
+    a.radius = 0;
+    a.ps_num = 2;
+    a.ps_range = 4;
+    return a;
+}
+
+int zb3d_tc_probe_cols(int width, int height, int block_step, int bm_range) {
+    const zb::MatchArgs a = probe_args(width, height, width, block_step, bm_range);
+    return zb::tc_eligible(a) ? zb::tc_debug_cols(a) : 0;
+}
+
+int zb3d_tc_probe(const float *d_plane, int width, int height, int pitch, int block_step, int bm_range,
+                  int32_t *d_list, float *d_dist, unsigned long long stats[4], char *err, size_t errlen) {
+    using namespace zb;
+    if (width < 8 || height < 8 || block_step < 1 || block_step > 8 || bm_range < 1 || pitch < width) {
+        set_err(err, errlen, "zb3d_tc_probe: bad geometry.");
+        return -1;
+    }
+    MatchArgs a = probe_args(width, height, pitch, block_step, bm_range);
+    if (!tc_eligible(a)) return 1;
+    a.frames = d_plane;
+    a.list = reinterpret_cast<int2 *>(d_list);
+    a.tc_dbg = d_dist;
+    const long long nb = (long long)a.nbx * a.nby;
+    int *ws = nullptr;
+    unsigned long long *st = nullptr;
+    cudaError_t ce = cudaMalloc(&ws, (kTcWsList + nb) * sizeof(int));
+    if (ce == cudaSuccess) ce = cudaMalloc(&st, 4 * sizeof(unsigned long long));
+    if (ce == cudaSuccess) ce = cudaMemset(st, 0, 4 * sizeof(unsigned long long));
+    a.tc_ws = ws;
+    a.tc_stats = st;
+    if (ce == cudaSuccess) ce = launch_match(a, M_SSD, 4, false, nullptr);
+    if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
+    int flag = 0;
+    if (ce == cudaSuccess) ce = cudaMemcpy(stats, st, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    if (ce == cudaSuccess) ce = cudaMemcpy(&flag, ws + 1, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(ws);
+    cudaFree(st);
+    if (ce != cudaSuccess) {
+        set_err(err, errlen, "zb3d_tc_probe: %s.", cudaGetErrorString(ce));
+        return -1;
+    }
+    if (flag) {
+        set_err(err, errlen, "zb3d_tc_probe: an MMA wait timed out (its tiles went to the FP32 scan).");
         return -1;
     }
     return 0;

@@ -25,12 +25,10 @@
 #include <cstdint>
 
 #include "zb3d_args.h"
+#include "zb3d_match.cuh"
 #include "zb3d_transforms.cuh"
 
 namespace zb {
-
-#define ZB_FLT_MAX 3.402823466e+38f
-#define ZB_FLT_EPS 1.192092896e-07f
 
 static constexpr unsigned kFull = 0xffffffffu;
 
@@ -61,44 +59,6 @@ __device__ __forceinline__ void stage_window(float *smem, int sp, const float *p
         }
     }
 }
-
-// ---------------------------------------------------------------------------
-// Top-8 list: sorted by distance; a candidate enters before the first strictly
-// larger entry (vszipcu src/bm3d.cu:641-653), so ties keep scan order.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void top8_insert(float (&e)[8], int (&q)[8], float err, int pos) {
-#pragma unroll
-    for (int i = 7; i > 0; --i) {
-        const bool ci = err < e[i];
-        const bool cp = err < e[i - 1];
-        e[i] = cp ? e[i - 1] : (ci ? err : e[i]);
-        q[i] = cp ? q[i - 1] : (ci ? pos : q[i]);
-    }
-    if (err < e[0]) {
-        e[0] = err;
-        q[0] = pos;
-    }
-}
-
-__device__ __forceinline__ void top8_insert_z(float (&e)[8], int (&q)[8], int (&z)[8], float err, int pos, int zz) {
-#pragma unroll
-    for (int i = 7; i > 0; --i) {
-        const bool ci = err < e[i];
-        const bool cp = err < e[i - 1];
-        e[i] = cp ? e[i - 1] : (ci ? err : e[i]);
-        q[i] = cp ? q[i - 1] : (ci ? pos : q[i]);
-        z[i] = cp ? z[i - 1] : (ci ? zz : z[i]);
-    }
-    if (err < e[0]) {
-        e[0] = err;
-        q[0] = pos;
-        z[0] = zz;
-    }
-}
-
-__device__ __forceinline__ int pack_pos(int x, int y) { return x | (y << 16); }
-__device__ __forceinline__ int pos_x(int p) { return p & 0xffff; }
-__device__ __forceinline__ int pos_y(int p) { return (int)((unsigned)p >> 16); }
 
 // ---------------------------------------------------------------------------
 // Patch distances, per half block (4 columns x 8 rows), vszipcu src/bm3d.cu:282-390.
@@ -266,34 +226,6 @@ __device__ __forceinline__ void tiled_chunk(const float4 (&X)[8], const float4 (
         else
             err = join_pair<M>(hd, kFull);
         if (dx >= lo && dx <= hi && err < e[7]) top8_insert(e, q, err, pack_pos(xb + dx, row));
-    }
-}
-
-// Writes a finished list (with self inclusion at radius 0) and its distances.
-__device__ __forceinline__ void store_list(const MatchArgs &a, long long bi, int xb, int y, float (&e)[8],
-                                           int (&q)[8]) {
-    const int self = pack_pos(xb, y);
-    if (a.self_incl) {
-        bool found = false;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) found |= (q[i] == self);
-        if (!found) {
-#pragma unroll
-            for (int i = 7; i > 0; --i) {
-                e[i] = e[i - 1];
-                q[i] = q[i - 1];
-            }
-            e[0] = 0.0f;
-            q[0] = self;
-        }
-    }
-    int2 *out = a.list + bi * 8;
-    const int zr = a.radius << 24;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) out[i] = make_int2(pos_x(q[i]), pos_y(q[i]) | zr);
-    if (a.errs) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) a.errs[bi * 8 + i] = e[i];
     }
 }
 
@@ -572,10 +504,14 @@ __global__ void __launch_bounds__(128) zb_match_global(MatchArgs a) {
     const int lane = threadIdx.x & 31;
     const long long pair = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 1;
     const int hh = lane & 1;
-    const long long nb = a.gen_mode ? a.nby : (long long)a.nby * a.nbx;
+    const long long nb = a.gen_mode == 2 ? (long long)a.tc_ws[0] : a.gen_mode ? a.nby : (long long)a.nby * a.nbx;
     if (pair >= nb) return;
     int kx, by;
-    if (a.gen_mode) {
+    if (a.gen_mode == 2) {
+        const int bi = a.tc_ws[kTcWsList + pair];
+        by = bi / a.nbx;
+        kx = bi - by * a.nbx;
+    } else if (a.gen_mode) {
         kx = a.nbx - 1;
         by = (int)pair;
     } else {
@@ -995,7 +931,8 @@ static cudaError_t launch_tiled_m(const MatchArgs &a, int rows_per_cta, cudaStre
 
 template <int M>
 static cudaError_t launch_global_m(const MatchArgs &a, cudaStream_t st) {
-    const long long nb = a.gen_mode ? a.nby : (long long)a.nby * a.nbx;
+    // listed blocks (gen_mode 2): the count is on the device, so size for every block
+    const long long nb = a.gen_mode == 1 ? a.nby : (long long)a.nby * a.nbx;
     const long long threads = nb * 2;
     zb_match_global<M><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a);
     return cudaGetLastError();
@@ -1013,10 +950,20 @@ size_t match_tile_bytes(const MatchArgs &a, int rows_per_cta) {
     return (size_t)((rows_per_cta - 1) * a.bs + 2 * a.range + 8) * a.tile_pitch * sizeof(float);
 }
 
+bool tc_eligible(const MatchArgs &a);                          // zb3d_match_tc.cu
+cudaError_t launch_match_tc(const MatchArgs &a, cudaStream_t st);
+
 cudaError_t launch_match(MatchArgs a, int metric, int rows_per_cta, bool use_tiled, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
     const bool tiled = use_tiled && (a.bs == 4 || a.bs == 8);
     a.self_incl = a.radius == 0;
+    if (metric == M_SSD && a.tc_ws != nullptr && tc_eligible(a)) {
+        // tensor-core bound + exact re-rank; the blocks it lists get the FP32 scan
+        if ((e = launch_match_tc(a, st)) != cudaSuccess) return e;
+        a.gen_mode = 2;
+        if ((e = launch_global_m<M_SSD>(a, st)) != cudaSuccess) return e;
+        goto temporal;
+    }
     if (tiled) {
         a.chunks = (2 * a.range + 1 + 3) / 4;
         a.tile_pitch = 128 + 4 * a.chunks;

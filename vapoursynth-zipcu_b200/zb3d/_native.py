@@ -37,7 +37,7 @@ class Args(ctypes.Structure):
         ("bm_error_s", ctypes.POINTER(c_char_p)), ("n_bm_error_s", c_int),
         ("transform_2d_s", ctypes.POINTER(c_char_p)), ("n_transform_2d_s", c_int),
         ("transform_1d_s", ctypes.POINTER(c_char_p)), ("n_transform_1d_s", c_int),
-        ("zero_init", c_int), ("fast_fused", c_int),
+        ("zero_init", c_int), ("fast_fused", c_int), ("match_form", c_int),
     ]
 
 
@@ -76,6 +76,10 @@ EXPORTS = {
     "zb3d_bm3d_plane_noalloc": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_float, c_int, c_int,
                                         c_int, c_void_p, c_char_p, c_size_t]),
     "zb3d_match_device": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_char_p, c_size_t]),
+    "zb3d_match_stats": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_ulonglong), c_int]),
+    "zb3d_tc_probe_cols": (c_int, [c_int, c_int, c_int, c_int]),
+    "zb3d_tc_probe": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
+                              ctypes.POINTER(ctypes.c_ulonglong), c_char_p, c_size_t]),
     "zb3d_vaggregate_device": (c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(c_int), c_int, c_int, c_int,
                                        c_int, c_int, ctypes.c_uint, c_void_p, c_void_p]),
     "zb3d_vaggregate_create": (c_void_p, [ctypes.POINTER(VideoInfo), ctypes.POINTER(VideoInfo),

@@ -2,8 +2,8 @@
 
     python -m zb3d.build        (from vapoursynth-zipcu_b200/)
 
-zb3d_kernels.cu is compiled with -use_fast_math (the reference kernel's
-floating-point mode), zb3d_vagg.cu without it (IEEE sums and division, no
+zb3d_kernels.cu and zb3d_match_tc.cu are compiled with -use_fast_math (the
+reference kernel's floating-point mode), zb3d_vagg.cu without it (IEEE sums and division, no
 flush-to-zero), the host in C++17; nvcc links them into one shared library.
 """
 from __future__ import annotations
@@ -24,11 +24,12 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", f"-I{INCLUDE}
 
 UNITS = [
     ("zb3d_kernels.cu", ARCH + ["-use_fast_math"]),
+    ("zb3d_match_tc.cu", ARCH + ["-use_fast_math"]),
     ("zb3d_vagg.cu", ARCH),
     ("zb3d_host.cpp", ARCH),
     ("zb3d_noalloc.cu", ARCH),
 ]
-HEADERS = ["zb3d_args.h", "zb3d_transforms.cuh"]
+HEADERS = ["zb3d_args.h", "zb3d_match.cuh", "zb3d_transforms.cuh"]
 
 
 def _stale(out, deps):

@@ -48,7 +48,7 @@ class DeviceFilter:
     def _defaults(kw):
         names = ("sigma", "block_step", "bm_range", "radius", "ps_num", "ps_range", "chroma", "device_id",
                  "num_streams", "extractor_exp", "bm_error_s", "transform_2d_s", "transform_1d_s", "zero_init",
-                 "fast_fused")
+                 "fast_fused", "match_form")
         return {n: kw.get(n) for n in names}
 
     def run(self, src_ptr: int, dst_ptr: int, stream: int = 0):
@@ -70,6 +70,13 @@ class DeviceFilter:
         mn, fn = ctypes.c_int(), ctypes.c_int()
         N.lib().zb3d_profile_collect(self.h, ctypes.byref(mm), ctypes.byref(mn), ctypes.byref(fm), ctypes.byref(fn))
         return mm.value, mn.value, fm.value, fn.value
+
+    def match_stats(self, reset: bool = False):
+        """Tensor-core form counters: (tiles, blocks, re-ranked candidates, fallback blocks)."""
+        out = (ctypes.c_ulonglong * 4)()
+        if N.lib().zb3d_match_stats(self.h, out, int(reset)) != 0:
+            raise Error("zb3d_match_stats failed")
+        return tuple(int(v) for v in out)
 
     def match(self, e: int, src_ptr: int, list_ptr: int, stream: int = 0):
         err = N.err_buf()

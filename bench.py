@@ -45,6 +45,9 @@ METRIC = "BM3Dv2 1080p Mpix/s: plain vs BF16+learned-pilot form at ΔPSNR≤0.05
 WORKLOAD = ("plain two-pass BM3Dv2, YUV420PS 1920x1080 / 960x540, sigma [10,10,10], block_step 4, "
             "bm_range 12, radius 0, dct/dct, extractor_exp 3")
 KW = dict(sigma=[SIGMA] * 3, block_step=BLOCK_STEP, bm_range=BM_RANGE, extractor_exp=EXTRACTOR_EXP)
+FORM_KEYS = {0: "fp32_scan", 1: "tensor_core"}
+FORM_NAMES = {0: "plain FP32: every candidate's SSD in the reference's order, match lists bit-exact",
+              1: "tensor-core: tcgen05 FP16 distance bound, exact FP32 re-rank, match lists bit-exact"}
 
 
 def plane_dims():
@@ -469,10 +472,14 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip timing the other block-matching form")
+    ap.add_argument("--match-form", type=int, choices=[0, 1], default=0,
+                    help="block matching: 0 = FP32 scan of every candidate, 1 = tensor-core bound + exact re-rank")
     ap.add_argument("--workload", choices=["twopass1080", "vbm3d", "gray640"], default="twopass1080",
                     help="twopass1080 is the metric's workload; the others print their own line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    KW["match_form"] = args.match_form
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -535,7 +542,7 @@ def main():
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32",
            "data": "synthetic: seeded gradient + 20 rectangles + sinusoidal texture, N(0, 10/255) noise",
-           "config": {"workload": WORKLOAD, "form": "plain FP32, match indices bit-exact with the reference",
+           "config": {"workload": WORKLOAD, "form": None,
                       "frames_per_gpu": FRAMES_PER_GPU, "batch_frames_per_step": BATCH,
                       "l2": f"inputs larger than L2: {FRAMES_PER_GPU} distinct frame buffers "
                             f"({FRAMES_PER_GPU * 2 * 12.4:.0f} MB) cycled",
@@ -552,6 +559,32 @@ def main():
                                        f"{sm_max:.0f} MHz (MEASURED_PEAKS.json has no FP32 figure)",
                         "filter_ms_per_launch": filt_ms / max(filt_n, 1)},
            "clocks": clk}
+    out["config"]["form"] = FORM_NAMES[args.match_form]
+    # the other block-matching form on the same frames: same lists and outputs bit for bit
+    forms = {FORM_KEYS[args.match_form]: {"value": value, "ms_per_step": ms / args.steps,
+                                          "match_ms_per_launch": match_ms / max(match_n, 1)}}
+    if rank == 0 and not args.no_forms:
+        pipe.close()
+        alt = 1 - args.match_form
+        KW["match_form"] = alt
+        p2 = DevicePipeline(torch)
+        p2.upload(frames, FRAMES_PER_GPU)
+        p2.timed(args.warmup)
+        ms2 = p2.timed(args.steps, start_frame=args.warmup * BATCH)
+        p2.profile(True)
+        for j in range(BATCH):
+            p2.run_frame(0, j)
+        torch.cuda.synchronize()
+        p2.profile(False)
+        m2_ms, m2_n, _, _ = p2.collect()
+        p2.close()
+        KW["match_form"] = args.match_form
+        forms[FORM_KEYS[alt]] = {"value": W * H * args.steps * BATCH / (ms2 / 1e3) / 1e6,
+                                 "ms_per_step": ms2 / args.steps, "match_ms_per_launch": m2_ms / max(m2_n, 1)}
+        pipe = None
+    forms["note"] = ("both forms give bit-identical match lists and outputs (delta PSNR 0 dB); "
+                     "tensor_core = tcgen05 FP16 distance bound in TMEM + exact FP32 re-rank")
+    out["forms"] = forms
     if rank == 0 and not args.no_ref_cuda:
         rms = run_ref_cuda(torch, frames, args.steps, args.warmup)
         if rms:
@@ -560,7 +593,8 @@ def main():
                                "what": "the reference's own bm3d.cu kernels (NVRTC-built, -use_fast_math) on "
                                        "this GPU, same frames, same two-pass chaining, device-resident",
                                "speedup_ours": value / world / rv}
-    pipe.close()
+    if pipe is not None:
+        pipe.close()
     if not args.no_e2e:
         dt, h2d, d2h = run_e2e(frames, args.steps, args.warmup)
         out["e2e"] = {"value": W * H * args.steps * BATCH * world / dt / 1e6, "unit": "Mpix/s",

@@ -187,12 +187,17 @@ int zb3d_match_stats(zb3d_filter *f, unsigned long long out[4], int reset);
  * the match lists like zb3d_match_device, and the pass-1 distance matrix of
  * tile (0, 0) to d_dist: [128][zb3d_tc_probe_cols(...)] floats, row m = block
  * (m mod 8, m / 8) of the tile, column = flat candidate index of the tile's
- * union; only the rows and columns the kernel reads are written.
+ * union; only the rows and columns the kernel reads are written.  d_prof (may be
+ * NULL): 16 counters per tile, zeroed by the caller: clock64 at the start, after
+ * the region load, the FP16 copies, the candidate tables, operand A, the MMA
+ * stream with the region reload, the exact errors and at the end (0-7), then the
+ * unsuccessful mbarrier polls of the block, builder and issuer warps (8-10).
  * Returns 0, 1 when the geometry is outside the tensor-core form, -1 on error.
  */
 int zb3d_tc_probe_cols(int width, int height, int block_step, int bm_range);
 int zb3d_tc_probe(const float *d_plane, int width, int height, int pitch, int block_step, int bm_range,
-                  int32_t *d_list, float *d_dist, unsigned long long stats[4], char *err, size_t errlen);
+                  int32_t *d_list, float *d_dist, unsigned long long *d_prof, unsigned long long stats[4], char *err,
+                  size_t errlen);
 
 /*
  * Temporal aggregation on the device over float accumulator stacks (the

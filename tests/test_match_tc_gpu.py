@@ -79,7 +79,7 @@ def _probe(plane, w, h, bs, R):
     st = (ctypes.c_ulonglong * 4)()
     err = N.err_buf()
     rc = N.lib().zb3d_tc_probe(d_plane.data_ptr(), w, h, plane.shape[1], bs, R, d_list.data_ptr(),
-                               d_dist.data_ptr(), st, err, len(err))
+                               d_dist.data_ptr(), None, st, err, len(err))
     assert rc == 0, err.value.decode()
     return d_dist.cpu().numpy(), unpack_list(d_list.cpu().numpy()), tuple(st)
 

@@ -29,6 +29,8 @@ struct MatchArgs {
     int *tc_ws;
     unsigned long long *tc_stats;
     float *tc_dbg;         // optional: pass-1 distances of tile (0, 0), [128][tiles flat candidates]
+    unsigned long long *tc_prof;  // optional: per tile [16]: clock64 phase marks [0..7], mbarrier
+                                  // polls of the block, builder and issuer warps [8..10]
 };
 
 constexpr int kTcWsList = 8;

@@ -956,7 +956,8 @@ int zb3d_tc_probe_cols(int width, int height, int block_step, int bm_range) {
 }
 
 int zb3d_tc_probe(const float *d_plane, int width, int height, int pitch, int block_step, int bm_range,
-                  int32_t *d_list, float *d_dist, unsigned long long stats[4], char *err, size_t errlen) {
+                  int32_t *d_list, float *d_dist, unsigned long long *d_prof, unsigned long long stats[4], char *err,
+                  size_t errlen) {
     using namespace zb;
     if (width < 8 || height < 8 || block_step < 1 || block_step > 8 || bm_range < 1 || pitch < width) {
         set_err(err, errlen, "zb3d_tc_probe: bad geometry.");
@@ -967,6 +968,7 @@ int zb3d_tc_probe(const float *d_plane, int width, int height, int pitch, int bl
     a.frames = d_plane;
     a.list = reinterpret_cast<int2 *>(d_list);
     a.tc_dbg = d_dist;
+    a.tc_prof = d_prof;
     const long long nb = (long long)a.nbx * a.nby;
     int *ws = nullptr;
     unsigned long long *st = nullptr;

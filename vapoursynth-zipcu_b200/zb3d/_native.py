@@ -78,7 +78,7 @@ EXPORTS = {
     "zb3d_match_device": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_char_p, c_size_t]),
     "zb3d_match_stats": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_ulonglong), c_int]),
     "zb3d_tc_probe_cols": (c_int, [c_int, c_int, c_int, c_int]),
-    "zb3d_tc_probe": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
+    "zb3d_tc_probe": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
                               ctypes.POINTER(ctypes.c_ulonglong), c_char_p, c_size_t]),
     "zb3d_vaggregate_device": (c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(c_int), c_int, c_int, c_int,
                                        c_int, c_int, ctypes.c_uint, c_void_p, c_void_p]),

@@ -215,7 +215,7 @@ def run_e2e(frames, steps: int, warmup: int, num_streams: int = 4):
     from zb3d import _native as N
     nfr = BATCH * (steps + warmup)
     host = [frames[i % len(frames)] for i in range(nfr)]
-    clip = zb3d.Clip.from_frames(host, family=N.YUV, subsampling=(1, 1))
+    clip = zb3d.Clip.from_frames(host, family=N.YUV, subsampling=(1, 1), pinned=True)
     basic = zb3d.BM3Dv2(clip, num_streams=num_streams, **KW)
     final = zb3d.BM3Dv2(clip, ref=basic, num_streams=num_streams, **KW)
     pool = ThreadPoolExecutor(num_streams)
@@ -599,7 +599,8 @@ def main():
         dt, h2d, d2h = run_e2e(frames, args.steps, args.warmup)
         out["e2e"] = {"value": W * H * args.steps * BATCH * world / dt / 1e6, "unit": "Mpix/s",
                       "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                      "how": "zb3d.BM3Dv2 twice (basic, then ref=basic) on host numpy frames, 4 request "
+                      "how": "zb3d.BM3Dv2 twice (basic, then ref=basic) on host frames in page-locked memory "
+                             "(the library DMAs them; outputs land in pooled page-locked frames), 4 request "
                              "threads, wall clock"}
     if rank == 0 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(frames)

@@ -248,6 +248,16 @@ void zb3d_vaggregate_free(zb3d_vagg *v);
 /* aggZ of src/bm3d.zig:46-48: the slot of stacked frame clamp(n-r+i) that belongs to frame n. */
 int zb3d_agg_z(int i, int n, int nframes, int radius);
 
+/*
+ * Page-locked host memory for frames, from a pool of reused blocks (not in the
+ * reference, whose frames come from VapourSynth).  zb3d_get_frame copies frames
+ * that live in page-locked memory (this allocator, cudaHostAlloc or
+ * cudaHostRegister) straight to and from the device, without the staging copy
+ * that pageable frames take.  Returns NULL when the allocation fails.
+ */
+void *zb3d_host_alloc(size_t bytes);
+void zb3d_host_free(void *p);
+
 /* Library version string. */
 const char *zb3d_version(void);
 

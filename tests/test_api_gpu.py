@@ -143,3 +143,40 @@ def test_unprocessed_planes_are_copied_and_errors_raise():
     assert np.array_equal(out[1], frames[0][1]) and np.array_equal(out[2], frames[0][2])
     with pytest.raises(zb3d.Error):
         zb3d.BM3Dv2(clip, sigma=5.0).get_frame(3)
+
+
+def test_pinned_and_pageable_frames_take_the_same_path_to_the_same_bytes():
+    """Page-locked caller frames are DMA'd directly (zb3d_get_frame's direct path),
+    pageable ones go through the slot's staging buffer: both give the same bytes,
+    for inputs (clip and ref) and outputs."""
+    import ctypes
+    w, h, sigma = 200, 120, 10.0
+    frames = [[synth.noisy_plane(w >> (p > 0), h >> (p > 0), sigma, frame=f, plane=p)[:, :w >> (p > 0)]
+               for p in range(3)] for f in range(2)]
+    kw = dict(sigma=[sigma] * 3, block_step=4, bm_range=12, extractor_exp=3)
+    outs = []
+    for pinned in (False, True):
+        clip = zb3d.Clip.from_frames(frames, family=N.YUV, subsampling=(1, 1), pinned=pinned)
+        basic = zb3d.BM3Dv2(clip, **kw)
+        final = zb3d.BM3Dv2(clip, ref=basic, **kw)
+        outs.append([[np.array(p) for p in final.get_frame(n)] for n in range(2)])
+    for n in range(2):
+        for p in range(3):
+            assert np.array_equal(outs[0][n][p], outs[1][n][p])
+    # pageable output buffers through the C ABI: the staging download path
+    clip = zb3d.Clip.from_frames(frames, family=N.YUV, subsampling=(1, 1), pinned=True)
+    nf = zb3d._create(1, clip, None, **{k: kw.get(k) for k in ("sigma", "block_step", "bm_range", "extractor_exp")},
+                      radius=None, ps_num=None, ps_range=None, chroma=None, device_id=None, num_streams=None,
+                      bm_error_s=None, transform_2d_s=None, transform_1d_s=None, zero_init=None, fast_fused=None)
+    keep = []
+    cf = (N.Frame * 1)(zb3d._frame_struct(clip.get_frame(0), keep))
+    planes = [np.zeros(np.shape(frames[0][p]), np.float32) for p in range(3)]
+    fo = N.FrameOut()
+    for p, a in enumerate(planes):
+        fo.ptr[p] = a.ctypes.data
+        fo.stride[p] = a.strides[0]
+    err = N.err_buf()
+    assert N.lib().zb3d_get_frame(nf.h, 0, cf, None, ctypes.byref(fo), err, len(err)) == 0, err.value
+    ref = zb3d.BM3Dv2(clip, **kw).get_frame(0)
+    for p in range(3):
+        assert np.array_equal(planes[p], ref[p])

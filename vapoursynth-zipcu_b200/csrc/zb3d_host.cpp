@@ -17,6 +17,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -452,6 +453,29 @@ void copy_plane_out(float *dst, ptrdiff_t stride_bytes, const float *src, int pi
 
 int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+// Page-locked (cudaHostAlloc'd or registered) host memory: copies to and from
+// it are DMA transfers the stream runs asynchronously, with no staging copy.
+bool is_pinned(const void *p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+// Pool of page-locked host blocks for zb3d_host_alloc: freed blocks are kept by
+// size and reused, so steady-state frame allocation costs no cudaHostAlloc.
+struct HostPool {
+    std::mutex mu;
+    std::multimap<size_t, void *> free_blocks;
+    std::map<void *, size_t> sizes;
+};
+HostPool &host_pool() {
+    static HostPool *p = new HostPool();  // never destroyed: frames may outlive static destructors
+    return *p;
+}
+
 }  // namespace
 
 }  // namespace zb
@@ -468,6 +492,36 @@ void zb3d_args_init(zb3d_args *a) {
 }
 
 const char *zb3d_version(void) { return "zb3d 0.1.0 (sm_100a)"; }
+
+void *zb3d_host_alloc(size_t bytes) {
+    zb::HostPool &hp = zb::host_pool();
+    const size_t sz = (bytes + 4095) & ~(size_t)4095;
+    {
+        std::lock_guard<std::mutex> lk(hp.mu);
+        auto it = hp.free_blocks.find(sz);
+        if (it != hp.free_blocks.end()) {
+            void *p = it->second;
+            hp.free_blocks.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, sz, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(hp.mu);
+    hp.sizes[p] = sz;
+    return p;
+}
+
+void zb3d_host_free(void *p) {
+    if (!p) return;
+    zb::HostPool &hp = zb::host_pool();
+    std::lock_guard<std::mutex> lk(hp.mu);
+    auto it = hp.sizes.find(p);
+    if (it != hp.sizes.end()) hp.free_blocks.emplace(it->second, p);
+}
 
 int zb3d_agg_z(int i, int n, int nframes, int radius) {
     return std::min(std::max(2 * radius - i, n - nframes + 1 + radius), n + radius);
@@ -1014,26 +1068,60 @@ static int get_frame_window(Filter *f, int n, const zb3d_frame *clip_frames, con
     const int slot = acquire_slot(f);
     Slot &s = f->slots[slot];
     cudaSetDevice(f->device);
-    // stage the window [clips][planes][t][h][pitch] per entry
-    for (const Entry &e : f->entries) {
-        for (int c = 0; c < f->nclips; ++c) {
-            const zb3d_frame *frames = (f->final_ && c == 0) ? ref_frames : clip_frames;
-            for (int i = 0; i < e.nplanes; ++i)
-                for (int t = 0; t < f->tw; ++t) {
-                    const int idx = clampi(n - f->radius + t, 0, nf - 1);
-                    const zb3d_frame &fr = frames[idx - first];
-                    const int p = e.planes[i];
-                    float *d = s.h_stage + e.src_off + ((size_t)(c * e.nplanes + i) * f->tw + t) * e.plane_elems;
-                    copy_plane_in(d, e.pitch, fr.ptr[p], fr.stride[p], e.w, e.h);
-                }
-        }
+    // the window [clips][planes][t][h][pitch] per entry: page-locked caller frames
+    // are copied to the device directly, anything else goes through the slot's
+    // pinned staging buffer (src/bm3d.zig:295-373)
+    bool direct_in = true;
+    auto each_src = [&](auto fn) {
+        for (const Entry &e : f->entries)
+            for (int c = 0; c < f->nclips; ++c) {
+                const zb3d_frame *frames = (f->final_ && c == 0) ? ref_frames : clip_frames;
+                for (int i = 0; i < e.nplanes; ++i)
+                    for (int t = 0; t < f->tw; ++t) {
+                        const int idx = clampi(n - f->radius + t, 0, nf - 1);
+                        const zb3d_frame &fr = frames[idx - first];
+                        const int p = e.planes[i];
+                        fn(e, e.src_off + ((size_t)(c * e.nplanes + i) * f->tw + t) * e.plane_elems, fr.ptr[p],
+                           fr.stride[p]);
+                    }
+            }
+    };
+    each_src([&](const Entry &, size_t, const float *ptr, ptrdiff_t) { direct_in = direct_in && is_pinned(ptr); });
+    cudaError_t ce = cudaSuccess;
+    if (direct_in) {
+        each_src([&](const Entry &e, size_t off, const float *ptr, ptrdiff_t stride) {
+            if (ce == cudaSuccess)
+                ce = cudaMemcpy2DAsync(s.d_src + off, (size_t)e.pitch * sizeof(float), ptr, (size_t)stride,
+                                       (size_t)e.w * sizeof(float), e.h, cudaMemcpyHostToDevice, s.cst);
+        });
+    } else {
+        each_src([&](const Entry &e, size_t off, const float *ptr, ptrdiff_t stride) {
+            copy_plane_in(s.h_stage + off, e.pitch, ptr, stride, e.w, e.h);
+        });
+        ce = cudaMemcpyAsync(s.d_src, s.h_stage, f->sum_src * sizeof(float), cudaMemcpyHostToDevice, s.cst);
     }
-    cudaError_t ce = cudaMemcpyAsync(s.d_src, s.h_stage, f->sum_src * sizeof(float), cudaMemcpyHostToDevice, s.cst);
     if (ce == cudaSuccess) ce = cudaEventRecord(s.ev_up, s.cst);
     if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s.st, s.ev_up, 0);
     if (ce == cudaSuccess) ce = run_window(f, s, s.d_src, s.d_dst);
+    // page-locked output planes receive the result directly (denoised planes only;
+    // the stacked accumulator layout goes through staging)
+    bool direct_out = !f->stacked_out();
+    for (const Entry &e : f->entries)
+        for (int i = 0; i < e.nplanes; ++i)
+            if ((e.proc_mask >> i) & 1) direct_out = direct_out && is_pinned(dst->ptr[e.planes[i]]);
     float *down = s.h_stage + s.stage_up;
-    if (ce == cudaSuccess) ce = cudaMemcpyAsync(down, s.d_dst, f->sum_dst * sizeof(float), cudaMemcpyDeviceToHost, s.st);
+    if (direct_out) {
+        for (const Entry &e : f->entries)
+            for (int i = 0; i < e.nplanes; ++i) {
+                if (!((e.proc_mask >> i) & 1) || ce != cudaSuccess) continue;
+                const int p = e.planes[i];
+                ce = cudaMemcpy2DAsync(dst->ptr[p], (size_t)dst->stride[p], s.d_dst + e.dst_off + (size_t)i * e.plane_elems,
+                                       (size_t)e.pitch * sizeof(float), (size_t)e.w * sizeof(float), e.h,
+                                       cudaMemcpyDeviceToHost, s.st);
+            }
+    } else if (ce == cudaSuccess) {
+        ce = cudaMemcpyAsync(down, s.d_dst, f->sum_dst * sizeof(float), cudaMemcpyDeviceToHost, s.st);
+    }
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(s.st);
     if (ce != cudaSuccess) {
         cudaStreamSynchronize(s.cst);
@@ -1043,6 +1131,7 @@ static int get_frame_window(Filter *f, int n, const zb3d_frame *clip_frames, con
         return -1;
     }
     for (const Entry &e : f->entries) {
+        if (direct_out) break;
         for (int i = 0; i < e.nplanes; ++i) {
             if (!((e.proc_mask >> i) & 1)) continue;
             const int p = e.planes[i];

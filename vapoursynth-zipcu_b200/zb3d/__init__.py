@@ -23,7 +23,7 @@ import numpy as np
 
 from . import _native as N
 
-__all__ = ["Clip", "Error", "BM3D", "BM3Dv2", "VAggregate", "GRAY", "YUV", "RGB", "version"]
+__all__ = ["Clip", "Error", "BM3D", "BM3Dv2", "VAggregate", "GRAY", "YUV", "RGB", "version", "pinned_empty"]
 
 GRAY, RGB, YUV = N.GRAY, N.RGB, N.YUV
 FLT_EPSILON = np.float32(1.19209290e-7)
@@ -31,6 +31,31 @@ FLT_EPSILON = np.float32(1.19209290e-7)
 
 class Error(Exception):
     """Raised where VapourSynth would raise vs.Error (create-time or frame errors)."""
+
+
+class _PinnedBlock:
+    """A page-locked host block from the library's pool (zb3d_host_alloc), exposed
+    to numpy; returned to the pool when the last array using it goes away."""
+
+    def __init__(self, shape):
+        n = int(np.prod(shape)) * 4
+        self.ptr = N.lib().zb3d_host_alloc(max(n, 4))
+        if not self.ptr:
+            raise MemoryError(f"zb3d_host_alloc({n}) failed")
+        self.__array_interface__ = {"shape": tuple(shape), "typestr": "<f4", "data": (self.ptr, False),
+                                    "version": 3}
+
+    def __del__(self):
+        try:
+            N.lib().zb3d_host_free(self.ptr)
+        except Exception:
+            pass
+
+
+def pinned_empty(shape) -> np.ndarray:
+    """float32 array in page-locked host memory: frames in it reach the device by DMA
+    alone (no staging copy)."""
+    return np.asarray(_PinnedBlock(shape))
 
 
 def version() -> str:
@@ -57,7 +82,22 @@ class Clip:
         self._lock = threading.Lock()
 
     @classmethod
-    def from_frames(cls, frames: Sequence[Sequence[np.ndarray]], family: int = GRAY, subsampling=(0, 0)) -> "Clip":
+    def from_frames(cls, frames: Sequence[Sequence[np.ndarray]], family: int = GRAY, subsampling=(0, 0),
+                    pinned: bool = False) -> "Clip":
+        """A clip over in-memory frames.  With ``pinned`` each plane is copied once into
+        page-locked memory, which the filters then read by DMA."""
+        if pinned:
+            seen: dict = {}
+
+            def pin(p):
+                key = id(p)
+                if key not in seen:
+                    a = pinned_empty(np.shape(p))
+                    a[...] = p
+                    seen[key] = (p, a)
+                return seen[key][1]
+
+            frames = [[pin(p) for p in f] for f in frames]
         frames = [[np.ascontiguousarray(p, dtype=np.float32) for p in f] for f in frames]
         h, w = frames[0][0].shape
         return cls(w, h, len(frames), family, subsampling, frame_fn=lambda n: frames[n], cache=0)
@@ -198,7 +238,7 @@ def _filter_clip(nf: _NativeFilter, clip: Clip, ref: Optional[Clip]) -> Clip:
             h, w = clip.plane_shape(p)
             if stacked:
                 h = h * out.height // clip.height
-            planes.append(np.empty((h, w), np.float32) if (process[p] or stacked)
+            planes.append(pinned_empty((h, w)) if (process[p] or stacked)
                           else np.array(src[p], dtype=np.float32, copy=True))
         fo = N.FrameOut()
         for p, a in enumerate(planes):

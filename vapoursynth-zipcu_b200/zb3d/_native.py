@@ -91,6 +91,8 @@ EXPORTS = {
     "zb3d_vaggregate_free": (None, [c_void_p]),
     "zb3d_agg_z": (c_int, [c_int, c_int, c_int, c_int]),
     "zb3d_version": (c_char_p, []),
+    "zb3d_host_alloc": (c_void_p, [c_size_t]),
+    "zb3d_host_free": (None, [c_void_p]),
 }
 
 _lib = None

@@ -473,13 +473,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other block-matching form")
-    ap.add_argument("--match-form", type=int, choices=[0, 1], default=0,
-                    help="block matching: 0 = FP32 scan of every candidate, 1 = tensor-core bound + exact re-rank")
+    ap.add_argument("--streams", type=int, default=4, help="CUDA streams the device pipeline spreads frames over")
+    ap.add_argument("--match-form", type=int, choices=[-1, 0, 1], default=-1,
+                    help="block matching: -1 = the library's autotuned choice per plane, 0 = FP32 scan of every "
+                         "candidate, 1 = tensor-core bound + exact re-rank")
     ap.add_argument("--workload", choices=["twopass1080", "vbm3d", "gray640"], default="twopass1080",
                     help="twopass1080 is the metric's workload; the others print their own line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    KW["match_form"] = args.match_form
+    if args.match_form >= 0:
+        KW["match_form"] = args.match_form
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -504,7 +507,7 @@ def main():
     from zb3d import _native as N
     N.lib()
     frames = synth_frames(rank, DISTINCT)
-    pipe = DevicePipeline(torch)
+    pipe = DevicePipeline(torch, args.streams)
     pipe.upload(frames, FRAMES_PER_GPU)
     pipe.timed(args.warmup)
     torch.cuda.synchronize()
@@ -559,15 +562,24 @@ def main():
                                        f"{sm_max:.0f} MHz (MEASURED_PEAKS.json has no FP32 figure)",
                         "filter_ms_per_launch": filt_ms / max(filt_n, 1)},
            "clocks": clk}
-    out["config"]["form"] = FORM_NAMES[args.match_form]
-    # the other block-matching form on the same frames: same lists and outputs bit for bit
-    forms = {FORM_KEYS[args.match_form]: {"value": value, "ms_per_step": ms / args.steps,
-                                          "match_ms_per_launch": match_ms / max(match_n, 1)}}
-    if rank == 0 and not args.no_forms:
-        pipe.close()
-        alt = 1 - args.match_form
+    tuned = [pipe.basic[0].tuning(e) for e in range(len(pipe.lay))]
+    chosen = args.match_form if args.match_form >= 0 else tuned[0][0]
+    out["config"]["form"] = FORM_NAMES[chosen] + ("" if args.match_form >= 0 else " (autotuned)")
+    out["config"]["matching_per_plane"] = [{"plane": "YUV"[lay.plane[0]], "form": FORM_KEYS[fm], "rows_per_cta": rw}
+                                           for lay, (fm, rw) in zip(pipe.lay, tuned)]
+    if chosen == 1:
+        out["roofline"]["kernel"] = "zb_match_tc (tensor-core bound + exact FP32 re-rank)"
+    # each block-matching form forced on the same frames: same lists and outputs bit for bit
+    forms = {}
+    if args.match_form >= 0:
+        forms[FORM_KEYS[args.match_form]] = {"value": value, "ms_per_step": ms / args.steps,
+                                             "match_ms_per_launch": match_ms / max(match_n, 1)}
+    for alt in ([] if args.no_forms or rank != 0 else [f for f in (0, 1) if f != args.match_form]):
+        if pipe is not None:
+            pipe.close()
+            pipe = None
         KW["match_form"] = alt
-        p2 = DevicePipeline(torch)
+        p2 = DevicePipeline(torch, args.streams)
         p2.upload(frames, FRAMES_PER_GPU)
         p2.timed(args.warmup)
         ms2 = p2.timed(args.steps, start_frame=args.warmup * BATCH)
@@ -578,10 +590,11 @@ def main():
         p2.profile(False)
         m2_ms, m2_n, _, _ = p2.collect()
         p2.close()
-        KW["match_form"] = args.match_form
         forms[FORM_KEYS[alt]] = {"value": W * H * args.steps * BATCH / (ms2 / 1e3) / 1e6,
                                  "ms_per_step": ms2 / args.steps, "match_ms_per_launch": m2_ms / max(m2_n, 1)}
-        pipe = None
+    KW.pop("match_form", None)
+    if args.match_form >= 0:
+        KW["match_form"] = args.match_form
     forms["note"] = ("both forms give bit-identical match lists and outputs (delta PSNR 0 dB); "
                      "tensor_core = tcgen05 FP16 distance bound in TMEM + exact FP32 re-rank")
     out["forms"] = forms

@@ -61,10 +61,11 @@ typedef struct zb3d_args {
     const char *const *transform_1d_s;  int n_transform_1d_s;
     int zero_init;
     int fast_fused;
-    /* Not in the reference.  Block-matching form for ssd: 0 (default) = the FP32
-     * scan of every candidate; 1 = tensor-core distance bound plus exact FP32
-     * re-rank of the candidates under it, where the tile geometry allows it
-     * (block_step 4 with bm_range <= 13, for example).  Both give the same lists. */
+    /* Not in the reference.  Block-matching form for ssd: 0 = the FP32 scan of
+     * every candidate; 1 = tensor-core distance bound plus exact FP32 re-rank of
+     * the candidates under it, where the tile geometry allows it (block_step 4
+     * with bm_range <= 13, for example); not given = the autotuner picks per plane
+     * (zb3d_entry_tuning).  Every form gives the same lists. */
     int match_form;
 } zb3d_args;
 
@@ -174,6 +175,16 @@ int zb3d_profile_collect(zb3d_filter *f, double *match_ms, int *match_launches, 
  */
 int zb3d_match_device(zb3d_filter *f, int e, const float *d_src, int32_t *d_list, void *stream, char *err,
                       size_t errlen);
+
+/*
+ * The matching configuration the autotuner chose for entry e at creation: form
+ * (0 FP32 scan, 1 tensor-core) and block rows per CTA of the tiled FP32 kernels.
+ * The choice is timed once per GPU and plane geometry and cached in
+ * $ZB3D_TUNE_CACHE (default ~/.cache/zb3d/tune-v1.txt); ZB3D_AUTOTUNE=0 skips the
+ * timing.  It replaces the reference's per-configuration module cache
+ * (src/bm3d.zig:57-70, 780-835).  Returns 0, or -1 for no such entry.
+ */
+int zb3d_entry_tuning(const zb3d_filter *f, int e, int *form, int *rows);
 
 /*
  * Counters of the tensor-core matching form, summed over every call since the

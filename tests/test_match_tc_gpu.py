@@ -195,3 +195,38 @@ def test_tc_out_of_range_tiles_fall_back():
     torch.cuda.synchronize()
     f0.close()
     assert torch.equal(d_list, d_list0)
+
+
+def test_autotuner_picks_a_valid_form_caches_it_and_stays_exact(tmp_path, monkeypatch):
+    import torch
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("ZB3D_TUNE_CACHE", str(cache))
+    w, h = 480, 272
+    plane = synth.noisy_plane(w, h, 10.0, clip=5)
+
+    def lists_for(**kw):
+        f = DeviceFilter(w, h, family=N.GRAY, num_frames=1, sigma=[10.0], block_step=4, bm_range=12,
+                         num_streams=1, **kw)
+        lay = f.entries[0]
+        src = np.zeros(f.src_elems, np.float32)
+        src[lay.src_offset:lay.src_offset + lay.src_elems].reshape(h, lay.pitch)[:, :w] = plane
+        d_src = torch.from_numpy(src).cuda()
+        nbx, nby = (w - 8 + 3) // 4 + 1, (h - 8 + 3) // 4 + 1
+        d_list = torch.zeros((nby, nbx, 8, 2), dtype=torch.int32, device="cuda")
+        f.match(0, d_src.data_ptr(), d_list.data_ptr())
+        torch.cuda.synchronize()
+        t = f.tuning(0)
+        f.close()
+        return d_list.cpu().numpy(), t
+
+    l_auto, (form, rows) = lists_for()
+    assert form in (0, 1) and rows in (2, 4)
+    text = cache.read_text()
+    assert f" {form} {rows}" in text and "_w480_h272_" in text
+    _, again = lists_for()
+    assert again == (form, rows)
+    assert cache.read_text() == text  # served from the cache, not re-timed
+    l0, _ = lists_for(match_form=0)
+    l1, t1 = lists_for(match_form=1)
+    assert t1[0] == 1
+    assert np.array_equal(l_auto, l0) and np.array_equal(l_auto, l1)

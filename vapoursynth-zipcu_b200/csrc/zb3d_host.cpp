@@ -17,6 +17,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <sys/stat.h>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -232,6 +233,8 @@ struct Entry {
     size_t dst_off, dst_elems;     // window output: [planes][h][pitch], stacked [planes][tw][2][h][pitch] if r > 0
     size_t out_off;                // BM3Dv2 temporal frame output [planes][h][pitch]
     size_t frame_off;              // offset inside one cached source frame [clips][entry planes][h][pitch]
+    int form = 0;                  // block matching: 0 FP32 scan, 1 tensor-core bound + exact re-rank
+    int rows = 4;                  // block rows per CTA of the tiled FP32 matchers
 };
 
 // Device scratch of one in-flight frame (the reference's per-stream slot).
@@ -270,7 +273,7 @@ struct Filter {
     zb3d_video_info vi_out{};
     bool v2 = false, passthrough = false;
     bool final_ = false, chroma = false, fused = false, zero_init = true;
-    int match_form = 0;            // 1: tensor-core bound + exact re-rank where eligible
+    int match_form = -1;           // -1: chosen per entry by the autotuner; 0 / 1: forced
     int radius = 0, tw = 1;
     int nclips = 1;
     float extractor = 0.0f;
@@ -334,7 +337,7 @@ bool alloc_slot(Filter *f, Slot &s) {
     if (!ok(cudaMalloc(&s.den, f->acc_elems * 8))) return false;
     if (!ok(cudaMalloc(&s.list, f->max_blocks * 8 * sizeof(int2)))) return false;
     if (f->radius > 0 && !ok(cudaMalloc(&s.errs, f->max_blocks * 8 * sizeof(float)))) return false;
-    if (f->match_form == 1) {
+    if (f->match_form != 0) {
         if (!ok(cudaMalloc(&s.tc_ws, (kTcWsList + f->max_blocks) * sizeof(int)))) return false;
         if (!ok(cudaMalloc(&s.tc_stats, 4 * sizeof(unsigned long long)))) return false;
         if (!ok(cudaMemset(s.tc_stats, 0, 4 * sizeof(unsigned long long)))) return false;
@@ -364,9 +367,9 @@ cudaError_t run_match(Filter *f, Slot &s, const Entry &en, const float *src) {
         ma.nbx_al = en.nbx_al;
         ma.list = s.list;
         ma.errs = f->radius > 0 ? s.errs : nullptr;
-        ma.tc_ws = s.tc_ws;  // null: the plain form
+        ma.tc_ws = en.form == 1 ? s.tc_ws : nullptr;  // null: the FP32 scan
         ma.tc_stats = s.tc_stats;
-        const int rows = 4;
+        const int rows = en.rows;
         bool tiled = (en.bs == 4 || en.bs == 8);
         if (tiled) {
             MatchArgs t = ma;
@@ -375,6 +378,164 @@ cudaError_t run_match(Filter *f, Slot &s, const Entry &en, const float *src) {
             tiled = match_tile_bytes(t, rows) <= 200 * 1024;
         }
         return launch_match(ma, en.metric, rows, tiled, s.st);
+}
+
+// ---- autotuner: per-entry matching configuration -----------------------------
+// Replaces the reference's per-configuration module cache (src/bm3d.zig:57-70,
+// 780-835): kernels here are compiled ahead of time, so what is cached is the
+// fastest launch configuration of the matching stage for a plane geometry,
+// timed on this GPU.  Every candidate gives bit-identical lists, so the choice
+// never changes results.  Cache file: $ZB3D_TUNE_CACHE, else
+// $XDG_CACHE_HOME/zb3d/tune-v1.txt or ~/.cache/zb3d/tune-v1.txt; one line per key
+// "key form rows".  ZB3D_AUTOTUNE=0 turns the timing off (defaults are used).
+struct TuneCache {
+    std::mutex mu;
+    bool loaded = false;
+    std::string path;
+    std::map<std::string, std::pair<int, int>> best;
+};
+
+TuneCache &tune_cache() {
+    static TuneCache *c = new TuneCache();
+    return *c;
+}
+
+std::string tune_path() {
+    const char *p = getenv("ZB3D_TUNE_CACHE");
+    if (p && *p) return p;
+    const char *x = getenv("XDG_CACHE_HOME");
+    if (x && *x) return std::string(x) + "/zb3d/tune-v1.txt";
+    const char *h = getenv("HOME");
+    if (h && *h) return std::string(h) + "/.cache/zb3d/tune-v1.txt";
+    return "";
+}
+
+void tune_load(TuneCache &c) {
+    c.loaded = true;
+    c.path = tune_path();
+    if (c.path.empty()) return;
+    FILE *fp = fopen(c.path.c_str(), "r");
+    if (!fp) return;
+    char key[256];
+    int form, rows;
+    while (fscanf(fp, "%255s %d %d", key, &form, &rows) == 3) c.best[key] = {form, rows};
+    fclose(fp);
+}
+
+void tune_store(TuneCache &c, const std::string &key, int form, int rows) {
+    c.best[key] = {form, rows};
+    if (c.path.empty()) return;
+    const size_t cut = c.path.find_last_of('/');
+    if (cut != std::string::npos) {
+        const std::string dir = c.path.substr(0, cut), parent = dir.substr(0, dir.find_last_of('/'));
+        mkdir(parent.c_str(), 0755);
+        mkdir(dir.c_str(), 0755);
+    }
+    FILE *fp = fopen(c.path.c_str(), "a");
+    if (!fp) return;
+    fprintf(fp, "%s %d %d\n", key.c_str(), form, rows);
+    fclose(fp);
+}
+
+// Chooses e.form / e.rows: FP32 scan with 2 or 4 block rows per CTA (tiled block
+// steps 4 and 8; the kernels take at most 4 warps) or the tensor-core form (ssd,
+// where eligible), by timing
+// each on a synthetic plane of the entry's geometry with slot s's buffers.
+void tune_entry(Filter *f, Slot &s, Entry &e) {
+    e.rows = 4;
+    MatchArgs ga{};
+    ga.w = e.w;
+    ga.h = e.h;
+    ga.bs = e.bs;
+    ga.range = e.range;
+    const bool tc_ok = e.metric == M_SSD && f->match_form != 0 && s.tc_ws != nullptr && tc_eligible(ga);
+    const bool tiled = e.bs == 4 || e.bs == 8;
+    e.form = (f->match_form == 1 && tc_ok) ? 1 : 0;
+    std::vector<std::pair<int, int>> cands;
+    if (f->match_form != 1 || !tc_ok) {
+        if (tiled)
+            for (int r : {2, 4}) cands.push_back({0, r});
+    }
+    if (tc_ok && f->match_form != 0) cands.push_back({1, 4});
+    if (cands.size() < 2) return;
+    const char *off = getenv("ZB3D_AUTOTUNE");
+    if (off && strcmp(off, "0") == 0) return;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, f->device) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    char key[256];
+    snprintf(key, sizeof key, "sm%d%d-%dsm_w%d_h%d_p%d_bs%d_R%d_m%d_r%d_c%d_f%d", prop.major, prop.minor,
+             prop.multiProcessorCount, e.w, e.h, e.pitch, e.bs, e.range, e.metric, f->radius, f->nclips,
+             f->match_form);
+    TuneCache &c = tune_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    if (!c.loaded || tune_path() != c.path) {  // first use, or the cache file was redirected
+        c.best.clear();
+        tune_load(c);
+    }
+    auto it = c.best.find(key);
+    if (it != c.best.end()) {
+        const int form = it->second.first, rows = it->second.second;
+        if ((form == 0 && (rows == 2 || rows == 4)) || (form == 1 && tc_ok)) {
+            e.form = form;
+            e.rows = rows;
+        }
+        return;
+    }
+    // synthetic plane in [0, 1]: gradient, a texture and uniform noise, in every window frame
+    std::vector<float> host((size_t)e.h * e.pitch, 0.0f);
+    unsigned st = 0x9e3779b9u;
+    for (int y = 0; y < e.h; ++y)
+        for (int x = 0; x < e.w; ++x) {
+            st = st * 1664525u + 1013904223u;
+            const float noise = ((st >> 8) * (1.0f / 16777216.0f) - 0.5f) * 0.08f;
+            host[(size_t)y * e.pitch + x] = 0.25f + 0.25f * (x + y) / (float)(e.w + e.h) +
+                                            0.1f * sinf(0.37f * x + 0.21f * y) + noise;
+        }
+    cudaEvent_t a = nullptr, b = nullptr;
+    bool ok = cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess;
+    for (int t = 0; ok && t < f->tw; ++t)
+        ok = cudaMemcpy(s.d_src + e.src_off + (size_t)t * e.plane_elems, host.data(), host.size() * sizeof(float),
+                        cudaMemcpyHostToDevice) == cudaSuccess;
+    float best_ms = 3.0e38f;
+    int bform = -1, brows = e.rows;
+    for (const auto &cand : cands) {
+        if (!ok) break;
+        Entry t = e;
+        t.form = cand.first;
+        t.rows = cand.second;
+        float lo = 3.0e38f;
+        bool good = true;
+        for (int it2 = 0; it2 < 4 && good; ++it2) {
+            good = cudaEventRecord(a, s.st) == cudaSuccess &&
+                   run_match(f, s, t, s.d_src + e.src_off) == cudaSuccess && cudaEventRecord(b, s.st) == cudaSuccess &&
+                   cudaEventSynchronize(b) == cudaSuccess;
+            float ms = 0.0f;
+            if (good && cudaEventElapsedTime(&ms, a, b) == cudaSuccess && it2 > 0) lo = std::min(lo, ms);
+        }
+        if (!good) {  // a configuration that cannot launch here is skipped
+            cudaGetLastError();
+            continue;
+        }
+        if (lo < best_ms) {
+            best_ms = lo;
+            bform = cand.first;
+            brows = cand.second;
+        }
+    }
+    ok = ok && bform >= 0;
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (s.tc_stats) cudaMemset(s.tc_stats, 0, 4 * sizeof(unsigned long long));
+    if (!ok) {
+        cudaGetLastError();
+        return;
+    }
+    e.form = bform;
+    e.rows = brows;
+    tune_store(c, key, bform, brows);
 }
 
 cudaEvent_t prof_event(Filter *f, std::vector<cudaEvent_t> &v, cudaStream_t st) {
@@ -633,8 +794,8 @@ static Filter *create_impl(const zb3d_video_info *clip, const zb3d_args *a, int 
         return nullptr;
     }
     f->zero_init = pick(a->zero_init, 1) != 0;
-    f->match_form = pick(a->match_form, 0);
-    if (f->match_form != 0 && f->match_form != 1) {
+    f->match_form = pick(a->match_form, -1);
+    if (f->match_form != -1 && f->match_form != 0 && f->match_form != 1) {
         set_err(err, errlen, "BM3D: \"match_form\" must be 0 or 1.");
         return nullptr;
     }
@@ -811,6 +972,7 @@ static Filter *create_impl(const zb3d_video_info *clip, const zb3d_args *a, int 
     }
     f->slots.resize(made);
     for (int i = made - 1; i >= 0; --i) f->free_slots.push_back(i);
+    for (Entry &e : f->entries) tune_entry(f.get(), f->slots[0], e);
     if (f->v2 && f->radius > 0) {
         // source frames: one request spans 4r+1 frames; accumulator stacks: 2r+1 centres
         const int span = 4 * f->radius + 1;
@@ -971,10 +1133,18 @@ int zb3d_match_device(zb3d_filter *fp, int e, const float *d_src, int32_t *d_lis
     return 0;
 }
 
+int zb3d_entry_tuning(const zb3d_filter *fp, int e, int *form, int *rows) {
+    const Filter *f = reinterpret_cast<const Filter *>(fp);
+    if (f->passthrough || e < 0 || e >= (int)f->entries.size()) return -1;
+    *form = f->entries[e].form;
+    *rows = f->entries[e].rows;
+    return 0;
+}
+
 int zb3d_match_stats(zb3d_filter *fp, unsigned long long out[4], int reset) {
     Filter *f = reinterpret_cast<Filter *>(fp);
     for (int i = 0; i < 4; ++i) out[i] = 0;
-    if (f->passthrough || f->match_form != 1) return 0;
+    if (f->passthrough) return 0;
     cudaSetDevice(f->device);
     for (zb::Slot &s : f->slots) {
         if (!s.tc_stats) continue;

@@ -77,6 +77,7 @@ EXPORTS = {
                                         c_int, c_void_p, c_char_p, c_size_t]),
     "zb3d_match_device": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_char_p, c_size_t]),
     "zb3d_match_stats": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_ulonglong), c_int]),
+    "zb3d_entry_tuning": (c_int, [c_void_p, c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
     "zb3d_tc_probe_cols": (c_int, [c_int, c_int, c_int, c_int]),
     "zb3d_tc_probe": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
                               ctypes.POINTER(ctypes.c_ulonglong), c_char_p, c_size_t]),

@@ -71,6 +71,13 @@ class DeviceFilter:
         N.lib().zb3d_profile_collect(self.h, ctypes.byref(mm), ctypes.byref(mn), ctypes.byref(fm), ctypes.byref(fn))
         return mm.value, mn.value, fm.value, fn.value
 
+    def tuning(self, e: int = 0):
+        """(form, rows) the autotuner chose for entry e."""
+        form, rows = ctypes.c_int(), ctypes.c_int()
+        if N.lib().zb3d_entry_tuning(self.h, e, ctypes.byref(form), ctypes.byref(rows)) != 0:
+            raise Error("no such entry")
+        return form.value, rows.value
+
     def match_stats(self, reset: bool = False):
         """Tensor-core form counters: (tiles, blocks, re-ranked candidates, fallback blocks)."""
         out = (ctypes.c_ulonglong * 4)()

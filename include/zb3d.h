@@ -269,6 +269,35 @@ int zb3d_agg_z(int i, int n, int nframes, int radius);
 void *zb3d_host_alloc(size_t bytes);
 void zb3d_host_free(void *p);
 
+/* ---- learned pilot (not in the reference) -------------------------------------
+ *
+ * Kernels of the residual conv net that can replace the BM3D step-1 estimate as
+ * step 2's reference (zb3d/pilot.py trains and runs it).  BF16 tensors (void *),
+ * NHWC with channel counts 16 or 48; weights [cout][3][3][cin]; FP32 accumulation.
+ * All calls are asynchronous on `stream` and return 0, or -1 on a launch error.
+ */
+/* y = conv3x3(x) + bias (may be NULL), ReLU if relu, zeroed where mask (NHWC, cout
+ * channels, may be NULL) is <= 0; y (may be NULL) BF16 NHWC; y0 (may be NULL) the
+ * FP32 channel 0 plus resid (may be NULL).  (cin, cout) in {(16,48), (48,48), (48,16)}. */
+int zb3d_pilot_conv3x3(const void *x, int n, int h, int w, int cin, const void *wgt, const float *bias, int cout,
+                       int relu, const void *mask, void *y, float *y0, const float *resid, void *stream);
+/* dw += dL/dw, db += dL/db of one layer from its input x and its pre-activation gradient dy. */
+int zb3d_pilot_conv3x3_wgrad(const void *x, const void *dy, int n, int h, int w, int cin, int cout, float *dw,
+                             float *db, void *stream);
+/* network input: channel 0 = noisy, 1 = sigma[image] / 255 * level_scale, others 0 (16 channels). */
+int zb3d_pilot_pack_input(const float *noisy, const float *sigma, int n, int h, int w, float level_scale, void *x0,
+                          void *stream);
+/* dy (16 channels) = scale * dMSE/dy in channel 0; *loss += sum of squared errors. */
+int zb3d_pilot_mse_grad(const float *y, const float *t, long long count, float scale, void *dy, double *loss,
+                        void *stream);
+/* Adam step (step >= 1) on FP32 weights w with loss-scaled gradient g / gscale; keep (may be NULL)
+ * pins entries to 0 where keep == 0; w16 (may be NULL) receives the BF16 copy. */
+int zb3d_pilot_adam(float *w, float *m, float *v, const float *g, long long count, float lr, float b1, float b2,
+                    float eps, int step, float gscale, const float *keep, void *w16, void *stream);
+/* wt[ci][8 - tap][co] = w[co][tap][ci]: weights of the backward pass to a layer's input. */
+int zb3d_pilot_flip_weights(const void *w, int cin, int cout, void *wt, void *stream);
+int zb3d_pilot_to_bf16(const float *a, long long count, void *b, void *stream);
+
 /* Library version string. */
 const char *zb3d_version(void);
 

@@ -92,6 +92,16 @@ EXPORTS = {
     "zb3d_vaggregate_free": (None, [c_void_p]),
     "zb3d_agg_z": (c_int, [c_int, c_int, c_int, c_int]),
     "zb3d_version": (c_char_p, []),
+    "zb3d_pilot_conv3x3": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_int, c_int,
+                                   c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "zb3d_pilot_conv3x3_wgrad": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p,
+                                         c_void_p, c_void_p]),
+    "zb3d_pilot_pack_input": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_void_p, c_void_p]),
+    "zb3d_pilot_mse_grad": (c_int, [c_void_p, c_void_p, ctypes.c_longlong, c_float, c_void_p, c_void_p, c_void_p]),
+    "zb3d_pilot_adam": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_longlong, c_float, c_float, c_float,
+                                c_float, c_int, c_float, c_void_p, c_void_p, c_void_p]),
+    "zb3d_pilot_flip_weights": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
+    "zb3d_pilot_to_bf16": (c_int, [c_void_p, ctypes.c_longlong, c_void_p, c_void_p]),
     "zb3d_host_alloc": (c_void_p, [c_size_t]),
     "zb3d_host_free": (None, [c_void_p]),
 }

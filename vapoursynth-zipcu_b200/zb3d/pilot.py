@@ -1,0 +1,270 @@
+"""Learned pilot: a residual conv net that stands in for BM3D's step-1 estimate.
+
+BM3Dv2's second pass (Wiener) matches blocks on, and takes its empirical Wiener
+coefficients from, a reference clip: normally the step-1 hard-threshold estimate.
+The pilot produces that reference with 10 layers of 3x3 convolutions (48 channels,
+ReLU, a noise-level input plane; output added to the noisy plane).  It is trained
+only on pairs (noisy synthetic frame, plain BM3D step-1 output of it), on the GPU,
+by the project's own kernels (csrc/zb3d_pilot.cu: BF16 operands, FP32
+accumulation).  Its forward and backward passes are checked against the numpy
+oracle (oracle/pilot_oracle.py).  Step 2 keeps exact block matching; the plain
+two-pass form remains the fallback: `PilotGate` accepts the pilot for a noise level
+only where its two-pass PSNR is within 0.05 dB of the plain two-pass PSNR on
+held-out synthetic frames.
+
+torch provides device memory and streams here; every operation on the data is a
+zb3d kernel.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+from . import synth
+
+SHAPES = [(16, 48)] + [(48, 48)] * 8 + [(48, 16)]  # (cin, cout) of the 10 layers, channels padded to 16
+REAL_IN, REAL_OUT = 2, 1
+LEVEL_SCALE = 4.0                                    # noise-level plane = sigma / 255 * LEVEL_SCALE
+LOSS_SCALE = 1024.0                                  # keeps BF16 gradients clear of underflow
+
+
+def _p(t) -> int:
+    return t.data_ptr() if t is not None else None
+
+
+def _ok(rc: int, what: str):
+    if rc != 0:
+        raise RuntimeError(f"zb3d pilot: {what} failed")
+
+
+class PilotNet:
+    """The network, its FP32 master weights and Adam state, on one CUDA device."""
+
+    def __init__(self, seed: int = 0, device: str = "cuda"):
+        import torch
+        self.torch, self.dev = torch, device
+        rng = np.random.default_rng(seed)
+        self.w32, self.b32, self.keep = [], [], []
+        for l, (cin, cout) in enumerate(SHAPES):
+            rin = REAL_IN if l == 0 else cin
+            rout = REAL_OUT if l == len(SHAPES) - 1 else cout
+            std = math.sqrt(2.0 / (9 * rin)) * (0.1 if l == len(SHAPES) - 1 else 1.0)
+            w = np.zeros((cout, 3, 3, cin), np.float32)
+            w[:rout, :, :, :rin] = rng.normal(0.0, std, size=(rout, 3, 3, rin))
+            k = np.zeros_like(w)
+            k[:rout, :, :, :rin] = 1.0
+            kb = np.zeros(cout, np.float32)
+            kb[:rout] = 1.0
+            self.w32.append(torch.from_numpy(w).to(device))
+            self.b32.append(torch.zeros(cout, dtype=torch.float32, device=device))
+            self.keep.append((torch.from_numpy(k).to(device), torch.from_numpy(kb).to(device)))
+        self.w16 = [torch.empty(w.shape, dtype=torch.bfloat16, device=device) for w in self.w32]
+        self.wt16 = [torch.empty((cin, 3, 3, cout), dtype=torch.bfloat16, device=device) for cin, cout in SHAPES]
+        self.m = [(torch.zeros_like(w), torch.zeros_like(b)) for w, b in zip(self.w32, self.b32)]
+        self.v = [(torch.zeros_like(w), torch.zeros_like(b)) for w, b in zip(self.w32, self.b32)]
+        self.step_count = 0
+        self._refresh()
+
+    # -- weights ---------------------------------------------------------------------
+    def _refresh(self):
+        lib = N.lib()
+        for l, (cin, cout) in enumerate(SHAPES):
+            _ok(lib.zb3d_pilot_to_bf16(_p(self.w32[l]), self.w32[l].numel(), _p(self.w16[l]), None), "to_bf16")
+            _ok(lib.zb3d_pilot_flip_weights(_p(self.w16[l]), cin, cout, _p(self.wt16[l]), None), "flip")
+
+    def state(self) -> dict:
+        out = {}
+        for l in range(len(SHAPES)):
+            out[f"w{l}"] = self.w32[l].cpu().numpy()
+            out[f"b{l}"] = self.b32[l].cpu().numpy()
+        return out
+
+    def load_state(self, st: dict):
+        torch = self.torch
+        for l in range(len(SHAPES)):
+            self.w32[l].copy_(torch.from_numpy(np.asarray(st[f"w{l}"], np.float32)))
+            self.b32[l].copy_(torch.from_numpy(np.asarray(st[f"b{l}"], np.float32)))
+        self._refresh()
+
+    def save(self, path: str):
+        np.savez_compressed(path, **self.state())
+
+    @classmethod
+    def load(cls, path: str, device: str = "cuda") -> "PilotNet":
+        net = cls(device=device)
+        with np.load(path) as f:
+            net.load_state({k: f[k] for k in f.files})
+        return net
+
+    # -- passes ------------------------------------------------------------------------
+    def forward(self, noisy, sigma, keep_acts: bool = False):
+        """noisy: float32 [n][h][w] device tensor, sigma: float32 [n] (8-bit scale).
+        Returns y = noisy + net output (float32 [n][h][w]) and, with keep_acts, the
+        stored BF16 activations of every layer's input."""
+        torch, lib = self.torch, N.lib()
+        n, h, w = noisy.shape
+        x = torch.empty((n, h, w, 16), dtype=torch.bfloat16, device=self.dev)
+        _ok(lib.zb3d_pilot_pack_input(_p(noisy), _p(sigma), n, h, w, LEVEL_SCALE, _p(x), None), "pack_input")
+        acts = [x]
+        y = torch.empty((n, h, w), dtype=torch.float32, device=self.dev)
+        last = len(SHAPES) - 1
+        for l, (cin, cout) in enumerate(SHAPES):
+            if l < last:
+                a = torch.empty((n, h, w, cout), dtype=torch.bfloat16, device=self.dev)
+                _ok(lib.zb3d_pilot_conv3x3(_p(acts[-1]), n, h, w, cin, _p(self.w16[l]), _p(self.b32[l]), cout, 1,
+                                           None, _p(a), None, None, None), f"conv {l}")
+                if keep_acts:
+                    acts.append(a)
+                else:
+                    acts = [a]
+            else:
+                _ok(lib.zb3d_pilot_conv3x3(_p(acts[-1]), n, h, w, cin, _p(self.w16[l]), _p(self.b32[l]), cout, 0,
+                                           None, None, _p(y), _p(noisy), None), "conv out")
+        return y, (acts if keep_acts else None)
+
+    def gradients(self, noisy, target, sigma):
+        """Loss-scaled gradients (dw, db per layer) of mean (y - target)^2, and the loss."""
+        torch, lib = self.torch, N.lib()
+        n, h, w = noisy.shape
+        y, acts = self.forward(noisy, sigma, keep_acts=True)
+        loss = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        d = torch.empty((n, h, w, 16), dtype=torch.bfloat16, device=self.dev)
+        _ok(lib.zb3d_pilot_mse_grad(_p(y), _p(target), y.numel(), LOSS_SCALE, _p(d), _p(loss), None), "mse_grad")
+        dws = [torch.zeros_like(wt) for wt in self.w32]
+        dbs = [torch.zeros_like(b) for b in self.b32]
+        for l in range(len(SHAPES) - 1, -1, -1):
+            cin, cout = SHAPES[l]
+            _ok(lib.zb3d_pilot_conv3x3_wgrad(_p(acts[l]), _p(d), n, h, w, cin, cout, _p(dws[l]), _p(dbs[l]), None),
+                f"wgrad {l}")
+            if l == 0:
+                break
+            dx = torch.empty((n, h, w, cin), dtype=torch.bfloat16, device=self.dev)
+            # backward pass to the layer input (= previous layer's output): conv with the flipped
+            # weights, ReLU derivative from the stored activation
+            _ok(lib.zb3d_pilot_conv3x3(_p(d), n, h, w, cout, _p(self.wt16[l]), None, cin, 0, _p(acts[l]), _p(dx),
+                                       None, None, None), f"dgrad {l}")
+            d = dx
+        return dws, dbs, float(loss.item()) / y.numel(), y
+
+    def train_step(self, noisy, target, sigma, lr: float = 1e-3) -> float:
+        lib = N.lib()
+        dws, dbs, loss, _ = self.gradients(noisy, target, sigma)
+        self.step_count += 1
+        for l in range(len(SHAPES)):
+            for p, g, m, v, k, w16 in ((self.w32[l], dws[l], self.m[l][0], self.v[l][0], self.keep[l][0], self.w16[l]),
+                                       (self.b32[l], dbs[l], self.m[l][1], self.v[l][1], self.keep[l][1], None)):
+                _ok(lib.zb3d_pilot_adam(_p(p), _p(m), _p(v), _p(g), p.numel(), lr, 0.9, 0.999, 1e-8,
+                                        self.step_count, LOSS_SCALE, _p(k), _p(w16), None), "adam")
+        for l, (cin, cout) in enumerate(SHAPES):
+            _ok(lib.zb3d_pilot_flip_weights(_p(self.w16[l]), cin, cout, _p(self.wt16[l]), None), "flip")
+        return loss
+
+    def denoise(self, plane: np.ndarray, sigma: float) -> np.ndarray:
+        """The pilot estimate of one float32 plane (host in, host out)."""
+        torch = self.torch
+        x = torch.from_numpy(np.ascontiguousarray(plane, np.float32))[None].to(self.dev)
+        s = torch.tensor([sigma], dtype=torch.float32, device=self.dev)
+        y, _ = self.forward(x, s)
+        return y[0].cpu().numpy()
+
+
+# ---------------------------------------------------------------------------------------
+# training data: (noisy synthetic frame, plain BM3D step-1 estimate) pairs
+# ---------------------------------------------------------------------------------------
+def step1_estimates(noisy: Sequence[np.ndarray], sigma: float, **bm3d_kw) -> list:
+    """Plain BM3D step 1 (hard threshold, the reference's defaults unless given) of each plane."""
+    import zb3d
+    h, w = noisy[0].shape
+    clip = zb3d.Clip.from_frames([[p] for p in noisy])
+    basic = zb3d.BM3D(clip, sigma=sigma, **bm3d_kw)
+    return [np.array(basic.get_frame(i)[0]) for i in range(len(noisy))]
+
+
+def make_pairs(count: int, size: int, sigmas: Sequence[float], seed: int = 1, clip0: int = 1000, **bm3d_kw):
+    """`count` frames of size x size per sigma: (noisy, step-1, clean, sigma) lists."""
+    noisy, target, clean, sig = [], [], [], []
+    for si, s in enumerate(sigmas):
+        fr = [synth.noisy_plane(size, size, s, clip=clip0 + seed * 100 + si, frame=f) for f in range(count)]
+        cl = [synth.clean_plane(size, size, clip0 + seed * 100 + si, f) for f in range(count)]
+        noisy += fr
+        clean += cl
+        target += step1_estimates(fr, s, **bm3d_kw)
+        sig += [float(s)] * count
+    return noisy, target, clean, sig
+
+
+def train(net: PilotNet, noisy, target, sigma, steps: int, batch: int = 32, crop: int = 64, lr: float = 1e-3,
+          seed: int = 0, log_every: int = 0) -> list:
+    """Adam on random crop x crop patches of the pairs; returns the loss history."""
+    torch = net.torch
+    rng = np.random.default_rng(seed)
+    dn = [torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(net.dev) for a in noisy]
+    dt = [torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(net.dev) for a in target]
+    hist = []
+    for it in range(steps):
+        idx = rng.integers(0, len(dn), size=batch)
+        xs, ts = [], []
+        for i in idx:
+            h, w = dn[i].shape
+            y0, x0 = rng.integers(0, h - crop + 1), rng.integers(0, w - crop + 1)
+            xs.append(dn[i][y0:y0 + crop, x0:x0 + crop])
+            ts.append(dt[i][y0:y0 + crop, x0:x0 + crop])
+        xb = torch.stack(xs).contiguous()
+        tb = torch.stack(ts).contiguous()
+        sb = torch.tensor([sigma[i] for i in idx], dtype=torch.float32, device=net.dev)
+        lr_t = lr * 0.5 * (1.0 + math.cos(math.pi * it / max(steps, 1)))
+        hist.append(net.train_step(xb, tb, sb, lr=lr_t))
+        if log_every and it % log_every == 0:
+            print(f"step {it} loss {hist[-1]:.3e}")
+    return hist
+
+
+# ---------------------------------------------------------------------------------------
+# two-pass BM3Dv2 with the plain step 1 or the pilot, and the 0.05 dB gate
+# ---------------------------------------------------------------------------------------
+def two_pass(noisy: np.ndarray, sigma: float, ref: Optional[np.ndarray] = None, **kw) -> np.ndarray:
+    """BM3Dv2 step 2 (Wiener) of a float32 plane with `ref` as its reference; ref None = plain step 1."""
+    import zb3d
+    clip = zb3d.Clip.from_frames([[noisy]])
+    if ref is None:
+        ref = np.array(zb3d.BM3Dv2(clip, sigma=sigma, **kw).get_frame(0)[0])
+    rclip = zb3d.Clip.from_frames([[np.ascontiguousarray(ref, np.float32)]])
+    return np.array(zb3d.BM3Dv2(clip, ref=rclip, sigma=sigma, **kw).get_frame(0)[0])
+
+
+class PilotGate:
+    """Per noise level: use the pilot only where its two-pass PSNR is within `tol` dB
+    of the plain two-pass PSNR on held-out synthetic frames."""
+
+    def __init__(self, net: PilotNet, tol: float = 0.05):
+        self.net, self.tol = net, tol
+        self.delta: dict = {}
+
+    def calibrate(self, sigmas: Sequence[float], frames: int = 2, size: int = 256, seed: int = 99, **kw) -> dict:
+        for si, s in enumerate(sigmas):
+            d = []
+            for f in range(frames):
+                cl = synth.clean_plane(size, size, 5000 + seed + si, f)
+                nz = synth.noisy_plane(size, size, s, clip=5000 + seed + si, frame=f)
+                plain = two_pass(nz, s, **kw)
+                piloted = two_pass(nz, s, ref=self.net.denoise(nz, s), **kw)
+                d.append(synth.psnr(piloted, cl) - synth.psnr(plain, cl))
+            self.delta[float(s)] = float(np.mean(d))
+        return dict(self.delta)
+
+    def accepts(self, sigma: float) -> bool:
+        if not self.delta:
+            return False
+        near = min(self.delta, key=lambda s: abs(s - sigma))
+        return self.delta[near] >= -self.tol
+
+    def reference(self, noisy: np.ndarray, sigma: float, **kw) -> np.ndarray:
+        """Step 2's reference: the pilot where accepted, else the plain step 1."""
+        if self.accepts(sigma):
+            return self.net.denoise(noisy, sigma)
+        import zb3d
+        return np.array(zb3d.BM3Dv2(zb3d.Clip.from_frames([[noisy]]), sigma=sigma, **kw).get_frame(0)[0])

@@ -209,6 +209,81 @@ class DevicePipeline:
             f.close()
 
 
+def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frames: int = 4):
+    """Two-pass BM3Dv2 with the learned pilot (zb3d/pilot.py, shipped weights) as the
+    step-2 reference in place of the step-1 estimate, on the same frames: device-resident
+    Mpix/s, and PSNR against the clean frames next to the plain two-pass form."""
+    from zb3d import _native as N
+    from zb3d import pilot as P
+    from zb3d import synth
+    from zb3d.device import DeviceFilter
+    net = P.shipped()
+    final = DeviceFilter(W, H, family=N.YUV, subsampling=(1, 1), num_streams=1, ref=True, **KW)
+    basic = DeviceFilter(W, H, family=N.YUV, subsampling=(1, 1), num_streams=1, **KW)
+    lay = final.entries
+    assert all(l.pitch == l.width for l in lay), "dense planes expected"
+    sig = torch.full((1,), SIGMA, dtype=torch.float32, device="cuda")
+    nf = len(frames)
+    bufs, outs = [], []
+    for i in range(nf):
+        fb, fo = [], []
+        for e, l in enumerate(lay):
+            pe = l.height * l.pitch
+            b = torch.zeros(2 * pe, dtype=torch.float32, device="cuda")
+            b[pe:].copy_(torch.from_numpy(np.ascontiguousarray(frames[i][l.plane[0]], np.float32).reshape(-1)))
+            fb.append(b)
+            fo.append(torch.empty(pe, dtype=torch.float32, device="cuda"))
+        bufs.append(fb)
+        outs.append(fo)
+
+    stream = torch.cuda.Stream()  # one stream for every launch: step 2 must follow its reference
+    st = stream.cuda_stream
+
+    def frame(i, use_pilot=True):
+        with torch.cuda.stream(stream):
+            for e, l in enumerate(lay):
+                b, pe = bufs[i][e], l.height * l.pitch
+                if use_pilot:
+                    net.forward(b[pe:].view(1, l.height, l.width), sig, out=b[:pe].view(1, l.height, l.width),
+                                stream=st)
+                else:
+                    basic.run_entry(e, b.data_ptr() + 4 * pe, b.data_ptr(), st)
+                final.run_entry(e, b.data_ptr(), outs[i][e].data_ptr(), st)
+
+    def psnrs(i):
+        return [synth.psnr(outs[i][e].view(l.height, l.width).cpu().numpy(),
+                           synth.clean_plane(l.width, l.height, clip, i, l.plane[0])) for e, l in enumerate(lay)]
+
+    plain, piloted = [], []
+    for i in range(min(psnr_frames, nf)):
+        frame(i, use_pilot=False)
+        torch.cuda.synchronize()
+        plain.append(psnrs(i))
+        frame(i, use_pilot=True)
+        torch.cuda.synchronize()
+        piloted.append(psnrs(i))
+    for j in range(warmup):
+        frame(j % nf)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for j in range(steps * BATCH):
+        frame(j % nf)
+    t1.record(stream)
+    t1.synchronize()
+    ms = t0.elapsed_time(t1)
+    plain, piloted = np.array(plain), np.array(piloted)
+    delta = float(np.mean(piloted - plain))
+    final.close()
+    basic.close()
+    return {"value": W * H * steps * BATCH / (ms / 1e3) / 1e6, "unit": "Mpix/s", "ms_per_frame": ms / (steps * BATCH),
+            "psnr_plain_two_pass_db": float(np.mean(plain)), "psnr_pilot_two_pass_db": float(np.mean(piloted)),
+            "delta_psnr_db": delta, "delta_psnr_db_per_plane": [float(d) for d in np.mean(piloted - plain, 0)],
+            "within_0_05_db": delta >= -0.05,
+            "what": "pilot (10 x conv3x3, 48 ch, BF16 mma.sync kernels, FP32 accumulation) as step 1 on every plane, "
+                    "then the exact step 2; PSNR over the first %d frames against the clean frames" % min(psnr_frames, nf)}
+
+
 def run_e2e(frames, steps: int, warmup: int, num_streams: int = 4):
     """Same job through the public API on host frames (zb3d.BM3Dv2)."""
     import zb3d
@@ -473,6 +548,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other block-matching form")
+    ap.add_argument("--no-pilot", action="store_true", help="skip the learned-pilot form")
     ap.add_argument("--streams", type=int, default=4, help="CUDA streams the device pipeline spreads frames over")
     ap.add_argument("--match-form", type=int, choices=[-1, 0, 1], default=-1,
                     help="block matching: -1 = the library's autotuned choice per plane, 0 = FP32 scan of every "
@@ -598,6 +674,11 @@ def main():
     forms["note"] = ("both forms give bit-identical match lists and outputs (delta PSNR 0 dB); "
                      "tensor_core = tcgen05 FP16 distance bound in TMEM + exact FP32 re-rank")
     out["forms"] = forms
+    if rank == 0 and not args.no_pilot:
+        if pipe is not None:
+            pipe.close()
+            pipe = None
+        out["pilot_form"] = run_pilot_form(torch, frames, rank, max(1, args.steps // 4), 1)
     if rank == 0 and not args.no_ref_cuda:
         rms = run_ref_cuda(torch, frames, args.steps, args.warmup)
         if rms:

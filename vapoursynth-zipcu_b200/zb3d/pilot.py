@@ -101,29 +101,30 @@ class PilotNet:
         return net
 
     # -- passes ------------------------------------------------------------------------
-    def forward(self, noisy, sigma, keep_acts: bool = False):
+    def forward(self, noisy, sigma, keep_acts: bool = False, out=None, stream=None):
         """noisy: float32 [n][h][w] device tensor, sigma: float32 [n] (8-bit scale).
-        Returns y = noisy + net output (float32 [n][h][w]) and, with keep_acts, the
-        stored BF16 activations of every layer's input."""
+        Returns y = noisy + net output (float32 [n][h][w], written to `out` if given)
+        and, with keep_acts, the stored BF16 activations of every layer's input.
+        `stream`: a CUDA stream handle (int) for every launch, or None for the default."""
         torch, lib = self.torch, N.lib()
         n, h, w = noisy.shape
         x = torch.empty((n, h, w, 16), dtype=torch.bfloat16, device=self.dev)
-        _ok(lib.zb3d_pilot_pack_input(_p(noisy), _p(sigma), n, h, w, LEVEL_SCALE, _p(x), None), "pack_input")
+        _ok(lib.zb3d_pilot_pack_input(_p(noisy), _p(sigma), n, h, w, LEVEL_SCALE, _p(x), stream), "pack_input")
         acts = [x]
-        y = torch.empty((n, h, w), dtype=torch.float32, device=self.dev)
+        y = out if out is not None else torch.empty((n, h, w), dtype=torch.float32, device=self.dev)
         last = len(SHAPES) - 1
         for l, (cin, cout) in enumerate(SHAPES):
             if l < last:
                 a = torch.empty((n, h, w, cout), dtype=torch.bfloat16, device=self.dev)
                 _ok(lib.zb3d_pilot_conv3x3(_p(acts[-1]), n, h, w, cin, _p(self.w16[l]), _p(self.b32[l]), cout, 1,
-                                           None, _p(a), None, None, None), f"conv {l}")
+                                           None, _p(a), None, None, stream), f"conv {l}")
                 if keep_acts:
                     acts.append(a)
                 else:
                     acts = [a]
             else:
                 _ok(lib.zb3d_pilot_conv3x3(_p(acts[-1]), n, h, w, cin, _p(self.w16[l]), _p(self.b32[l]), cout, 0,
-                                           None, None, _p(y), _p(noisy), None), "conv out")
+                                           None, None, _p(y), _p(noisy), stream), "conv out")
         return y, (acts if keep_acts else None)
 
     def gradients(self, noisy, target, sigma):
@@ -184,12 +185,13 @@ def step1_estimates(noisy: Sequence[np.ndarray], sigma: float, **bm3d_kw) -> lis
     return [np.array(basic.get_frame(i)[0]) for i in range(len(noisy))]
 
 
-def make_pairs(count: int, size: int, sigmas: Sequence[float], seed: int = 1, clip0: int = 1000, **bm3d_kw):
-    """`count` frames of size x size per sigma: (noisy, step-1, clean, sigma) lists."""
+def make_pairs(count: int, size, sigmas: Sequence[float], seed: int = 1, clip0: int = 1000, **bm3d_kw):
+    """`count` frames per sigma of size x size (or (width, height)): (noisy, step-1, clean, sigma) lists."""
+    w, h = (size, size) if isinstance(size, int) else size
     noisy, target, clean, sig = [], [], [], []
     for si, s in enumerate(sigmas):
-        fr = [synth.noisy_plane(size, size, s, clip=clip0 + seed * 100 + si, frame=f) for f in range(count)]
-        cl = [synth.clean_plane(size, size, clip0 + seed * 100 + si, f) for f in range(count)]
+        fr = [synth.noisy_plane(w, h, s, clip=clip0 + seed * 100 + si, frame=f) for f in range(count)]
+        cl = [synth.clean_plane(w, h, clip0 + seed * 100 + si, f) for f in range(count)]
         noisy += fr
         clean += cl
         target += step1_estimates(fr, s, **bm3d_kw)
@@ -268,3 +270,73 @@ class PilotGate:
             return self.net.denoise(noisy, sigma)
         import zb3d
         return np.array(zb3d.BM3Dv2(zb3d.Clip.from_frames([[noisy]]), sigma=sigma, **kw).get_frame(0)[0])
+
+
+# ---------------------------------------------------------------------------------------
+# the shipped pilot
+# ---------------------------------------------------------------------------------------
+import os as _os
+
+WEIGHTS = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_bs4_r12.npz")
+TRAIN_KW = dict(block_step=4, bm_range=12)   # step-1 configuration the shipped pilot imitates
+TRAIN_SIGMAS = (5.0, 10.0, 15.0, 20.0, 25.0)
+
+
+def shipped(device: str = "cuda") -> PilotNet:
+    """The pilot trained by `python -m zb3d.pilot train` (weights next to this file)."""
+    return PilotNet.load(WEIGHTS, device=device)
+
+
+def evaluate(net: PilotNet, sigmas=TRAIN_SIGMAS, frames: int = 4, size: int = 384, seed: int = 77, **kw) -> list:
+    """Held-out synthetic frames: PSNR against the clean frame of the noisy input, plain
+    step 1, the pilot, plain two-pass and pilot two-pass."""
+    rows = []
+    for si, s in enumerate(sigmas):
+        acc = np.zeros(5)
+        for f in range(frames):
+            cl = synth.clean_plane(size, size, 9000 + seed + si, f)
+            nz = synth.noisy_plane(size, size, s, clip=9000 + seed + si, frame=f)
+            st1 = step1_estimates([nz], s, **kw)[0]
+            pe = net.denoise(nz, s)
+            acc += [synth.psnr(nz, cl), synth.psnr(st1, cl), synth.psnr(pe, cl),
+                    synth.psnr(two_pass(nz, s, ref=st1, **kw), cl), synth.psnr(two_pass(nz, s, ref=pe, **kw), cl)]
+        rows.append((float(s), *(acc / frames)))
+    return rows
+
+
+def main(argv=None):
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m zb3d.pilot")
+    ap.add_argument("cmd", choices=["train", "eval"])
+    ap.add_argument("--frames", type=int, default=6, help="training frames per noise level and frame size")
+    ap.add_argument("--dims", default="1920x1080,960x540", help="training frame sizes (the 1080p YUV420 planes)")
+    ap.add_argument("--steps", type=int, default=6250, help="Adam steps of 32 crops (6250 = 200k crops)")
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--out", default=WEIGHTS)
+    a = ap.parse_args(argv)
+    import time
+    if a.cmd == "train":
+        t0 = time.time()
+        noisy, target, sig = [], [], []
+        for k, d in enumerate(a.dims.split(",")):
+            wd, ht = (int(v) for v in d.split("x"))
+            nz, tg, _, sg = make_pairs(a.frames, (wd, ht), TRAIN_SIGMAS, seed=11 + k, **TRAIN_KW)
+            noisy, target, sig = noisy + nz, target + tg, sig + sg
+        print(f"{len(noisy)} training pairs ({a.dims}, step 1 with {TRAIN_KW}) in {time.time() - t0:.1f} s")
+        net = PilotNet(seed=0)
+        t0 = time.time()
+        hist = train(net, noisy, target, sig, steps=a.steps, batch=32, crop=64, lr=a.lr, seed=5)
+        net.torch.cuda.synchronize()
+        print(f"{a.steps} steps x 32 crops of 64x64 in {time.time() - t0:.1f} s; "
+              f"loss {np.mean(hist[:50]):.3e} -> {np.mean(hist[-50:]):.3e}")
+        net.save(a.out)
+        print(f"saved {a.out}")
+    else:
+        net = PilotNet.load(a.out)
+    print("sigma  noisy  step1  pilot  two-pass(step1)  two-pass(pilot)  delta")
+    for s, n0, s1, p1, tp, tq in evaluate(net, **TRAIN_KW):
+        print(f"{s:5.1f} {n0:6.2f} {s1:6.2f} {p1:6.2f} {tp:10.2f} {tq:15.2f} {tq - tp:+8.3f}")
+
+
+if __name__ == "__main__":
+    main()

@@ -180,3 +180,30 @@ def test_pinned_and_pageable_frames_take_the_same_path_to_the_same_bytes():
     ref = zb3d.BM3Dv2(clip, **kw).get_frame(0)
     for p in range(3):
         assert np.array_equal(planes[p], ref[p])
+
+
+def test_graph_replay_equals_direct_launches():
+    """Device entry points capture a window's launches into a CUDA graph on first use and
+    replay it; profiling forces direct launches.  All three give the same bytes."""
+    import torch
+    from zb3d.device import DeviceFilter
+    w, h = 320, 200
+    f = DeviceFilter(w, h, family=N.YUV, subsampling=(1, 1), num_streams=1, sigma=[10.0] * 3, block_step=4,
+                     bm_range=12, extractor_exp=3)
+    src = np.zeros(f.src_elems, np.float32)
+    for e, lay in enumerate(f.entries):
+        src[lay.src_offset:lay.src_offset + lay.src_elems].reshape(lay.height, lay.pitch)[:, :lay.width] = \
+            synth.noisy_plane(lay.width, lay.height, 10.0, plane=e)
+    d_src = torch.from_numpy(src).cuda()
+    outs = []
+    for profile in (False, False, True):
+        f.profile(profile)
+        d_dst = torch.full((f.dst_elems,), float("nan"), dtype=torch.float32, device="cuda")
+        f.run(d_src.data_ptr(), d_dst.data_ptr())
+        torch.cuda.synchronize()
+        outs.append(d_dst.cpu().numpy())
+    f.profile(False)
+    f.profile_collect()
+    f.close()
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+    assert np.array_equal(outs[0].view(np.uint32), outs[2].view(np.uint32))

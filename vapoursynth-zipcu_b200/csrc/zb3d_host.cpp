@@ -19,6 +19,7 @@
 #include <cstring>
 #include <sys/stat.h>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -294,6 +295,11 @@ struct Filter {
     // temporal caches (src/framecache.zig): source frames and accumulator stacks
     DevCache src_cache, acc_cache;
 
+    // CUDA graphs of whole windows / entries, captured once per buffer pair and replayed
+    std::mutex graph_mu;
+    std::map<std::tuple<const void *, const void *, int>, cudaGraphExec_t> graphs;
+    bool graphs_ok = true;
+
     // optional launch timing (zb3d_profile_enable)
     bool profile = false;
     std::mutex prof_mu;
@@ -549,6 +555,57 @@ cudaEvent_t prof_event(Filter *f, std::vector<cudaEvent_t> &v, cudaStream_t st) 
 
 // Runs every entry of one window (d_src, entry layout) into d_dst on the slot's stream.
 cudaError_t run_entry(Filter *f, Slot &s, const Entry &en, const float *src, float *dst);
+
+// Runs `fn(s)` (launches on s.st) as a CUDA graph: captured once per key on the slot's
+// own stream, then replayed on `launch`.  A window's whole launch sequence (memsets,
+// matching, filtering, finishing of every plane) becomes one graph launch.  Graphs bake
+// in the slot's scratch buffers, so replays of one key must not overlap (the device
+// entry points' rule).  ZB3D_GRAPHS=0, profiling, or a failed capture -> direct launches.
+template <class Fn>
+cudaError_t run_graphed(Filter *f, Slot &s, std::tuple<const void *, const void *, int> key, cudaStream_t launch,
+                        Fn fn) {
+    static const bool env_off = [] {
+        const char *v = getenv("ZB3D_GRAPHS");
+        return v && strcmp(v, "0") == 0;
+    }();
+    if (env_off || f->profile || !f->graphs_ok) {
+        Slot d = s;
+        d.st = launch;
+        return fn(d);
+    }
+    cudaGraphExec_t exec = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(f->graph_mu);
+        auto it = f->graphs.find(key);
+        if (it != f->graphs.end()) exec = it->second;
+    }
+    if (!exec) {
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(s.st, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            const cudaError_t e1 = fn(s);
+            e = cudaStreamEndCapture(s.st, &g);
+            if (e1 != cudaSuccess) e = e1;
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
+            if (g) cudaGraphDestroy(g);
+        }
+        if (e != cudaSuccess) {  // not capturable here: launch directly from now on
+            cudaGetLastError();
+            if (exec) cudaGraphExecDestroy(exec);
+            f->graphs_ok = false;
+            Slot d = s;
+            d.st = launch;
+            return fn(d);
+        }
+        std::lock_guard<std::mutex> lk(f->graph_mu);
+        if (f->graphs.size() >= 256) {  // bounded: drop everything, re-capture on demand
+            for (auto &kv : f->graphs) cudaGraphExecDestroy(kv.second);
+            f->graphs.clear();
+        }
+        f->graphs[key] = exec;
+    }
+    return cudaGraphLaunch(exec, launch);
+}
 
 cudaError_t run_window(Filter *f, Slot &s, const float *d_src, float *d_dst) {
     for (const Entry &en : f->entries) {
@@ -1057,9 +1114,10 @@ int zb3d_process_device(zb3d_filter *fp, const float *d_src, float *d_dst, void 
         return -1;
     }
     cudaSetDevice(f->device);
-    zb::Slot s = f->slots[0];
-    s.st = stream ? (cudaStream_t)stream : f->slots[0].st;
-    cudaError_t e = zb::run_window(f, s, d_src, d_dst);
+    zb::Slot &s = f->slots[0];
+    const cudaStream_t st = stream ? (cudaStream_t)stream : s.st;
+    cudaError_t e = zb::run_graphed(f, s, std::make_tuple((const void *)d_src, (const void *)d_dst, -1), st,
+                                    [&](zb::Slot &x) { return zb::run_window(f, x, d_src, d_dst); });
     if (e != cudaSuccess) {
         zb::set_err(err, errlen, "BM3D: process frame failed (%s).", cudaGetErrorString(e));
         return -1;
@@ -1075,9 +1133,11 @@ int zb3d_process_entry_device(zb3d_filter *fp, int e, const float *d_src, float 
         return -1;
     }
     cudaSetDevice(f->device);
-    zb::Slot s = f->slots[0];
-    s.st = stream ? (cudaStream_t)stream : f->slots[0].st;
-    cudaError_t ce = zb::run_entry(f, s, f->entries[e], d_src, d_dst);
+    zb::Slot &s = f->slots[0];
+    const cudaStream_t st = stream ? (cudaStream_t)stream : s.st;
+    const zb::Entry &en = f->entries[e];
+    cudaError_t ce = zb::run_graphed(f, s, std::make_tuple((const void *)d_src, (const void *)d_dst, e), st,
+                                     [&](zb::Slot &x) { return zb::run_entry(f, x, en, d_src, d_dst); });
     if (ce != cudaSuccess) {
         zb::set_err(err, errlen, "BM3D: process frame failed (%s).", cudaGetErrorString(ce));
         return -1;
@@ -1272,7 +1332,9 @@ static int get_frame_window(Filter *f, int n, const zb3d_frame *clip_frames, con
     }
     if (ce == cudaSuccess) ce = cudaEventRecord(s.ev_up, s.cst);
     if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s.st, s.ev_up, 0);
-    if (ce == cudaSuccess) ce = run_window(f, s, s.d_src, s.d_dst);
+    if (ce == cudaSuccess)
+        ce = run_graphed(f, s, std::make_tuple((const void *)s.d_src, (const void *)s.d_dst, -1), s.st,
+                         [&](Slot &x) { return run_window(f, x, x.d_src, x.d_dst); });
     // page-locked output planes receive the result directly (denoised planes only;
     // the stacked accumulator layout goes through staging)
     bool direct_out = !f->stacked_out();
@@ -1502,6 +1564,9 @@ void zb3d_free(zb3d_filter *fp) {
     if (!f) return;
     if (!f->passthrough) {
         cudaSetDevice(f->device);
+        cudaDeviceSynchronize();
+        for (auto &kv : f->graphs) cudaGraphExecDestroy(kv.second);
+        f->graphs.clear();
         for (auto &s : f->slots) {
             if (s.st) cudaStreamSynchronize(s.st);
             if (s.cst) cudaStreamSynchronize(s.cst);

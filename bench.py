@@ -538,6 +538,98 @@ def run_gray640(torch, steps: int, warmup: int):
                                    "extractor_exp 3, single pass"}}
 
 
+def run_batched(torch, steps: int, warmup: int, nstreams: int = 4):
+    """Uneven batch: 720x480, 1280x720 and 3840x2160 clips of 16 frames, YUV420 per plane or
+    YUV444 CBM3D (chroma=1, matched on Y), radius 0 or 1 (stacked output), sigma drawn per
+    clip from U[5, 20], autotuned matching.  Every clip frame is one device window, replayed
+    as a CUDA graph; windows are spread round-robin over `nstreams` streams.  A step is all
+    64 windows.  Latency per window: its CUDA events on its stream, queueing included."""
+    from zb3d import _native as N
+    from zb3d import synth
+    from zb3d.device import DeviceFilter
+    rng = np.random.default_rng(2024)
+    clips = [dict(w=720, h=480, fam=N.YUV, sub=(1, 1), chroma=0, radius=0),
+             dict(w=1280, h=720, fam=N.YUV, sub=(0, 0), chroma=1, radius=0),
+             dict(w=1280, h=720, fam=N.YUV, sub=(1, 1), chroma=0, radius=1),
+             dict(w=3840, h=2160, fam=N.YUV, sub=(1, 1), chroma=0, radius=0)]
+    nfr = 16
+    for c in clips:
+        c["sigma"] = float(rng.uniform(5.0, 20.0))
+        c["filters"] = [DeviceFilter(c["w"], c["h"], family=c["fam"], subsampling=c["sub"], num_streams=1,
+                                     num_frames=nfr, sigma=[c["sigma"]] * 3, chroma=c["chroma"], radius=c["radius"],
+                                     block_step=4, bm_range=12, extractor_exp=EXTRACTOR_EXP) for _ in range(nstreams)]
+        f0 = c["filters"][0]
+        c["src"], c["dst"] = [], []
+        tw = 2 * c["radius"] + 1
+        planes = [synth.noisy_plane(c["w"] >> (p > 0 and c["sub"][0]), c["h"] >> (p > 0 and c["sub"][1]),
+                                    c["sigma"], clip=7, frame=0, plane=p) for p in range(3)]
+        for n in range(nfr):  # the same content in every window keeps the set-up short; the work is identical
+            host = np.zeros(f0.src_elems, np.float32)
+            for lay in f0.entries:
+                v = host[lay.src_offset:lay.src_offset + lay.src_elems].reshape(
+                    lay.nclips, lay.nplanes, lay.tw, lay.height, lay.pitch)
+                for i in range(lay.nplanes):
+                    v[:, i, :, :, :lay.width] = planes[lay.plane[i]][:, :lay.width]
+            c["src"].append(torch.from_numpy(host).cuda())
+            c["dst"].append(torch.empty(f0.dst_elems, dtype=torch.float32, device="cuda"))
+        c["tw"] = tw
+    streams = [torch.cuda.Stream() for _ in range(nstreams)]
+    order = [(ci, n) for n in range(nfr) for ci in range(len(clips))]
+
+    def step(record=None):
+        for k, (ci, n) in enumerate(order):
+            c, j = clips[ci], k % nstreams
+            st = streams[j]
+            if record is not None:
+                a = torch.cuda.Event(enable_timing=True)
+                a.record(st)
+            c["filters"][j].run(c["src"][n].data_ptr(), c["dst"][n].data_ptr(), st.cuda_stream)
+            if record is not None:
+                z = torch.cuda.Event(enable_timing=True)
+                z.record(st)
+                record.append((ci, a, z))
+
+    for _ in range(max(warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t0.record(streams[0])
+    for s in streams[1:]:
+        s.wait_event(t0)
+    recs = []
+    for _ in range(steps):
+        step(recs)
+    for s in streams[1:]:
+        e = torch.cuda.Event()
+        e.record(s)
+        streams[0].wait_event(e)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t1.record(streams[0])
+    t1.synchronize()
+    ms = t0.elapsed_time(t1)
+    lat = {ci: [] for ci in range(len(clips))}
+    for ci, a, z in recs:
+        lat[ci].append(a.elapsed_time(z))
+    px = sum(c["w"] * c["h"] * nfr for c in clips) * steps
+    per_clip = []
+    for ci, c in enumerate(clips):
+        l = np.array(lat[ci])
+        per_clip.append({"clip": f"{c['w']}x{c['h']} {'YUV444 CBM3D' if c['chroma'] else 'YUV420'} r{c['radius']}",
+                         "sigma": round(c["sigma"], 2), "frames": nfr,
+                         "latency_ms_p50": float(np.percentile(l, 50)), "latency_ms_p99": float(np.percentile(l, 99)),
+                         "matching": [list(f) for f in (c["filters"][0].tuning(e) for e in range(len(c["filters"][0].entries)))]})
+    for c in clips:
+        for f in c["filters"]:
+            f.close()
+    return {"metric": "batched uneven BM3D Mpix/s (luma)", "value": px / (ms / 1e3) / 1e6, "unit": "Mpix/s",
+            "ms_per_step": ms / steps, "steps": steps, "warmup": warmup,
+            "config": {"workload": "4 clips x 16 frames: 720x480 YUV420 r0, 1280x720 YUV444 CBM3D r0, 1280x720 "
+                                   "YUV420 r1 (stacked output), 3840x2160 YUV420 r0; sigma U[5,20] per clip; "
+                                   "block_step 4, bm_range 12, single pass", "streams": nstreams,
+                       "launch": "one CUDA graph per window (all planes' memsets, matching, filtering, finishing)",
+                       "per_clip": per_clip}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -553,7 +645,7 @@ def main():
     ap.add_argument("--match-form", type=int, choices=[-1, 0, 1], default=-1,
                     help="block matching: -1 = the library's autotuned choice per plane, 0 = FP32 scan of every "
                          "candidate, 1 = tensor-core bound + exact re-rank")
-    ap.add_argument("--workload", choices=["twopass1080", "vbm3d", "gray640"], default="twopass1080",
+    ap.add_argument("--workload", choices=["twopass1080", "vbm3d", "gray640", "batched"], default="twopass1080",
                     help="twopass1080 is the metric's workload; the others print their own line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -569,7 +661,7 @@ def main():
     import torch
     torch.cuda.set_device(local)
     if args.workload != "twopass1080":
-        fn = run_vbm3d if args.workload == "vbm3d" else run_gray640
+        fn = {"vbm3d": run_vbm3d, "gray640": run_gray640, "batched": run_batched}[args.workload]
         out = fn(torch, args.steps, args.warmup)
         out.update({"n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic"})
         print(json.dumps(out))

@@ -273,14 +273,25 @@ void zb3d_host_free(void *p);
  *
  * Kernels of the residual conv net that can replace the BM3D step-1 estimate as
  * step 2's reference (zb3d/pilot.py trains and runs it).  BF16 tensors (void *),
- * NHWC with channel counts 16 or 48; weights [cout][3][3][cin]; FP32 accumulation.
+ * NHWC with channel counts 16, 32 or 48; weights [cout][3][3][cin]; FP32 accumulation.
  * All calls are asynchronous on `stream` and return 0, or -1 on a launch error.
  */
 /* y = conv3x3(x) + bias (may be NULL), ReLU if relu, zeroed where mask (NHWC, cout
  * channels, may be NULL) is <= 0; y (may be NULL) BF16 NHWC; y0 (may be NULL) the
- * FP32 channel 0 plus resid (may be NULL).  (cin, cout) in {(16,48), (48,48), (48,16)}. */
+ * FP32 channel 0 plus resid (may be NULL).  (cin, cout) in {(16,48), (48,48), (48,16), (16,32),
+ * (32,32), (32,16)}.  mma.sync BF16 tiles of 8 x 16 pixels; the training passes use it. */
 int zb3d_pilot_conv3x3(const void *x, int n, int h, int w, int cin, const void *wgt, const float *bias, int cout,
                        int relu, const void *mask, void *y, float *y0, const float *resid, void *stream);
+/* The same forward convolution (no mask) on the tensor cores, for inference: tcgen05.mma
+ * with the accumulator in tensor memory, input rows staged by TMA, persistent CTAs down
+ * 128-pixel column strips.  x and y use the channel-blocked layout [n][C/8][h][w][8]
+ * (BF16); same shapes; x, wgt and y 16-byte aligned.  status (device int, may be NULL)
+ * becomes non-zero if a pipeline wait timed out. */
+int zb3d_pilot_conv3x3_tc(const void *x, int n, int h, int w, int cin, const void *wgt, const float *bias, int cout,
+                          int relu, void *y, float *y0, const float *resid, int *status, void *stream);
+/* The network input of zb3d_pilot_pack_input in the channel-blocked layout ([n][2][h][w][8]). */
+int zb3d_pilot_pack_input_blocked(const float *noisy, const float *sigma, int n, int h, int w, float level_scale,
+                                  void *x0, void *stream);
 /* dw += dL/dw, db += dL/db of one layer from its input x and its pre-activation gradient dy. */
 int zb3d_pilot_conv3x3_wgrad(const void *x, const void *dy, int n, int h, int w, int cin, int cout, float *dw,
                              float *db, void *stream);

@@ -1,0 +1,495 @@
+// Learned pilot: inference convolution on the 5th-generation tensor cores.
+//
+// y = conv3x3(x) + bias (ReLU) as an implicit GEMM per tile of 128 consecutive
+// pixels of one image row: D[128 x COUT] = sum over the 9 taps and CIN / 16
+// K-steps of A[128 x 16] . B[16 x COUT], BF16 operands in shared memory, FP32
+// accumulator in tensor memory (tcgen05.mma kind::f16, M = 128, N = COUT).
+//
+// Activations use the channel-blocked layout [n][C / 8][h][w][8] (BF16): one
+// channel block of an image row is a contiguous run of 16-byte pixels.
+//
+// No im2col: a CTA walks down strips of 128 columns and TMA stages every input
+// row it needs once (130 pixels with the halo, zero-filled outside the image)
+// into a ring of row slots laid out [channel block][pixel][8 channels], one
+// contiguous 2080-byte box per channel block.  In that layout the A operand of
+// tap (ky, kx), K-step s, is the canonical no-swizzle K-major matrix that starts
+// at pixel kx of the slot holding input row y + ky - 1, channel block 2 s: 8-pixel core matrices 128 bytes apart (SBO) and
+// the two 8-channel halves one channel block apart (LBO).  The weights stay in
+// shared memory for the CTA's lifetime as [tap][channel block][cout][8].
+//
+// Two CTAs per SM, each owning a contiguous range of tiles in (image, strip, row)
+// order (balanced to one tile).  The row ring fills the shared memory the weights
+// leave (up to 16 slots), so TMA keeps RING - 3 rows in flight ahead of the MMAs.
+//
+// Roles (256 threads): warp 0 lane 0 issues the TMA row loads, warp 1 lane 0
+// issues the MMAs, warp 2 owns the tensor-memory allocation, warps 4-7 (one per
+// 32-lane quarter of tensor memory) drain the 4 accumulator buffers: bias,
+// ReLU, BF16 store (16 bytes per channel block, 512 contiguous bytes per warp),
+// or for the last layer channel 0 plus the residual in FP32.  mbarriers link the
+// roles; every wait is bounded, and a timeout sets the status word and ends every
+// role early.
+//
+// Same arithmetic as the mma.sync kernel in zb3d_pilot.cu (BF16 products, FP32
+// sums, bias then ReLU then one BF16 rounding); only the summation order differs.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace zb {
+namespace pilot_tc {
+
+constexpr int TILE = 128;                // output pixels per tile (MMA M)
+constexpr int HALO = TILE + 2;           // staged input pixels per row
+constexpr int BOX_BYTES = HALO * 16;     // one channel block of a staged row (TMA box 8 x 130)
+constexpr int CB_BYTES = 2176;           // ... padded to a multiple of 128 bytes
+constexpr int MAX_RING = 16;             // staged input row slots, at most
+constexpr int CTAS_PER_SM = 2;           // two independent pipelines per SM
+constexpr int SMEM_BUDGET = 112 * 1024;  // shared memory of the ring and the weights, per CTA
+constexpr int NACC = 4;                  // accumulator buffers
+constexpr int ACC_COLS = 64;             // tensor-memory columns per accumulator buffer
+constexpr int TMEM_COLS = NACC * ACC_COLS;
+constexpr int THREADS = 256;
+constexpr unsigned WAIT_LIMIT = 1u << 20;  // try_wait rounds on an mbarrier before giving up (about a second)
+
+struct Args {
+    const __nv_bfloat16 *wgt;  // [cout][9][cin]
+    const float *bias;         // [cout]
+    __nv_bfloat16 *y;          // [n][cout / 8][h][w][8] or null
+    float *y0;                 // [n][h][w] or null: output channel 0 (+ resid) in FP32
+    const float *resid;        // [n][h][w] or null
+    int n, h, w, relu;
+    int strips;                // ceil(w / 128)
+    int *status;               // set non-zero when a wait timed out (may be null)
+};
+
+template <int CIN, int COUT>
+struct Shape {
+    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= ACC_COLS, "unsupported layer shape");
+    static constexpr int CB = CIN / 8;
+    static constexpr int KSTEPS = CIN / 16;
+    static constexpr int ROW_BYTES = CB * CB_BYTES;
+    static constexpr int W_BYTES = 9 * CB * COUT * 16;
+    static constexpr int RING_FIT = (SMEM_BUDGET - W_BYTES) / ROW_BYTES;
+    static constexpr int RING = RING_FIT < MAX_RING ? RING_FIT : MAX_RING;
+    static_assert(RING >= 4, "row ring too small");
+    static constexpr int OFF_W = RING * ROW_BYTES;
+    static constexpr int OFF_BAR = OFF_W + W_BYTES;
+    static constexpr int NBAR = 2 * RING + 2 * NACC + 1;  // row_full, row_free, acc_full, acc_empty, drain
+    static constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
+    static constexpr int SMEM = OFF_MISC + 16 + 128;  // tensor-memory address, abort flag; alignment slack
+    // kind::f16 instruction descriptor: FP32 accumulator (bit 4), BF16 A (bits 7-9 = 1) and
+    // B (bits 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
+    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(COUT >> 3) << 17) |
+                                      ((uint32_t)(TILE >> 4) << 24);
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor, K-major without swizzle (layout type 0):
+// start address, LBO (the two 8-element K halves) and SBO (8-row groups) in
+// 16-byte units, version 1 at bits 46-47.
+__device__ __forceinline__ uint64_t desc_k(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3fff) | ((uint64_t)((lbo >> 4) & 0x3fff) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3fff) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.u32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mbar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_tx(uint32_t mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// try_wait suspends the thread until the phase completes or a hardware time limit
+// passes, so waiting threads take no issue slots from the working ones
+__device__ __forceinline__ bool mbar_test(uint32_t mbar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Waits for phase `parity` of an mbarrier.  Gives up when another role has
+// aborted, or after WAIT_LIMIT tries: then it raises the abort flag and records
+// `code` in the status word.
+__device__ __forceinline__ bool wait_bar(uint32_t mbar, uint32_t parity, volatile int *abort_flag, int *status,
+                                         int code) {
+    for (unsigned i = 0; i < WAIT_LIMIT; ++i) {
+        if (mbar_test(mbar, parity)) return true;
+        if (*abort_flag) return false;
+    }
+    *abort_flag = 1;
+    if (status) atomicExch(status, code);
+    return false;
+}
+
+// 130 pixels from x of row y of channel-block plane `plane` (= image * CIN / 8 + block)
+__device__ __forceinline__ void tma_row(uint32_t dst, const CUtensorMap *map, int c, int x, int y, int plane,
+                                        uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];\n" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c), "r"(x), "r"(y), "r"(plane), "r"(mbar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t slot_saddr, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(slot_saddr), "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// 16 consecutive FP32 columns of this warp's 32 lanes (no wait)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(lo)) |
+           ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(hi)) << 16);
+}
+
+// A maximal run of this CTA's tiles in one strip: output rows [ya, yb).
+struct Seg {
+    int img, x0, ya, yb;
+};
+
+// Tiles are numbered (image, strip, row); the CTA owns [t, t1).  Takes the next run.
+__device__ __forceinline__ bool next_seg(const Args &p, long long &t, long long t1, Seg &k) {
+    if (t >= t1) return false;
+    const long long u = t / p.h;
+    k.ya = (int)(t - u * p.h);
+    k.img = (int)(u / p.strips);
+    k.x0 = (int)(u - (long long)k.img * p.strips) * TILE;
+    k.yb = (int)min((long long)p.h, k.ya + (t1 - t));
+    t += k.yb - k.ya;
+    return true;
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(THREADS, CTAS_PER_SM) conv3x3_tc(const __grid_constant__ CUtensorMap xmap, Args p) {
+    using S = Shape<CIN, COUT>;
+    constexpr int RING = S::RING;
+    extern __shared__ uint8_t smraw[];
+    const uint32_t raw = smem_u32(smraw);
+    const uint32_t pad = ((raw + 127u) & ~127u) - raw;
+    uint8_t *sm = smraw + pad;
+    const uint32_t sb = raw + pad;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t bar = sb + S::OFF_BAR;
+    // barrier k lives at bar + 8 k: row_full[s] = s, row_free[s] = RING + s,
+    // acc_full[b] = 2 RING + b, acc_empty[b] = 2 RING + NACC + b, drain = 2 RING + 2 NACC
+    const uint32_t row_full = bar, row_free = bar + 8u * RING;
+    const uint32_t acc_full = bar + 8u * (2 * RING), acc_empty = acc_full + 8u * NACC;
+    const uint32_t drain = acc_empty + 8u * NACC;
+    const long long tiles = (long long)p.n * p.strips * p.h;
+    const long long t_begin = tiles * blockIdx.x / gridDim.x, t_end = tiles * (blockIdx.x + 1) / gridDim.x;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + S::OFF_MISC);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(sm + S::OFF_MISC + 4);
+
+    for (int i = threadIdx.x; i < 9 * S::CB * COUT; i += THREADS) {
+        const int co = i % COUT, rest = i / COUT, cb = rest % S::CB, tap = rest / S::CB;
+        *reinterpret_cast<uint4 *>(sm + S::OFF_W + 16 * i) =
+            __ldg(reinterpret_cast<const uint4 *>(p.wgt + ((size_t)co * 9 + tap) * CIN + cb * 8));
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < RING; ++s) {
+            mbar_init(row_full + 8u * s, 1);
+            mbar_init(row_free + 8u * s, 1);
+        }
+        for (int b = 0; b < NACC; ++b) {
+            mbar_init(acc_full + 8u * b, 1);
+            mbar_init(acc_empty + 8u * b, 4);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 2) tmem_alloc(smem_u32(tslot), TMEM_COLS);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // weights: generic stores -> MMA reads
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 0 && lane == 0) {
+        // producer: input rows ya - 1 .. yb of every run, in order, into the ring
+        uint32_t e = 0;
+        bool ok = true;
+        long long t = t_begin;
+        Seg k;
+        while (ok && next_seg(p, t, t_end, k)) {
+            for (int r = k.ya - 1; r <= k.yb; ++r, ++e) {
+                const int s = (int)(e % RING);
+                if (e >= RING && !wait_bar(row_free + 8u * s, ((e / RING) - 1) & 1, abort_flag, p.status, 1)) {
+                    ok = false;
+                    break;
+                }
+                mbar_arrive_tx(row_full + 8u * s, S::CB * BOX_BYTES);
+                const uint32_t dst = sb + s * S::ROW_BYTES;
+#pragma unroll
+                for (int cb = 0; cb < S::CB; ++cb)
+                    tma_row(dst + cb * CB_BYTES, &xmap, 0, k.x0 - 1, r, k.img * S::CB + cb, row_full + 8u * s);
+            }
+        }
+        if (!ok) {
+            // let the row loads already issued land before the CTA can end
+            for (uint32_t q = e > RING ? e - RING : 0; q < e; ++q) {
+                for (unsigned i = 0; i < WAIT_LIMIT && !mbar_test(row_full + 8u * (q % RING), (q / RING) & 1); ++i) {
+                }
+            }
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        const uint64_t a_desc0 = desc_k(sb, CB_BYTES, 128);
+        const uint64_t b_desc0 = desc_k(sb + S::OFF_W, COUT * 16, 128);
+        uint32_t e = 0, t = 0;
+        bool ok = true;
+        long long tt = t_begin;
+        Seg k;
+        while (ok && next_seg(p, tt, t_end, k)) {
+            const uint32_t base = e;
+            for (int y = k.ya; y < k.yb && ok; ++y, ++t) {
+                const uint32_t e0 = base + (uint32_t)(y - k.ya);
+                for (uint32_t q = (y == k.ya ? e0 : e0 + 2); q <= e0 + 2; ++q)
+                    if (!wait_bar(row_full + 8u * (q % RING), (q / RING) & 1, abort_flag, p.status, 2)) {
+                        ok = false;
+                        break;
+                    }
+                const int b = (int)(t % NACC);
+                if (ok && t >= NACC && !wait_bar(acc_empty + 8u * b, ((t / NACC) - 1) & 1, abort_flag, p.status, 3))
+                    ok = false;
+                if (!ok) break;
+                fence_after_sync();
+                const uint32_t d = tmem + (uint32_t)(b * ACC_COLS);
+                // descriptors advance by constant offsets (16-byte units in the low bits)
+#pragma unroll
+                for (int ky = 0; ky < 3; ++ky) {
+                    const uint64_t arow = a_desc0 + (uint64_t)(((e0 + ky) % RING) * (S::ROW_BYTES >> 4));
+#pragma unroll
+                    for (int kx = 0; kx < 3; ++kx)
+#pragma unroll
+                        for (int ks = 0; ks < S::KSTEPS; ++ks)
+                            mma_bf16(d, arow + (uint64_t)((2 * ks * CB_BYTES + kx * 16) >> 4),
+                                     b_desc0 + (uint64_t)((((ky * 3 + kx) * S::CB + 2 * ks) * COUT * 16) >> 4),
+                                     S::IDESC, (ky | kx | ks) != 0);
+                }
+                mma_commit(acc_full + 8u * b);                  // accumulator ready
+                mma_commit(row_free + 8u * (e0 % RING));        // input row y - 1 no longer needed
+                if (y == k.yb - 1) {
+                    mma_commit(row_free + 8u * ((e0 + 1) % RING));
+                    mma_commit(row_free + 8u * ((e0 + 2) % RING));
+                }
+            }
+            e = base + (uint32_t)(k.yb - k.ya + 2);
+        }
+        // every MMA issued has completed before the CTA ends
+        mma_commit(drain);
+        for (unsigned i = 0; i < WAIT_LIMIT && !mbar_test(drain, 0); ++i) {
+        }
+    } else if (warp >= 4) {
+        // epilogue: warp 4 + q drains tensor-memory lanes 32 q .. 32 q + 31 (pixels of the tile)
+        const int q = warp & 3;
+        float bias[COUT];
+#pragma unroll
+        for (int i = 0; i < COUT; ++i) bias[i] = p.bias ? __ldg(p.bias + i) : 0.0f;
+        uint32_t t = 0;
+        bool ok = true;
+        long long tt = t_begin;
+        Seg k;
+        while (ok && next_seg(p, tt, t_end, k)) {
+            for (int y = k.ya; y < k.yb; ++y, ++t) {
+                const int b = (int)(t % NACC);
+                if (!wait_bar(acc_full + 8u * b, (t / NACC) & 1, abort_flag, p.status, 4)) {
+                    ok = false;
+                    break;
+                }
+                fence_after_sync();
+                float v[COUT];
+                const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * ACC_COLS);
+#pragma unroll
+                for (int cc = 0; cc < COUT; cc += 16) tmem_ld16(ta + cc, v + cc);
+                tmem_wait_ld();
+                fence_before_sync();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(acc_empty + 8u * b);
+                const int x = k.x0 + q * 32 + lane;
+                if (x >= p.w) continue;
+                const size_t plane = (size_t)p.h * p.w;
+                const size_t pix = (size_t)y * p.w + x;
+#pragma unroll
+                for (int i = 0; i < COUT; ++i) {
+                    v[i] += bias[i];
+                    if (p.relu) v[i] = fmaxf(v[i], 0.0f);
+                }
+                if (p.y) {
+                    uint4 *dst = reinterpret_cast<uint4 *>(p.y) + (size_t)k.img * (COUT / 8) * plane + pix;
+#pragma unroll
+                    for (int i = 0; i < COUT / 8; ++i)
+                        dst[i * plane] = make_uint4(pack_bf16(v[8 * i], v[8 * i + 1]), pack_bf16(v[8 * i + 2], v[8 * i + 3]),
+                                                    pack_bf16(v[8 * i + 4], v[8 * i + 5]), pack_bf16(v[8 * i + 6], v[8 * i + 7]));
+                }
+                if (p.y0) {
+                    const size_t o = (size_t)k.img * plane + pix;
+                    p.y0[o] = v[0] + (p.resid ? p.resid[o] : 0.0f);
+                }
+            }
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 2) {
+        fence_after_sync();
+        tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+// x0 [n][2][h][w][8]: block 0 = (noisy, sigma / 255 * level_scale, 0 x 6), block 1 = 0
+__global__ void pack_input_blocked(const float *noisy, const float *sigma, int n, int h, int w, float level_scale,
+                                   __nv_bfloat16 *x0) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long plane = (long long)h * w;
+    if (i >= n * plane) return;
+    const long long img = i / plane, pix = i - img * plane;
+    uint4 *o = reinterpret_cast<uint4 *>(x0) + img * 2 * plane + pix;
+    o[0] = make_uint4(pack_bf16(noisy[i], sigma[img] * (1.0f / 255.0f) * level_scale), 0u, 0u, 0u);
+    o[plane] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+}  // namespace pilot_tc
+
+// ---- launcher ----------------------------------------------------------------------
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(f);
+    }
+    return fn;
+}
+
+template <int CIN, int COUT>
+static cudaError_t conv_tc_t(const void *x, pilot_tc::Args a, cudaStream_t st) {
+    using S = pilot_tc::Shape<CIN, COUT>;
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return cudaErrorNotSupported;
+    // channel-blocked input as a 4-D tensor (channel in block, x, y, image * CIN / 8 + block);
+    // box = 8 channels x 130 pixels = 2080 contiguous bytes
+    CUtensorMap map;
+    const cuuint64_t dims[4] = {8, (cuuint64_t)a.w, (cuuint64_t)a.h, (cuuint64_t)a.n * (CIN / 8)};
+    const cuuint64_t strides[3] = {16, (cuuint64_t)a.w * 16, (cuuint64_t)a.h * a.w * 16};
+    const cuuint32_t box[4] = {8, (cuuint32_t)pilot_tc::HALO, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(x), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaErrorInvalidValue;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    a.strips = (a.w + pilot_tc::TILE - 1) / pilot_tc::TILE;
+    // CTAS_PER_SM CTAs per SM, at least 4 tiles each
+    const long long tiles = (long long)a.n * a.strips * a.h;
+    const long long want = (tiles + 3) / 4, slots = (long long)pilot_tc::CTAS_PER_SM * sms;
+    const int grid = (int)(want < slots ? want : slots);
+    auto k = pilot_tc::conv3x3_tc<CIN, COUT>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM);
+    if (e != cudaSuccess) return e;
+    k<<<grid, pilot_tc::THREADS, S::SMEM, st>>>(map, a);
+    return cudaGetLastError();
+}
+
+}  // namespace zb
+
+// ---- C ABI (include/zb3d.h) ---------------------------------------------------------
+
+extern "C" int zb3d_pilot_conv3x3_tc(const void *x, int n, int h, int w, int cin, const void *wgt, const float *bias,
+                                     int cout, int relu, void *y, float *y0, const float *resid, int *status,
+                                     void *stream) {
+    if (n <= 0 || h <= 0 || w <= 0) return n == 0 ? 0 : -1;
+    if ((reinterpret_cast<uintptr_t>(x) & 15) || (reinterpret_cast<uintptr_t>(wgt) & 15) ||
+        (reinterpret_cast<uintptr_t>(y) & 15))
+        return -1;
+    zb::pilot_tc::Args a{};
+    a.wgt = static_cast<const __nv_bfloat16 *>(wgt);
+    a.bias = bias;
+    a.y = static_cast<__nv_bfloat16 *>(y);
+    a.y0 = y0;
+    a.resid = resid;
+    a.n = n;
+    a.h = h;
+    a.w = w;
+    a.relu = relu;
+    a.status = status;
+    cudaError_t e = cudaErrorInvalidValue;
+    const cudaStream_t st = (cudaStream_t)stream;
+    if (cin == 16 && cout == 48) e = zb::conv_tc_t<16, 48>(x, a, st);
+    else if (cin == 48 && cout == 48) e = zb::conv_tc_t<48, 48>(x, a, st);
+    else if (cin == 48 && cout == 16) e = zb::conv_tc_t<48, 16>(x, a, st);
+    else if (cin == 16 && cout == 32) e = zb::conv_tc_t<16, 32>(x, a, st);
+    else if (cin == 32 && cout == 32) e = zb::conv_tc_t<32, 32>(x, a, st);
+    else if (cin == 32 && cout == 16) e = zb::conv_tc_t<32, 16>(x, a, st);
+    return e == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int zb3d_pilot_pack_input_blocked(const float *noisy, const float *sigma, int n, int h, int w,
+                                             float level_scale, void *x0, void *stream) {
+    const long long np = (long long)n * h * w;
+    if (np <= 0) return np == 0 ? 0 : -1;
+    zb::pilot_tc::pack_input_blocked<<<(unsigned)((np + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        noisy, sigma, n, h, w, level_scale, static_cast<__nv_bfloat16 *>(x0));
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}

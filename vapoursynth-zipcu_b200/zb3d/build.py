@@ -27,6 +27,7 @@ UNITS = [
     ("zb3d_match_tc.cu", ARCH + ["-use_fast_math"]),
     ("zb3d_vagg.cu", ARCH),
     ("zb3d_pilot.cu", ARCH),
+    ("zb3d_pilot_tc.cu", ARCH),
     ("zb3d_host.cpp", ARCH),
     ("zb3d_noalloc.cu", ARCH),
 ]

@@ -2,11 +2,12 @@
 
 BM3Dv2's second pass (Wiener) matches blocks on, and takes its empirical Wiener
 coefficients from, a reference clip: normally the step-1 hard-threshold estimate.
-The pilot produces that reference with 10 layers of 3x3 convolutions (48 channels,
-ReLU, a noise-level input plane; output added to the noisy plane).  It is trained
+The pilot produces that reference with a stack of 3x3 convolutions (32 or 48
+channels, ReLU, a noise-level input plane; output added to the noisy plane).  It is trained
 only on pairs (noisy synthetic frame, plain BM3D step-1 output of it), on the GPU,
 by the project's own kernels (csrc/zb3d_pilot.cu: BF16 operands, FP32
-accumulation).  Its forward and backward passes are checked against the numpy
+accumulation); inference runs on the tensor cores (csrc/zb3d_pilot_tc.cu: tcgen05.mma
+with the accumulator in tensor memory, TMA-staged input rows).  Its forward and backward passes are checked against the numpy
 oracle (oracle/pilot_oracle.py).  Step 2 keeps exact block matching; the plain
 two-pass form remains the fallback: `PilotGate` accepts the pilot for a noise level
 only where its two-pass PSNR is within 0.05 dB of the plain two-pass PSNR on
@@ -26,7 +27,14 @@ import numpy as np
 from . import _native as N
 from . import synth
 
-SHAPES = [(16, 48)] + [(48, 48)] * 8 + [(48, 16)]  # (cin, cout) of the 10 layers, channels padded to 16
+
+
+def arch(width: int = 48, layers: int = 10) -> list:
+    """(cin, cout) of each layer; the 2 input and 1 output channels are padded to 16."""
+    return [(16, width)] + [(width, width)] * (layers - 2) + [(width, 16)]
+
+
+SHAPES = arch(48, 10)                                # the default architecture
 REAL_IN, REAL_OUT = 2, 1
 LEVEL_SCALE = 4.0                                    # noise-level plane = sigma / 255 * LEVEL_SCALE
 LOSS_SCALE = 1024.0                                  # keeps BF16 gradients clear of underflow
@@ -44,15 +52,17 @@ def _ok(rc: int, what: str):
 class PilotNet:
     """The network, its FP32 master weights and Adam state, on one CUDA device."""
 
-    def __init__(self, seed: int = 0, device: str = "cuda"):
+    def __init__(self, seed: int = 0, device: str = "cuda", width: int = 48, layers: int = 10):
         import torch
         self.torch, self.dev = torch, device
+        self.width, self.layers = width, layers
+        self.shapes = arch(width, layers)
         rng = np.random.default_rng(seed)
         self.w32, self.b32, self.keep = [], [], []
-        for l, (cin, cout) in enumerate(SHAPES):
+        for l, (cin, cout) in enumerate(self.shapes):
             rin = REAL_IN if l == 0 else cin
-            rout = REAL_OUT if l == len(SHAPES) - 1 else cout
-            std = math.sqrt(2.0 / (9 * rin)) * (0.1 if l == len(SHAPES) - 1 else 1.0)
+            rout = REAL_OUT if l == len(self.shapes) - 1 else cout
+            std = math.sqrt(2.0 / (9 * rin)) * (0.1 if l == len(self.shapes) - 1 else 1.0)
             w = np.zeros((cout, 3, 3, cin), np.float32)
             w[:rout, :, :, :rin] = rng.normal(0.0, std, size=(rout, 3, 3, rin))
             k = np.zeros_like(w)
@@ -63,7 +73,7 @@ class PilotNet:
             self.b32.append(torch.zeros(cout, dtype=torch.float32, device=device))
             self.keep.append((torch.from_numpy(k).to(device), torch.from_numpy(kb).to(device)))
         self.w16 = [torch.empty(w.shape, dtype=torch.bfloat16, device=device) for w in self.w32]
-        self.wt16 = [torch.empty((cin, 3, 3, cout), dtype=torch.bfloat16, device=device) for cin, cout in SHAPES]
+        self.wt16 = [torch.empty((cin, 3, 3, cout), dtype=torch.bfloat16, device=device) for cin, cout in self.shapes]
         self.m = [(torch.zeros_like(w), torch.zeros_like(b)) for w, b in zip(self.w32, self.b32)]
         self.v = [(torch.zeros_like(w), torch.zeros_like(b)) for w, b in zip(self.w32, self.b32)]
         self.step_count = 0
@@ -72,20 +82,20 @@ class PilotNet:
     # -- weights ---------------------------------------------------------------------
     def _refresh(self):
         lib = N.lib()
-        for l, (cin, cout) in enumerate(SHAPES):
+        for l, (cin, cout) in enumerate(self.shapes):
             _ok(lib.zb3d_pilot_to_bf16(_p(self.w32[l]), self.w32[l].numel(), _p(self.w16[l]), None), "to_bf16")
             _ok(lib.zb3d_pilot_flip_weights(_p(self.w16[l]), cin, cout, _p(self.wt16[l]), None), "flip")
 
     def state(self) -> dict:
-        out = {}
-        for l in range(len(SHAPES)):
+        out = {"arch": np.array([self.width, self.layers], np.int32)}
+        for l in range(len(self.shapes)):
             out[f"w{l}"] = self.w32[l].cpu().numpy()
             out[f"b{l}"] = self.b32[l].cpu().numpy()
         return out
 
     def load_state(self, st: dict):
         torch = self.torch
-        for l in range(len(SHAPES)):
+        for l in range(len(self.shapes)):
             self.w32[l].copy_(torch.from_numpy(np.asarray(st[f"w{l}"], np.float32)))
             self.b32[l].copy_(torch.from_numpy(np.asarray(st[f"b{l}"], np.float32)))
         self._refresh()
@@ -95,36 +105,56 @@ class PilotNet:
 
     @classmethod
     def load(cls, path: str, device: str = "cuda") -> "PilotNet":
-        net = cls(device=device)
         with np.load(path) as f:
-            net.load_state({k: f[k] for k in f.files})
+            st = {k: f[k] for k in f.files}
+        width, layers = (int(v) for v in st.get("arch", (48, 10)))
+        net = cls(device=device, width=width, layers=layers)
+        net.load_state(st)
         return net
 
     # -- passes ------------------------------------------------------------------------
-    def forward(self, noisy, sigma, keep_acts: bool = False, out=None, stream=None):
+    def forward(self, noisy, sigma, keep_acts: bool = False, out=None, stream=None, tc: Optional[bool] = None):
         """noisy: float32 [n][h][w] device tensor, sigma: float32 [n] (8-bit scale).
         Returns y = noisy + net output (float32 [n][h][w], written to `out` if given)
-        and, with keep_acts, the stored BF16 activations of every layer's input.
-        `stream`: a CUDA stream handle (int) for every launch, or None for the default."""
+        and, with keep_acts, the stored BF16 activations of every layer's input (NHWC, or
+        channel-blocked [n][c/8][h][w][8] with tc).
+        `stream`: a CUDA stream handle (int) for every launch, or None for the default.
+        tc: convolutions on the tensor cores (tcgen05); default for inference (no keep_acts),
+        while the training passes keep the mma.sync kernels their gradients are checked with."""
         torch, lib = self.torch, N.lib()
+        if tc is None:
+            tc = not keep_acts
         n, h, w = noisy.shape
-        x = torch.empty((n, h, w, 16), dtype=torch.bfloat16, device=self.dev)
-        _ok(lib.zb3d_pilot_pack_input(_p(noisy), _p(sigma), n, h, w, LEVEL_SCALE, _p(x), stream), "pack_input")
+
+        def act(c):  # NHWC for the mma.sync kernels, channel-blocked [n][c/8][h][w][8] for tcgen05
+            shape = (n, c // 8, h, w, 8) if tc else (n, h, w, c)
+            return torch.empty(shape, dtype=torch.bfloat16, device=self.dev)
+
+        x = act(16)
+        pack = lib.zb3d_pilot_pack_input_blocked if tc else lib.zb3d_pilot_pack_input
+        _ok(pack(_p(noisy), _p(sigma), n, h, w, LEVEL_SCALE, _p(x), stream), "pack_input")
         acts = [x]
         y = out if out is not None else torch.empty((n, h, w), dtype=torch.float32, device=self.dev)
-        last = len(SHAPES) - 1
-        for l, (cin, cout) in enumerate(SHAPES):
+        last = len(self.shapes) - 1
+
+        def conv(x_, l, relu, a_, y0_, resid_):
+            cin, cout = self.shapes[l]
+            if tc:
+                return lib.zb3d_pilot_conv3x3_tc(_p(x_), n, h, w, cin, _p(self.w16[l]), _p(self.b32[l]), cout, relu,
+                                                 _p(a_), _p(y0_), _p(resid_), None, stream)
+            return lib.zb3d_pilot_conv3x3(_p(x_), n, h, w, cin, _p(self.w16[l]), _p(self.b32[l]), cout, relu,
+                                          None, _p(a_), _p(y0_), _p(resid_), stream)
+
+        for l, (cin, cout) in enumerate(self.shapes):
             if l < last:
-                a = torch.empty((n, h, w, cout), dtype=torch.bfloat16, device=self.dev)
-                _ok(lib.zb3d_pilot_conv3x3(_p(acts[-1]), n, h, w, cin, _p(self.w16[l]), _p(self.b32[l]), cout, 1,
-                                           None, _p(a), None, None, stream), f"conv {l}")
+                a = act(cout)
+                _ok(conv(acts[-1], l, 1, a, None, None), f"conv {l}")
                 if keep_acts:
                     acts.append(a)
                 else:
                     acts = [a]
             else:
-                _ok(lib.zb3d_pilot_conv3x3(_p(acts[-1]), n, h, w, cin, _p(self.w16[l]), _p(self.b32[l]), cout, 0,
-                                           None, None, _p(y), _p(noisy), stream), "conv out")
+                _ok(conv(acts[-1], l, 0, None, y, noisy), "conv out")
         return y, (acts if keep_acts else None)
 
     def gradients(self, noisy, target, sigma):
@@ -137,8 +167,8 @@ class PilotNet:
         _ok(lib.zb3d_pilot_mse_grad(_p(y), _p(target), y.numel(), LOSS_SCALE, _p(d), _p(loss), None), "mse_grad")
         dws = [torch.zeros_like(wt) for wt in self.w32]
         dbs = [torch.zeros_like(b) for b in self.b32]
-        for l in range(len(SHAPES) - 1, -1, -1):
-            cin, cout = SHAPES[l]
+        for l in range(len(self.shapes) - 1, -1, -1):
+            cin, cout = self.shapes[l]
             _ok(lib.zb3d_pilot_conv3x3_wgrad(_p(acts[l]), _p(d), n, h, w, cin, cout, _p(dws[l]), _p(dbs[l]), None),
                 f"wgrad {l}")
             if l == 0:
@@ -155,12 +185,12 @@ class PilotNet:
         lib = N.lib()
         dws, dbs, loss, _ = self.gradients(noisy, target, sigma)
         self.step_count += 1
-        for l in range(len(SHAPES)):
+        for l in range(len(self.shapes)):
             for p, g, m, v, k, w16 in ((self.w32[l], dws[l], self.m[l][0], self.v[l][0], self.keep[l][0], self.w16[l]),
                                        (self.b32[l], dbs[l], self.m[l][1], self.v[l][1], self.keep[l][1], None)):
                 _ok(lib.zb3d_pilot_adam(_p(p), _p(m), _p(v), _p(g), p.numel(), lr, 0.9, 0.999, 1e-8,
                                         self.step_count, LOSS_SCALE, _p(k), _p(w16), None), "adam")
-        for l, (cin, cout) in enumerate(SHAPES):
+        for l, (cin, cout) in enumerate(self.shapes):
             _ok(lib.zb3d_pilot_flip_weights(_p(self.w16[l]), cin, cout, _p(self.wt16[l]), None), "flip")
         return loss
 
@@ -312,6 +342,8 @@ def main(argv=None):
     ap.add_argument("--dims", default="1920x1080,960x540", help="training frame sizes (the 1080p YUV420 planes)")
     ap.add_argument("--steps", type=int, default=6250, help="Adam steps of 32 crops (6250 = 200k crops)")
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--width", type=int, default=48, help="channels of the hidden layers (32 or 48)")
+    ap.add_argument("--layers", type=int, default=10, help="number of 3x3 convolutions")
     ap.add_argument("--out", default=WEIGHTS)
     a = ap.parse_args(argv)
     import time
@@ -323,7 +355,7 @@ def main(argv=None):
             nz, tg, _, sg = make_pairs(a.frames, (wd, ht), TRAIN_SIGMAS, seed=11 + k, **TRAIN_KW)
             noisy, target, sig = noisy + nz, target + tg, sig + sg
         print(f"{len(noisy)} training pairs ({a.dims}, step 1 with {TRAIN_KW}) in {time.time() - t0:.1f} s")
-        net = PilotNet(seed=0)
+        net = PilotNet(seed=0, width=a.width, layers=a.layers)
         t0 = time.time()
         hist = train(net, noisy, target, sig, steps=a.steps, batch=32, crop=64, lr=a.lr, seed=5)
         net.torch.cuda.synchronize()

@@ -28,6 +28,7 @@ import statistics
 import sys
 import threading
 import time
+from typing import Optional
 from concurrent.futures import ThreadPoolExecutor
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -209,22 +210,25 @@ class DevicePipeline:
             f.close()
 
 
-def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frames: int = 4):
+def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frames: int = 4, nstreams: int = 4,
+                   weights: Optional[str] = None):
     """Two-pass BM3Dv2 with the learned pilot (zb3d/pilot.py, shipped weights) as the
     step-2 reference in place of the step-1 estimate, on the same frames: device-resident
-    Mpix/s, and PSNR against the clean frames next to the plain two-pass form."""
+    Mpix/s, and PSNR against the clean frames next to the plain two-pass form.  Frames
+    run on `nstreams` streams, each with its own step-2 filter and pilot buffers."""
     from zb3d import _native as N
     from zb3d import pilot as P
     from zb3d import synth
     from zb3d.device import DeviceFilter
-    net = P.shipped()
-    final = DeviceFilter(W, H, family=N.YUV, subsampling=(1, 1), num_streams=1, ref=True, **KW)
+    net = P.PilotNet.load(weights) if weights else P.shipped()
+    finals = [DeviceFilter(W, H, family=N.YUV, subsampling=(1, 1), num_streams=1, ref=True, **KW)
+              for _ in range(nstreams)]
     basic = DeviceFilter(W, H, family=N.YUV, subsampling=(1, 1), num_streams=1, **KW)
-    lay = final.entries
+    lay = finals[0].entries
     assert all(l.pitch == l.width for l in lay), "dense planes expected"
     sig = torch.full((1,), SIGMA, dtype=torch.float32, device="cuda")
     nf = len(frames)
-    bufs, outs = [], []
+    bufs, outs = [], []  # per frame and plane: [reference | noisy] (the step-2 filter's input) and the output
     for i in range(nf):
         fb, fo = [], []
         for e, l in enumerate(lay):
@@ -235,12 +239,12 @@ def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frame
             fo.append(torch.empty(pe, dtype=torch.float32, device="cuda"))
         bufs.append(fb)
         outs.append(fo)
+    streams = [torch.cuda.Stream() for _ in range(nstreams)]
 
-    stream = torch.cuda.Stream()  # one stream for every launch: step 2 must follow its reference
-    st = stream.cuda_stream
-
-    def frame(i, use_pilot=True):
-        with torch.cuda.stream(stream):
+    def frame(i, k=0, use_pilot=True):
+        s = streams[k]
+        st = s.cuda_stream
+        with torch.cuda.stream(s):
             for e, l in enumerate(lay):
                 b, pe = bufs[i][e], l.height * l.pitch
                 if use_pilot:
@@ -248,7 +252,7 @@ def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frame
                                 stream=st)
                 else:
                     basic.run_entry(e, b.data_ptr() + 4 * pe, b.data_ptr(), st)
-                final.run_entry(e, b.data_ptr(), outs[i][e].data_ptr(), st)
+                finals[k].run_entry(e, b.data_ptr(), outs[i][e].data_ptr(), st)
 
     def psnrs(i):
         return [synth.psnr(outs[i][e].view(l.height, l.width).cpu().numpy(),
@@ -262,26 +266,35 @@ def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frame
         frame(i, use_pilot=True)
         torch.cuda.synchronize()
         piloted.append(psnrs(i))
-    for j in range(warmup):
-        frame(j % nf)
+    for j in range(max(warmup, nstreams)):
+        frame(j % nf, j % nstreams)
     torch.cuda.synchronize()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t0.record(stream)
+    s0 = streams[0]
+    t0.record(s0)
+    for s in streams[1:]:
+        s.wait_event(t0)
     for j in range(steps * BATCH):
-        frame(j % nf)
-    t1.record(stream)
+        frame(j % nf, j % nstreams)
+    for s in streams[1:]:
+        ev = torch.cuda.Event()
+        ev.record(s)
+        s0.wait_event(ev)
+    t1.record(s0)
     t1.synchronize()
     ms = t0.elapsed_time(t1)
     plain, piloted = np.array(plain), np.array(piloted)
     delta = float(np.mean(piloted - plain))
-    final.close()
+    for f in finals:
+        f.close()
     basic.close()
     return {"value": W * H * steps * BATCH / (ms / 1e3) / 1e6, "unit": "Mpix/s", "ms_per_frame": ms / (steps * BATCH),
             "psnr_plain_two_pass_db": float(np.mean(plain)), "psnr_pilot_two_pass_db": float(np.mean(piloted)),
             "delta_psnr_db": delta, "delta_psnr_db_per_plane": [float(d) for d in np.mean(piloted - plain, 0)],
-            "within_0_05_db": delta >= -0.05,
-            "what": "pilot (10 x conv3x3, 48 ch, BF16 mma.sync kernels, FP32 accumulation) as step 1 on every plane, "
-                    "then the exact step 2; PSNR over the first %d frames against the clean frames" % min(psnr_frames, nf)}
+            "within_0_05_db": delta >= -0.05, "streams": nstreams,
+            "what": "pilot (%d x conv3x3, %d ch, BF16 tcgen05 kernels, FP32 accumulation in tensor memory) as step 1 "
+                    "on every plane, then the exact step 2; PSNR over the first %d frames against the clean frames"
+                    % (net.layers, net.width, min(psnr_frames, nf))}
 
 
 def run_e2e(frames, steps: int, warmup: int, num_streams: int = 4):
@@ -641,6 +654,7 @@ def main():
     ap.add_argument("--no-ref-cuda", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other block-matching form")
     ap.add_argument("--no-pilot", action="store_true", help="skip the learned-pilot form")
+    ap.add_argument("--pilot-weights", default=None, help="pilot weights (.npz) instead of the shipped ones")
     ap.add_argument("--streams", type=int, default=4, help="CUDA streams the device pipeline spreads frames over")
     ap.add_argument("--match-form", type=int, choices=[-1, 0, 1], default=-1,
                     help="block matching: -1 = the library's autotuned choice per plane, 0 = FP32 scan of every "
@@ -774,7 +788,8 @@ def main():
         if pipe is not None:
             pipe.close()
             pipe = None
-        out["pilot_form"] = run_pilot_form(torch, frames, rank, max(1, args.steps // 4), 1)
+        out["pilot_form"] = run_pilot_form(torch, frames, rank, max(1, args.steps // 4), 1,
+                                           weights=args.pilot_weights)
     if rank == 0 and not args.no_ref_cuda:
         rms = run_ref_cuda(torch, frames, args.steps, args.warmup)
         if rms:

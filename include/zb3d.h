@@ -279,7 +279,7 @@ void zb3d_host_free(void *p);
 /* y = conv3x3(x) + bias (may be NULL), ReLU if relu, zeroed where mask (NHWC, cout
  * channels, may be NULL) is <= 0; y (may be NULL) BF16 NHWC; y0 (may be NULL) the
  * FP32 channel 0 plus resid (may be NULL).  (cin, cout) in {(16,48), (48,48), (48,16), (16,32),
- * (32,32), (32,16)}.  mma.sync BF16 tiles of 8 x 16 pixels; the training passes use it. */
+ * (32,32), (32,16), (16,16)}.  mma.sync BF16 tiles of 8 x 16 pixels; the training passes use it. */
 int zb3d_pilot_conv3x3(const void *x, int n, int h, int w, int cin, const void *wgt, const float *bias, int cout,
                        int relu, const void *mask, void *y, float *y0, const float *resid, void *stream);
 /* The same forward convolution (no mask) on the tensor cores, for inference: tcgen05.mma

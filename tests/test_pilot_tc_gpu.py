@@ -18,7 +18,7 @@ from zb3d import pilot as P
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(16, 48), (48, 48), (48, 16), (16, 32), (32, 32), (32, 16)]
+SHAPES = [(16, 48), (48, 48), (48, 16), (16, 32), (32, 32), (32, 16), (16, 16)]
 SIZES = [(1, 9, 20), (2, 37, 150), (1, 70, 384), (3, 16, 257)]
 ULP = 2.0 ** -7  # one BF16 rounding step, relative to the value (2^-8 .. 2^-7)
 
@@ -115,7 +115,7 @@ def test_tc_last_layer_fp32_output_and_residual():
         assert np.abs(o - ref).max() < 1e-5 * max(1.0, np.abs(ref).max())
 
 
-@pytest.mark.parametrize("width,layers", [(48, 10), (32, 8)])
+@pytest.mark.parametrize("width,layers", [(48, 10), (32, 8), (16, 8)])
 def test_tc_network_forward_matches_mma_sync(width, layers):
     import torch
     net = P.PilotNet(seed=2, width=width, layers=layers)

@@ -1,7 +1,7 @@
 // Learned pilot: kernels of a small residual convolutional network that stands in
 // for the BM3D step-1 (hard-threshold) estimate as the reference of step 2.
 //
-// Network: 3x3 convolutions, 32 or 48 channels, ReLU after all but the last; the
+// Network: 3x3 convolutions, 16, 32 or 48 channels, ReLU after all but the last; the
 // input is the noisy plane plus a noise-level plane, the output (channel 0 of the
 // last layer) is added to the noisy plane.  Weights and activations are BF16,
 // every product is accumulated in FP32 (mma.sync m16n8k16 BF16 -> FP32).
@@ -357,6 +357,7 @@ cudaError_t pilot_conv(int cin, int cout, const pilot::ConvArgs &a, cudaStream_t
     if (cin == 16 && cout == 32) return conv_t<16, 32>(a, st);
     if (cin == 32 && cout == 32) return conv_t<32, 32>(a, st);
     if (cin == 32 && cout == 16) return conv_t<32, 16>(a, st);
+    if (cin == 16 && cout == 16) return conv_t<16, 16>(a, st);
     return cudaErrorInvalidValue;
 }
 
@@ -367,6 +368,7 @@ cudaError_t pilot_wgrad(int cin, int cout, const pilot::WgradArgs &a, cudaStream
     if (cin == 16 && cout == 32) return wgrad_t<16, 32>(a, st);
     if (cin == 32 && cout == 32) return wgrad_t<32, 32>(a, st);
     if (cin == 32 && cout == 16) return wgrad_t<32, 16>(a, st);
+    if (cin == 16 && cout == 16) return wgrad_t<16, 16>(a, st);
     return cudaErrorInvalidValue;
 }
 

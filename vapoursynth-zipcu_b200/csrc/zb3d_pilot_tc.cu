@@ -1,33 +1,45 @@
 // Learned pilot: inference convolution on the 5th-generation tensor cores.
 //
-// y = conv3x3(x) + bias (ReLU) as an implicit GEMM per tile of 128 consecutive
-// pixels of one image row: D[128 x COUT] = sum over the 9 taps and CIN / 16
-// K-steps of A[128 x 16] . B[16 x COUT], BF16 operands in shared memory, FP32
-// accumulator in tensor memory (tcgen05.mma kind::f16, M = 128, N = COUT).
+// y = conv3x3(x) + bias (ReLU), BF16 operands in shared memory, FP32 accumulators
+// in tensor memory (tcgen05.mma kind::f16, M = 128 pixels of one image row).
 //
 // Activations use the channel-blocked layout [n][C / 8][h][w][8] (BF16): one
 // channel block of an image row is a contiguous run of 16-byte pixels.
 //
-// No im2col: a CTA walks down strips of 128 columns and TMA stages every input
-// row it needs once (130 pixels with the halo, zero-filled outside the image)
-// into a ring of row slots laid out [channel block][pixel][8 channels], one
-// contiguous 2080-byte box per channel block.  In that layout the A operand of
-// tap (ky, kx), K-step s, is the canonical no-swizzle K-major matrix that starts
-// at pixel kx of the slot holding input row y + ky - 1, channel block 2 s: 8-pixel core matrices 128 bytes apart (SBO) and
-// the two 8-channel halves one channel block apart (LBO).  The weights stay in
-// shared memory for the CTA's lifetime as [tap][channel block][cout][8].
+// Row-stationary implicit GEMM, no im2col.  A CTA walks down strips of 128
+// columns; TMA stages each input row once (130 pixels with the halo, zero-filled
+// outside the image) into a ring of row slots laid out [channel block][pixel][8].
+// When the width is a multiple of 8 a box is 18 lines of 128 bytes (8-pixel
+// groups from x0 - 8, so the halo pixel x0 - 1 sits at slot pixel 7); otherwise
+// 130 lines of one 16-byte pixel from x0 - 1, which keeps the zero fill exact at a
+// ragged right edge.  In that layout the pixels x + kx - 1 of channel block 2 s form the canonical
+// no-swizzle K-major A operand (8-pixel core matrices 128 bytes apart = SBO, the
+// two 8-channel halves one channel block apart = LBO).  Input row r feeds output
+// rows r + 1, r and r - 1 through the kernel rows ky = 0, 1, 2, so B stacks the
+// three ky weight blocks (N = 3 COUT) and one MMA per (kx, K-step) adds row r's
+// share into the accumulators of all three output rows at once: each staged row
+// is read 3 x CIN / 16 times as an operand instead of 9 x CIN / 16, and is free
+// again as soon as its own MMAs complete.  For that the accumulators of
+// consecutive output rows sit next to each other in tensor memory, in descending
+// order (a ring of K slots; where the ring wraps, the MMA splits in two).  The
+// first contribution to an accumulator (kx = 0, K-step 0 of the row that first
+// touches it) is a separate MMA that overwrites instead of adding, so nothing
+// has to clear tensor memory.
+// A run of n output rows takes n + 2 input rows and n + 4 accumulators (the 4 at
+// its ends only collect halo contributions and are discarded).
 //
 // Two CTAs per SM, each owning a contiguous range of tiles in (image, strip, row)
 // order (balanced to one tile).  The row ring fills the shared memory the weights
-// leave (up to 16 slots), so TMA keeps RING - 3 rows in flight ahead of the MMAs.
+// leave (up to 16 slots).
 //
-// Roles (256 threads): warp 0 lane 0 issues the TMA row loads, warp 1 lane 0
-// issues the MMAs, warp 2 owns the tensor-memory allocation, warps 4-7 (one per
-// 32-lane quarter of tensor memory) drain the 4 accumulator buffers: bias,
-// ReLU, BF16 store (16 bytes per channel block, 512 contiguous bytes per warp),
-// or for the last layer channel 0 plus the residual in FP32.  mbarriers link the
-// roles; every wait is bounded, and a timeout sets the status word and ends every
-// role early.
+// Roles (384 threads): warp 0 lane 0 issues the TMA row loads, warp 1 lane 0
+// issues the MMAs, warp 2 owns the tensor-memory allocation, and two quads of
+// epilogue warps (4-7 and 8-11, warp w on the 32-lane quarter w % 4 of tensor
+// memory) take the accumulators in turn, so that one quad's tensor-memory loads
+// and stores overlap the other's: bias, ReLU, BF16 store
+// (16 bytes per channel block, 512 contiguous bytes per warp), or for the last
+// layer channel 0 plus the residual in FP32.  mbarriers link the roles; every wait
+// is bounded, and a timeout sets the status word and ends every role early.
 //
 // Same arithmetic as the mma.sync kernel in zb3d_pilot.cu (BF16 products, FP32
 // sums, bias then ReLU then one BF16 rounding); only the summation order differs.
@@ -41,16 +53,15 @@ namespace zb {
 namespace pilot_tc {
 
 constexpr int TILE = 128;                // output pixels per tile (MMA M)
-constexpr int HALO = TILE + 2;           // staged input pixels per row
-constexpr int BOX_BYTES = HALO * 16;     // one channel block of a staged row (TMA box 8 x 130)
-constexpr int CB_BYTES = 2176;           // ... padded to a multiple of 128 bytes
+constexpr int BOX_PIX = 130;             // TMA box of 130 single pixels (any width)
+constexpr int BOX_GROUPS = 18;           // TMA box of 18 groups of 8 pixels (width a multiple of 8)
+constexpr int CB_BYTES = BOX_GROUPS * 128;  // one channel block of a staged row (2304 bytes)
 constexpr int MAX_RING = 16;             // staged input row slots, at most
 constexpr int CTAS_PER_SM = 2;           // two independent pipelines per SM
 constexpr int SMEM_BUDGET = 112 * 1024;  // shared memory of the ring and the weights, per CTA
-constexpr int NACC = 4;                  // accumulator buffers
-constexpr int ACC_COLS = 64;             // tensor-memory columns per accumulator buffer
-constexpr int TMEM_COLS = NACC * ACC_COLS;
-constexpr int THREADS = 256;
+constexpr int TMEM_COLS = 512 / CTAS_PER_SM;  // accumulator ring of each CTA
+constexpr int EPI_GROUPS = 2;            // epilogue warp quads, taking accumulators in turn
+constexpr int THREADS = 128 + 128 * EPI_GROUPS;
 constexpr unsigned WAIT_LIMIT = 1u << 20;  // try_wait rounds on an mbarrier before giving up (about a second)
 
 struct Args {
@@ -61,13 +72,16 @@ struct Args {
     const float *resid;        // [n][h][w] or null
     int n, h, w, relu;
     int strips;                // ceil(w / 128)
+    int grouped;               // boxes of 8-pixel groups (w % 8 == 0), else of single pixels
     int *status;               // set non-zero when a wait timed out (may be null)
 };
 
 template <int CIN, int COUT>
 struct Shape {
-    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= ACC_COLS, "unsupported layer shape");
+    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && 3 * COUT <= 256, "unsupported layer shape");
     static constexpr int CB = CIN / 8;
+    static constexpr int NACC = TMEM_COLS / COUT;  // accumulator slots
+    static_assert(NACC >= 5, "accumulator ring too small");
     static constexpr int KSTEPS = CIN / 16;
     static constexpr int ROW_BYTES = CB * CB_BYTES;
     static constexpr int W_BYTES = 9 * CB * COUT * 16;
@@ -78,12 +92,16 @@ struct Shape {
     static constexpr int OFF_BAR = OFF_W + W_BYTES;
     static constexpr int NBAR = 2 * RING + 2 * NACC + 1;  // row_full, row_free, acc_full, acc_empty, drain
     static constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
-    static constexpr int SMEM = OFF_MISC + 16 + 128;  // tensor-memory address, abort flag; alignment slack
-    // kind::f16 instruction descriptor: FP32 accumulator (bit 4), BF16 A (bits 7-9 = 1) and
-    // B (bits 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
-    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(COUT >> 3) << 17) |
-                                      ((uint32_t)(TILE >> 4) << 24);
+    static constexpr int OFF_BIAS = OFF_MISC + 16;    // after the tensor-memory address and abort flag
+    static constexpr int SMEM = OFF_BIAS + COUT * 4 + 128;  // + alignment slack
+    static constexpr int B_ROWS = 3 * COUT;          // stacked ky blocks of one (kx, channel block)
 };
+
+// kind::f16 instruction descriptor: FP32 accumulator (bit 4), BF16 A (bits 7-9 = 1) and
+// B (bits 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
+__host__ __device__ constexpr uint32_t idesc_bf16(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TILE >> 4) << 24);
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -214,7 +232,7 @@ __device__ __forceinline__ bool next_seg(const Args &p, long long &t, long long 
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) conv3x3_tc(const __grid_constant__ CUtensorMap xmap, Args p) {
     using S = Shape<CIN, COUT>;
-    constexpr int RING = S::RING;
+    constexpr int RING = S::RING, NACC = S::NACC;
     extern __shared__ uint8_t smraw[];
     const uint32_t raw = smem_u32(smraw);
     const uint32_t pad = ((raw + 127u) & ~127u) - raw;
@@ -222,8 +240,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) conv3x3_tc(const __grid_
     const uint32_t sb = raw + pad;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t bar = sb + S::OFF_BAR;
-    // barrier k lives at bar + 8 k: row_full[s] = s, row_free[s] = RING + s,
-    // acc_full[b] = 2 RING + b, acc_empty[b] = 2 RING + NACC + b, drain = 2 RING + 2 NACC
+    // barriers: row_full[RING], row_free[RING], acc_full[NACC], acc_empty[NACC], drain
     const uint32_t row_full = bar, row_free = bar + 8u * RING;
     const uint32_t acc_full = bar + 8u * (2 * RING), acc_empty = acc_full + 8u * NACC;
     const uint32_t drain = acc_empty + 8u * NACC;
@@ -231,12 +248,18 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) conv3x3_tc(const __grid_
     const long long t_begin = tiles * blockIdx.x / gridDim.x, t_end = tiles * (blockIdx.x + 1) / gridDim.x;
     uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + S::OFF_MISC);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(sm + S::OFF_MISC + 4);
+    // accumulator g (the CTA's running count) lives in slot NACC - 1 - g % NACC: the
+    // slots of consecutive output rows descend, so rows r + 1, r, r - 1 are adjacent
+    auto acc_slot = [](uint32_t g) { return (int)(NACC - 1 - g % NACC); };
 
+    // weights as B operands [kx][channel block][ky][cout][8]: N = 3 COUT rows per (kx, block)
     for (int i = threadIdx.x; i < 9 * S::CB * COUT; i += THREADS) {
-        const int co = i % COUT, rest = i / COUT, cb = rest % S::CB, tap = rest / S::CB;
+        const int co = i % COUT, r1 = i / COUT, ky = r1 % 3, r2 = r1 / 3, cb = r2 % S::CB, kx = r2 / S::CB;
         *reinterpret_cast<uint4 *>(sm + S::OFF_W + 16 * i) =
-            __ldg(reinterpret_cast<const uint4 *>(p.wgt + ((size_t)co * 9 + tap) * CIN + cb * 8));
+            __ldg(reinterpret_cast<const uint4 *>(p.wgt + ((size_t)co * 9 + ky * 3 + kx) * CIN + cb * 8));
     }
+    float *sbias = reinterpret_cast<float *>(sm + S::OFF_BIAS);
+    if (threadIdx.x < COUT) sbias[threadIdx.x] = p.bias ? __ldg(p.bias + threadIdx.x) : 0.0f;
     if (threadIdx.x == 0) {
         for (int s = 0; s < RING; ++s) {
             mbar_init(row_full + 8u * s, 1);
@@ -263,18 +286,20 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) conv3x3_tc(const __grid_
         bool ok = true;
         long long t = t_begin;
         Seg k;
+        const uint32_t box_bytes = p.grouped ? CB_BYTES : BOX_PIX * 16;
         while (ok && next_seg(p, t, t_end, k)) {
+            const int bx = p.grouped ? (k.x0 >> 3) - 1 : k.x0 - 1;  // first 8-pixel group / pixel of the box
             for (int r = k.ya - 1; r <= k.yb; ++r, ++e) {
                 const int s = (int)(e % RING);
                 if (e >= RING && !wait_bar(row_free + 8u * s, ((e / RING) - 1) & 1, abort_flag, p.status, 1)) {
                     ok = false;
                     break;
                 }
-                mbar_arrive_tx(row_full + 8u * s, S::CB * BOX_BYTES);
+                mbar_arrive_tx(row_full + 8u * s, S::CB * box_bytes);
                 const uint32_t dst = sb + s * S::ROW_BYTES;
 #pragma unroll
                 for (int cb = 0; cb < S::CB; ++cb)
-                    tma_row(dst + cb * CB_BYTES, &xmap, 0, k.x0 - 1, r, k.img * S::CB + cb, row_full + 8u * s);
+                    tma_row(dst + cb * CB_BYTES, &xmap, 0, bx, r, k.img * S::CB + cb, row_full + 8u * s);
             }
         }
         if (!ok) {
@@ -285,86 +310,118 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) conv3x3_tc(const __grid_
             }
         }
     } else if (warp == 1 && lane == 0) {
-        // MMA issuer
-        const uint64_t a_desc0 = desc_k(sb, CB_BYTES, 128);
-        const uint64_t b_desc0 = desc_k(sb + S::OFF_W, COUT * 16, 128);
-        uint32_t e = 0, t = 0;
+        // MMA issuer: input row i of a run (global count e) adds into accumulators
+        // g, g + 1, g + 2 (output rows r - 1, r, r + 1), g = run base + i
+        // pixel x0 - 1 sits at slot pixel 7 (group boxes) or 0 (pixel boxes)
+        const uint64_t a_desc0 = desc_k(sb + (p.grouped ? 7 * 16 : 0), CB_BYTES, 128);
+        const uint64_t b_desc0 = desc_k(sb + S::OFF_W, S::B_ROWS * 16, 128);
+        uint32_t e = 0, gbase = 0;
         bool ok = true;
         long long tt = t_begin;
         Seg k;
         while (ok && next_seg(p, tt, t_end, k)) {
-            const uint32_t base = e;
-            for (int y = k.ya; y < k.yb && ok; ++y, ++t) {
-                const uint32_t e0 = base + (uint32_t)(y - k.ya);
-                for (uint32_t q = (y == k.ya ? e0 : e0 + 2); q <= e0 + 2; ++q)
-                    if (!wait_bar(row_full + 8u * (q % RING), (q / RING) & 1, abort_flag, p.status, 2)) {
+            const int n = k.yb - k.ya;
+            for (int i = 0; i <= n + 1 && ok; ++i, ++e) {
+                const uint32_t g = gbase + (uint32_t)i;
+                if (!wait_bar(row_full + 8u * (e % RING), (e / RING) & 1, abort_flag, p.status, 2)) {
+                    ok = false;
+                    break;
+                }
+                // accumulators touched for the first time: g, g + 1, g + 2 at the run's first row, else g + 2
+                for (uint32_t q = (i == 0 ? g : g + 2); q <= g + 2; ++q)
+                    if (q >= (uint32_t)NACC &&
+                        !wait_bar(acc_empty + 8u * acc_slot(q), ((q / NACC) - 1) & 1, abort_flag, p.status, 3)) {
                         ok = false;
                         break;
                     }
-                const int b = (int)(t % NACC);
-                if (ok && t >= NACC && !wait_bar(acc_empty + 8u * b, ((t / NACC) - 1) & 1, abort_flag, p.status, 3))
-                    ok = false;
                 if (!ok) break;
                 fence_after_sync();
-                const uint32_t d = tmem + (uint32_t)(b * ACC_COLS);
-                // descriptors advance by constant offsets (16-byte units in the low bits)
+                const uint64_t arow = a_desc0 + (uint64_t)((e % RING) * (S::ROW_BYTES >> 4));
+                const int s0 = acc_slot(g);  // slot of output row r - 1 (ky = 2)
+                // B rows ky * COUT .. of (kx, K-step): descriptor offsets in 16-byte units
+                constexpr uint64_t KY1 = (COUT * 16) >> 4, KY2 = (2 * COUT * 16) >> 4;
+                const uint32_t d0 = tmem + (uint32_t)(s0 * COUT);
 #pragma unroll
-                for (int ky = 0; ky < 3; ++ky) {
-                    const uint64_t arow = a_desc0 + (uint64_t)(((e0 + ky) % RING) * (S::ROW_BYTES >> 4));
+                for (int kx = 0; kx < 3; ++kx)
 #pragma unroll
-                    for (int kx = 0; kx < 3; ++kx)
-#pragma unroll
-                        for (int ks = 0; ks < S::KSTEPS; ++ks)
-                            mma_bf16(d, arow + (uint64_t)((2 * ks * CB_BYTES + kx * 16) >> 4),
-                                     b_desc0 + (uint64_t)((((ky * 3 + kx) * S::CB + 2 * ks) * COUT * 16) >> 4),
-                                     S::IDESC, (ky | kx | ks) != 0);
-                }
-                mma_commit(acc_full + 8u * b);                  // accumulator ready
-                mma_commit(row_free + 8u * (e0 % RING));        // input row y - 1 no longer needed
-                if (y == k.yb - 1) {
-                    mma_commit(row_free + 8u * ((e0 + 1) % RING));
-                    mma_commit(row_free + 8u * ((e0 + 2) % RING));
+                    for (int ks = 0; ks < S::KSTEPS; ++ks) {
+                        const uint64_t ad = arow + (uint64_t)((2 * ks * CB_BYTES + kx * 16) >> 4);
+                        const uint64_t bd = b_desc0 + (uint64_t)(((kx * S::CB + 2 * ks) * S::B_ROWS * 16) >> 4);
+                        if (kx == 0 && ks == 0 && i > 0) {
+                            // row r + 1's accumulator is fresh: its first product overwrites
+                            const int s2 = s0 >= 2 ? s0 - 2 : s0 + NACC - 2;
+                            mma_bf16(tmem + (uint32_t)(s2 * COUT), ad, bd, idesc_bf16(COUT), 0);
+                            if (s0 >= 1) {  // slots s0 - 1, s0 = rows r, r - 1
+                                mma_bf16(d0 - COUT, ad, bd + KY1, idesc_bf16(2 * COUT), 1);
+                            } else {
+                                mma_bf16(tmem + (uint32_t)((NACC - 1) * COUT), ad, bd + KY1, idesc_bf16(COUT), 1);
+                                mma_bf16(tmem, ad, bd + KY2, idesc_bf16(COUT), 1);
+                            }
+                            continue;
+                        }
+                        // a run's first row: all three accumulators are fresh
+                        const uint32_t acc = (kx == 0 && ks == 0) ? 0u : 1u;
+                        if (s0 >= 2) {  // slots s0 - 2, s0 - 1, s0 = rows r + 1, r, r - 1: one MMA
+                            mma_bf16(d0 - 2 * COUT, ad, bd, idesc_bf16(3 * COUT), acc);
+                        } else if (s0 == 1) {  // slots 0, 1 = rows r, r - 1; slot NACC - 1 = row r + 1
+                            mma_bf16(tmem, ad, bd + KY1, idesc_bf16(2 * COUT), acc);
+                            mma_bf16(tmem + (uint32_t)((NACC - 1) * COUT), ad, bd, idesc_bf16(COUT), acc);
+                        } else {  // slot 0 = row r - 1; slots NACC - 2, NACC - 1 = rows r + 1, r
+                            mma_bf16(tmem, ad, bd + KY2, idesc_bf16(COUT), acc);
+                            mma_bf16(tmem + (uint32_t)((NACC - 2) * COUT), ad, bd, idesc_bf16(2 * COUT), acc);
+                        }
+                    }
+                mma_commit(row_free + 8u * (e % RING));  // the staged row is done
+                mma_commit(acc_full + 8u * acc_slot(g));  // output row r - 1 is complete
+                if (i == n + 1) {                         // the run's last two (halo) accumulators
+                    mma_commit(acc_full + 8u * acc_slot(g + 1));
+                    mma_commit(acc_full + 8u * acc_slot(g + 2));
                 }
             }
-            e = base + (uint32_t)(k.yb - k.ya + 2);
+            gbase += (uint32_t)(n + 4);
         }
         // every MMA issued has completed before the CTA ends
         mma_commit(drain);
         for (unsigned i = 0; i < WAIT_LIMIT && !mbar_test(drain, 0); ++i) {
         }
     } else if (warp >= 4) {
-        // epilogue: warp 4 + q drains tensor-memory lanes 32 q .. 32 q + 31 (pixels of the tile)
-        const int q = warp & 3;
-        float bias[COUT];
-#pragma unroll
-        for (int i = 0; i < COUT; ++i) bias[i] = p.bias ? __ldg(p.bias + i) : 0.0f;
-        uint32_t t = 0;
+        // epilogue: warp w drains tensor-memory lanes 32 (w % 4) .. + 31 (pixels of the tile) of
+        // the accumulators g with g % EPI_GROUPS == its quad
+        const int q = warp & 3, grp = (warp - 4) >> 2;
+        uint32_t g = 0;
         bool ok = true;
         long long tt = t_begin;
         Seg k;
         while (ok && next_seg(p, tt, t_end, k)) {
-            for (int y = k.ya; y < k.yb; ++y, ++t) {
-                const int b = (int)(t % NACC);
-                if (!wait_bar(acc_full + 8u * b, (t / NACC) & 1, abort_flag, p.status, 4)) {
+            const int n = k.yb - k.ya;
+            // accumulator j of the run = output row ya - 2 + j; rows ya .. yb - 1 are real
+            for (int j = 0; j < n + 4; ++j, ++g) {
+                if ((int)(g % EPI_GROUPS) != grp) continue;
+                const int slot = acc_slot(g);
+                if (!wait_bar(acc_full + 8u * slot, (g / NACC) & 1, abort_flag, p.status, 4)) {
                     ok = false;
                     break;
                 }
                 fence_after_sync();
+                const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(slot * COUT);
+                const bool real = j >= 2 && j <= n + 1;
                 float v[COUT];
-                const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * ACC_COLS);
+                if (real) {
 #pragma unroll
-                for (int cc = 0; cc < COUT; cc += 16) tmem_ld16(ta + cc, v + cc);
-                tmem_wait_ld();
+                    for (int cc = 0; cc < COUT; cc += 16) tmem_ld16(ta + cc, v + cc);
+                    tmem_wait_ld();
+                }
                 fence_before_sync();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(acc_empty + 8u * b);
+                if (lane == 0) mbar_arrive(acc_empty + 8u * slot);
                 const int x = k.x0 + q * 32 + lane;
-                if (x >= p.w) continue;
+                if (!real || x >= p.w) continue;
+                const int y = k.ya - 2 + j;
                 const size_t plane = (size_t)p.h * p.w;
                 const size_t pix = (size_t)y * p.w + x;
 #pragma unroll
                 for (int i = 0; i < COUT; ++i) {
-                    v[i] += bias[i];
+                    v[i] += sbias[i];
                     if (p.relu) v[i] = fmaxf(v[i], 0.0f);
                 }
                 if (p.y) {
@@ -426,12 +483,16 @@ static cudaError_t conv_tc_t(const void *x, pilot_tc::Args a, cudaStream_t st) {
     using S = pilot_tc::Shape<CIN, COUT>;
     EncodeTiledFn enc = encode_tiled();
     if (!enc) return cudaErrorNotSupported;
-    // channel-blocked input as a 4-D tensor (channel in block, x, y, image * CIN / 8 + block);
-    // box = 8 channels x 130 pixels = 2080 contiguous bytes
+    // channel-blocked input as a 4-D tensor (element, x, y, image * CIN / 8 + block): with
+    // w % 8 == 0 an element run is 8 pixels x 8 channels (128 bytes) and x counts 8-pixel
+    // groups, box 18 groups; else a run is one pixel (16 bytes), box 130 pixels
     CUtensorMap map;
-    const cuuint64_t dims[4] = {8, (cuuint64_t)a.w, (cuuint64_t)a.h, (cuuint64_t)a.n * (CIN / 8)};
-    const cuuint64_t strides[3] = {16, (cuuint64_t)a.w * 16, (cuuint64_t)a.h * a.w * 16};
-    const cuuint32_t box[4] = {8, (cuuint32_t)pilot_tc::HALO, 1, 1};
+    a.grouped = (a.w % 8) == 0;
+    const cuuint64_t xs = a.grouped ? (cuuint64_t)(a.w / 8) : (cuuint64_t)a.w;
+    const cuuint64_t dims[4] = {a.grouped ? 64ull : 8ull, xs, (cuuint64_t)a.h, (cuuint64_t)a.n * (CIN / 8)};
+    const cuuint64_t strides[3] = {a.grouped ? 128ull : 16ull, (cuuint64_t)a.w * 16, (cuuint64_t)a.h * a.w * 16};
+    const cuuint32_t box[4] = {a.grouped ? 64u : 8u, a.grouped ? (cuuint32_t)pilot_tc::BOX_GROUPS : (cuuint32_t)pilot_tc::BOX_PIX,
+                               1, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(x), dims, strides, box, estr,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -482,6 +543,7 @@ extern "C" int zb3d_pilot_conv3x3_tc(const void *x, int n, int h, int w, int cin
     else if (cin == 16 && cout == 32) e = zb::conv_tc_t<16, 32>(x, a, st);
     else if (cin == 32 && cout == 32) e = zb::conv_tc_t<32, 32>(x, a, st);
     else if (cin == 32 && cout == 16) e = zb::conv_tc_t<32, 16>(x, a, st);
+    else if (cin == 16 && cout == 16) e = zb::conv_tc_t<16, 16>(x, a, st);
     return e == cudaSuccess ? 0 : -1;
 }
 

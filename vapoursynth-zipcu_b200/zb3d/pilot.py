@@ -2,7 +2,7 @@
 
 BM3Dv2's second pass (Wiener) matches blocks on, and takes its empirical Wiener
 coefficients from, a reference clip: normally the step-1 hard-threshold estimate.
-The pilot produces that reference with a stack of 3x3 convolutions (32 or 48
+The pilot produces that reference with a stack of 3x3 convolutions (16, 32 or 48
 channels, ReLU, a noise-level input plane; output added to the noisy plane).  It is trained
 only on pairs (noisy synthetic frame, plain BM3D step-1 output of it), on the GPU,
 by the project's own kernels (csrc/zb3d_pilot.cu: BF16 operands, FP32
@@ -29,12 +29,12 @@ from . import synth
 
 
 
-def arch(width: int = 48, layers: int = 10) -> list:
+def arch(width: int = 32, layers: int = 8) -> list:
     """(cin, cout) of each layer; the 2 input and 1 output channels are padded to 16."""
     return [(16, width)] + [(width, width)] * (layers - 2) + [(width, 16)]
 
 
-SHAPES = arch(48, 10)                                # the default architecture
+SHAPES = arch(32, 8)                                 # the default (and shipped) architecture
 REAL_IN, REAL_OUT = 2, 1
 LEVEL_SCALE = 4.0                                    # noise-level plane = sigma / 255 * LEVEL_SCALE
 LOSS_SCALE = 1024.0                                  # keeps BF16 gradients clear of underflow
@@ -52,7 +52,7 @@ def _ok(rc: int, what: str):
 class PilotNet:
     """The network, its FP32 master weights and Adam state, on one CUDA device."""
 
-    def __init__(self, seed: int = 0, device: str = "cuda", width: int = 48, layers: int = 10):
+    def __init__(self, seed: int = 0, device: str = "cuda", width: int = 32, layers: int = 8):
         import torch
         self.torch, self.dev = torch, device
         self.width, self.layers = width, layers
@@ -74,6 +74,7 @@ class PilotNet:
             self.keep.append((torch.from_numpy(k).to(device), torch.from_numpy(kb).to(device)))
         self.w16 = [torch.empty(w.shape, dtype=torch.bfloat16, device=device) for w in self.w32]
         self.wt16 = [torch.empty((cin, 3, 3, cout), dtype=torch.bfloat16, device=device) for cin, cout in self.shapes]
+        self._ws = {}  # inference activation buffers per (n, h, w, stream), reused across calls
         self.m = [(torch.zeros_like(w), torch.zeros_like(b)) for w, b in zip(self.w32, self.b32)]
         self.v = [(torch.zeros_like(w), torch.zeros_like(b)) for w, b in zip(self.w32, self.b32)]
         self.step_count = 0
@@ -130,7 +131,14 @@ class PilotNet:
             shape = (n, c // 8, h, w, 8) if tc else (n, h, w, c)
             return torch.empty(shape, dtype=torch.bfloat16, device=self.dev)
 
-        x = act(16)
+        reuse = tc and not keep_acts
+        if reuse:
+            # input and two ping-pong activation buffers, private to the stream that uses them
+            key = (n, h, w, stream)
+            if key not in self._ws:
+                self._ws[key] = [act(16), act(self.width), act(self.width)]
+            ws = self._ws[key]
+        x = ws[0] if reuse else act(16)
         pack = lib.zb3d_pilot_pack_input_blocked if tc else lib.zb3d_pilot_pack_input
         _ok(pack(_p(noisy), _p(sigma), n, h, w, LEVEL_SCALE, _p(x), stream), "pack_input")
         acts = [x]
@@ -147,7 +155,7 @@ class PilotNet:
 
         for l, (cin, cout) in enumerate(self.shapes):
             if l < last:
-                a = act(cout)
+                a = ws[1 + (l & 1)] if reuse else act(cout)  # hidden layers: cout == width
                 _ok(conv(acts[-1], l, 1, a, None, None), f"conv {l}")
                 if keep_acts:
                     acts.append(a)
@@ -334,19 +342,76 @@ def evaluate(net: PilotNet, sigmas=TRAIN_SIGMAS, frames: int = 4, size: int = 38
     return rows
 
 
+def time_kernels(width_layers=((32, 8), (48, 10)), w: int = 1920, h: int = 1080, reps: int = 20) -> list:
+    """CUDA-event times of the inference convolution per layer shape on one w x h plane
+    (tcgen05 and mma.sync), and of whole nets on a YUV420 frame (the plane plus two
+    half-size planes).  Lines of text."""
+    import torch
+    lib = N.lib()
+
+    def timeit(fn, n):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    out = []
+    shapes = sorted({s for wd, ly in width_layers for s in arch(wd, ly)})
+    for cin, cout in shapes:
+        xb = torch.randn((1, cin // 8, h, w, 8), device="cuda").to(torch.bfloat16)
+        xn = torch.randn((1, h, w, cin), device="cuda").to(torch.bfloat16)
+        wt = (torch.randn((cout, 3, 3, cin), device="cuda") * 0.05).to(torch.bfloat16)
+        b = torch.zeros(cout, device="cuda")
+        yb = torch.empty((1, cout // 8, h, w, 8), dtype=torch.bfloat16, device="cuda")
+        yn = torch.empty((1, h, w, cout), dtype=torch.bfloat16, device="cuda")
+        st = torch.zeros(1, dtype=torch.int32, device="cuda")
+        ttc = timeit(lambda: _ok(lib.zb3d_pilot_conv3x3_tc(_p(xb), 1, h, w, cin, _p(wt), _p(b), cout, 1, _p(yb), None,
+                                                           None, _p(st), None), "conv tc"), reps)
+        tmm = timeit(lambda: _ok(lib.zb3d_pilot_conv3x3(_p(xn), 1, h, w, cin, _p(wt), _p(b), cout, 1, None, _p(yn),
+                                                        None, None, None), "conv"), reps)
+        if int(st.item()) != 0:
+            raise RuntimeError("zb3d pilot: tensor-core convolution reported a pipeline timeout")
+        fl, by = 2.0 * h * w * 9 * cin * cout, h * w * 2.0 * (cin + cout)
+        out.append(f"conv {cin}->{cout} {w}x{h}: tcgen05 {ttc * 1e3:7.1f} us ({fl / ttc / 1e9:6.1f} TFLOP/s, "
+                   f"{by / ttc / 1e6:6.0f} GB/s)   mma.sync {tmm * 1e3:7.1f} us ({fl / tmm / 1e9:6.1f} TFLOP/s)")
+    for wd, ly in width_layers:
+        net = PilotNet(seed=0, width=wd, layers=ly)
+        y = torch.rand((1, h, w), device="cuda")
+        c = torch.rand((1, h // 2, w // 2), device="cuda")
+        s1 = torch.tensor([10.0], device="cuda")
+
+        def frame(tc):
+            net.forward(y, s1, tc=tc)
+            net.forward(c, s1, tc=tc)
+            net.forward(c, s1, tc=tc)
+        out.append(f"net {wd} ch x {ly} layers per {w}x{h} YUV420 frame: tcgen05 {timeit(lambda: frame(True), 10):.3f} ms"
+                   f"   mma.sync {timeit(lambda: frame(False), 5):.3f} ms")
+    return out
+
+
 def main(argv=None):
     import argparse
     ap = argparse.ArgumentParser(prog="python -m zb3d.pilot")
-    ap.add_argument("cmd", choices=["train", "eval"])
+    ap.add_argument("cmd", choices=["train", "eval", "time"])
     ap.add_argument("--frames", type=int, default=6, help="training frames per noise level and frame size")
     ap.add_argument("--dims", default="1920x1080,960x540", help="training frame sizes (the 1080p YUV420 planes)")
     ap.add_argument("--steps", type=int, default=6250, help="Adam steps of 32 crops (6250 = 200k crops)")
     ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--width", type=int, default=48, help="channels of the hidden layers (32 or 48)")
-    ap.add_argument("--layers", type=int, default=10, help="number of 3x3 convolutions")
+    ap.add_argument("--width", type=int, default=32, help="channels of the hidden layers (16, 32 or 48)")
+    ap.add_argument("--layers", type=int, default=8, help="number of 3x3 convolutions")
     ap.add_argument("--out", default=WEIGHTS)
     a = ap.parse_args(argv)
     import time
+    if a.cmd == "time":
+        for line in time_kernels():
+            print(line)
+        return
     if a.cmd == "train":
         t0 = time.time()
         noisy, target, sig = [], [], []

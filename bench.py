@@ -211,7 +211,7 @@ class DevicePipeline:
 
 
 def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frames: int = 4, nstreams: int = 4,
-                   weights: Optional[str] = None):
+                   weights: Optional[str] = None, conv_ctas_per_sm: int = 2):
     """Two-pass BM3Dv2 with the learned pilot (zb3d/pilot.py, shipped weights) as the
     step-2 reference in place of the step-1 estimate, on the same frames: device-resident
     Mpix/s, and PSNR against the clean frames next to the plain two-pass form.  Frames
@@ -221,6 +221,8 @@ def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frame
     from zb3d import synth
     from zb3d.device import DeviceFilter
     net = P.PilotNet.load(weights) if weights else P.shipped()
+    if N.lib().zb3d_pilot_tc_ctas_per_sm(conv_ctas_per_sm) != 0:
+        raise SystemExit(f"unsupported --pilot-conv-ctas {conv_ctas_per_sm}")
     finals = [DeviceFilter(W, H, family=N.YUV, subsampling=(1, 1), num_streams=1, ref=True, **KW)
               for _ in range(nstreams)]
     basic = DeviceFilter(W, H, family=N.YUV, subsampling=(1, 1), num_streams=1, **KW)
@@ -291,7 +293,7 @@ def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frame
     return {"value": W * H * steps * BATCH / (ms / 1e3) / 1e6, "unit": "Mpix/s", "ms_per_frame": ms / (steps * BATCH),
             "psnr_plain_two_pass_db": float(np.mean(plain)), "psnr_pilot_two_pass_db": float(np.mean(piloted)),
             "delta_psnr_db": delta, "delta_psnr_db_per_plane": [float(d) for d in np.mean(piloted - plain, 0)],
-            "within_0_05_db": delta >= -0.05, "streams": nstreams,
+            "within_0_05_db": delta >= -0.05, "streams": nstreams, "conv_ctas_per_sm": conv_ctas_per_sm,
             "what": "pilot (%d x conv3x3, %d ch, BF16 tcgen05 kernels, FP32 accumulation in tensor memory) as step 1 "
                     "on every plane, then the exact step 2; PSNR over the first %d frames against the clean frames"
                     % (net.layers, net.width, min(psnr_frames, nf))}
@@ -518,6 +520,102 @@ def run_vbm3d(torch, steps: int, warmup: int):
                                    "temporal aggregation per output frame", "batch_frames_per_step": BATCH}}
 
 
+def run_pilot4k(torch, steps: int, warmup: int, nstreams: int = 4):
+    """Learned-pilot BM3Dv2 on GRAYS 3840x2160: 4 clips of 8 frames, sigma per clip from
+    U[5, 25], block_step 4, bm_range 12, with the 48-channel, 10-layer pilot trained on 4K
+    planes (shipped weights).  Per clip, the two-pass PSNR against the clean frames is
+    measured with the plain step 1 and with the pilot as step 2's reference; the form
+    falls back to the plain step 1 where the pilot loses more than 0.05 dB.  Both forms are
+    timed (device-resident, `nstreams` streams); `value` is the gated form's Mpix/s.  The
+    blind gate (`PilotGate`, calibrated per sigma on held-out 4K frames) is reported beside
+    each clip's measured decision."""
+    from zb3d import _native as N
+    from zb3d import pilot as P
+    from zb3d import synth
+    from zb3d.device import DeviceFilter
+    w, h, nclips, nfr = 3840, 2160, 4, 8
+    kw = dict(block_step=4, bm_range=12, extractor_exp=EXTRACTOR_EXP)
+    net = P.PilotNet.load(P.WEIGHTS_4K)
+    gate = P.PilotGate(net)
+    gate.calibrate([5.0, 10.0, 15.0, 20.0, 25.0], frames=1, size=(w, h), **kw)
+    rng = np.random.default_rng(4040)
+    streams = [torch.cuda.Stream() for _ in range(nstreams)]
+    pe = w * h
+    total_ms, rows = 0.0, []
+    for c in range(nclips):
+        sigma = float(rng.uniform(5.0, 25.0))
+        basic = [DeviceFilter(w, h, family=N.GRAY, num_streams=1, sigma=[sigma], **kw) for _ in range(nstreams)]
+        final = [DeviceFilter(w, h, family=N.GRAY, num_streams=1, sigma=[sigma], ref=True, **kw)
+                 for _ in range(nstreams)]
+        sig = torch.full((1,), sigma, dtype=torch.float32, device="cuda")
+        bufs, outs, clean = [], [], []
+        for f in range(nfr):
+            b = torch.empty(2 * pe, dtype=torch.float32, device="cuda")  # [reference | noisy]
+            b[pe:].copy_(torch.from_numpy(synth.noisy_plane(w, h, sigma, clip=3000 + c, frame=f).reshape(-1)))
+            bufs.append(b)
+            outs.append(torch.empty(pe, dtype=torch.float32, device="cuda"))
+            clean.append(synth.clean_plane(w, h, 3000 + c, f))
+
+        def frame(f, k, pilot):
+            s = streams[k]
+            with torch.cuda.stream(s):
+                b = bufs[f]
+                if pilot:
+                    net.forward(b[pe:].view(1, h, w), sig, out=b[:pe].view(1, h, w), stream=s.cuda_stream)
+                else:
+                    basic[k].run(b.data_ptr() + 4 * pe, b.data_ptr(), s.cuda_stream)
+                final[k].run(b.data_ptr(), outs[f].data_ptr(), s.cuda_stream)
+
+        def psnrs(pilot):
+            for f in range(nfr):
+                frame(f, f % nstreams, pilot)
+            torch.cuda.synchronize()
+            return [synth.psnr(outs[f].view(h, w).cpu().numpy(), clean[f]) for f in range(nfr)]
+
+        def timed(pilot):
+            for _ in range(max(warmup, 1)):
+                for f in range(nfr):
+                    frame(f, f % nstreams, pilot)
+            torch.cuda.synchronize()
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(streams[0])
+            for s in streams[1:]:
+                s.wait_event(t0)
+            for _ in range(steps):
+                for f in range(nfr):
+                    frame(f, f % nstreams, pilot)
+            for s in streams[1:]:
+                e = torch.cuda.Event()
+                e.record(s)
+                streams[0].wait_event(e)
+            t1.record(streams[0])
+            t1.synchronize()
+            return t0.elapsed_time(t1)
+
+        plain, piloted = np.mean(psnrs(False)), np.mean(psnrs(True))
+        delta = float(piloted - plain)
+        use_pilot = delta >= -0.05
+        ms_plain, ms_pilot = timed(False), timed(True)
+        total_ms += ms_pilot if use_pilot else ms_plain
+        rows.append({"sigma": round(sigma, 3), "delta_psnr_db": delta, "step1": "pilot" if use_pilot else "plain",
+                     "blind_gate_step1": "pilot" if gate.accepts(sigma) else "plain",
+                     "psnr_plain_two_pass_db": float(plain), "psnr_pilot_two_pass_db": float(piloted),
+                     "ms_per_frame_plain": ms_plain / (steps * nfr), "ms_per_frame_pilot": ms_pilot / (steps * nfr)})
+        for fl in basic + final:
+            fl.close()
+        del bufs, outs
+    px = w * h * nclips * nfr * steps
+    return {"metric": "learned-pilot BM3Dv2 GRAYS 3840x2160 Mpix/s (0.05 dB fallback)",
+            "value": px / (total_ms / 1e3) / 1e6, "unit": "Mpix/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
+            "ms_per_step": total_ms / steps, "higher_is_better": True, "dtype": "bf16 pilot / f32 BM3D",
+            "data": "synthetic",
+            "config": {"workload": "GRAYS 3840x2160, 4 clips x 8 frames, sigma per clip U[5,25], block_step 4, "
+                                   "bm_range 12, pilot 48 ch x 10 layers trained on 4K planes (tcgen05), plain "
+                                   "step 1 where the pilot loses more than 0.05 dB", "streams": nstreams},
+            "blind_gate_delta_db_by_sigma": {str(k): round(v, 3) for k, v in gate.delta.items()},
+            "clips": rows}
+
+
 def run_gray640(torch, steps: int, warmup: int):
     """640x480 GRAYS single-pass BM3D, sigma 3, block_step 8, bm_range 9; a step is 8 frames."""
     from zb3d import synth
@@ -655,11 +753,14 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other block-matching form")
     ap.add_argument("--no-pilot", action="store_true", help="skip the learned-pilot form")
     ap.add_argument("--pilot-weights", default=None, help="pilot weights (.npz) instead of the shipped ones")
+    ap.add_argument("--pilot-conv-ctas", type=int, default=2,
+                    help="CTAs per SM of the pilot's convolutions (1 leaves room for step 2 of other frames)")
     ap.add_argument("--streams", type=int, default=4, help="CUDA streams the device pipeline spreads frames over")
     ap.add_argument("--match-form", type=int, choices=[-1, 0, 1], default=-1,
                     help="block matching: -1 = the library's autotuned choice per plane, 0 = FP32 scan of every "
                          "candidate, 1 = tensor-core bound + exact re-rank")
-    ap.add_argument("--workload", choices=["twopass1080", "vbm3d", "gray640", "batched"], default="twopass1080",
+    ap.add_argument("--workload", choices=["twopass1080", "vbm3d", "gray640", "batched", "pilot4k"],
+                    default="twopass1080",
                     help="twopass1080 is the metric's workload; the others print their own line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -675,9 +776,10 @@ def main():
     import torch
     torch.cuda.set_device(local)
     if args.workload != "twopass1080":
-        fn = {"vbm3d": run_vbm3d, "gray640": run_gray640, "batched": run_batched}[args.workload]
+        fn = {"vbm3d": run_vbm3d, "gray640": run_gray640, "batched": run_batched, "pilot4k": run_pilot4k}[args.workload]
         out = fn(torch, args.steps, args.warmup)
-        out.update({"n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic"})
+        for k, v in {"n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic"}.items():
+            out.setdefault(k, v)
         print(json.dumps(out))
         return 0
     dist = None
@@ -789,7 +891,13 @@ def main():
             pipe.close()
             pipe = None
         out["pilot_form"] = run_pilot_form(torch, frames, rank, max(1, args.steps // 4), 1,
-                                           weights=args.pilot_weights)
+                                           weights=args.pilot_weights, conv_ctas_per_sm=args.pilot_conv_ctas)
+        if args.pilot_weights is None:
+            # the 48-channel, 10-layer net of the learned-pilot configuration, on the same frames
+            from zb3d import pilot as P
+            out["pilot_form_w48_l10"] = run_pilot_form(torch, frames, rank, max(1, args.steps // 4), 1,
+                                                       weights=P.WEIGHTS_W48_L10,
+                                                       conv_ctas_per_sm=args.pilot_conv_ctas)
     if rank == 0 and not args.no_ref_cuda:
         rms = run_ref_cuda(torch, frames, args.steps, args.warmup)
         if rms:

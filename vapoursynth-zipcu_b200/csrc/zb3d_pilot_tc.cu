@@ -47,6 +47,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 namespace zb {
@@ -462,6 +463,10 @@ __global__ void pack_input_blocked(const float *noisy, const float *sigma, int n
 
 // ---- launcher ----------------------------------------------------------------------
 
+// CTAs per SM of the launch grid: 2 fills each SM's shared memory (fastest alone), 1
+// leaves half of it to kernels of other streams (step 2 of other frames)
+static std::atomic<int> g_conv_ctas_per_sm{pilot_tc::CTAS_PER_SM};
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -502,9 +507,9 @@ static cudaError_t conv_tc_t(const void *x, pilot_tc::Args a, cudaStream_t st) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     a.strips = (a.w + pilot_tc::TILE - 1) / pilot_tc::TILE;
-    // CTAS_PER_SM CTAs per SM, at least 4 tiles each
+    // up to CTAS_PER_SM CTAs per SM (g_conv_ctas_per_sm), at least 4 tiles each
     const long long tiles = (long long)a.n * a.strips * a.h;
-    const long long want = (tiles + 3) / 4, slots = (long long)pilot_tc::CTAS_PER_SM * sms;
+    const long long want = (tiles + 3) / 4, slots = (long long)g_conv_ctas_per_sm.load() * sms;
     const int grid = (int)(want < slots ? want : slots);
     auto k = pilot_tc::conv3x3_tc<CIN, COUT>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM);
@@ -545,6 +550,12 @@ extern "C" int zb3d_pilot_conv3x3_tc(const void *x, int n, int h, int w, int cin
     else if (cin == 32 && cout == 16) e = zb::conv_tc_t<32, 16>(x, a, st);
     else if (cin == 16 && cout == 16) e = zb::conv_tc_t<16, 16>(x, a, st);
     return e == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int zb3d_pilot_tc_ctas_per_sm(int ctas) {
+    if (ctas < 1 || ctas > zb::pilot_tc::CTAS_PER_SM) return -1;
+    zb::g_conv_ctas_per_sm.store(ctas);
+    return 0;
 }
 
 extern "C" int zb3d_pilot_pack_input_blocked(const float *noisy, const float *sigma, int n, int h, int w,

@@ -284,12 +284,16 @@ class PilotGate:
         self.net, self.tol = net, tol
         self.delta: dict = {}
 
-    def calibrate(self, sigmas: Sequence[float], frames: int = 2, size: int = 256, seed: int = 99, **kw) -> dict:
+    def calibrate(self, sigmas: Sequence[float], frames: int = 2, size=256, seed: int = 99, **kw) -> dict:
+        """Measure the two-pass difference per noise level on held-out synthetic frames of
+        `size` (or (width, height)): calibrate at the frame size the gate will serve, since
+        the synthetic content's scale changes with it."""
+        w, h = (size, size) if isinstance(size, int) else size
         for si, s in enumerate(sigmas):
             d = []
             for f in range(frames):
-                cl = synth.clean_plane(size, size, 5000 + seed + si, f)
-                nz = synth.noisy_plane(size, size, s, clip=5000 + seed + si, frame=f)
+                cl = synth.clean_plane(w, h, 5000 + seed + si, f)
+                nz = synth.noisy_plane(w, h, s, clip=5000 + seed + si, frame=f)
                 plain = two_pass(nz, s, **kw)
                 piloted = two_pass(nz, s, ref=self.net.denoise(nz, s), **kw)
                 d.append(synth.psnr(piloted, cl) - synth.psnr(plain, cl))
@@ -315,14 +319,23 @@ class PilotGate:
 # ---------------------------------------------------------------------------------------
 import os as _os
 
-WEIGHTS = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_bs4_r12.npz")
+WEIGHTS = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_bs4_r12.npz")  # 32 ch x 8 layers
+# the 48-channel, 10-layer net, trained by `python -m zb3d.pilot train --width 48 --layers 10`
+WEIGHTS_W48_L10 = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_w48_l10_bs4_r12.npz")
+# 48 ch x 10 layers trained on 3840x2160 planes:
+# `python -m zb3d.pilot train --width 48 --layers 10 --dims 3840x2160 --frames 4`
+WEIGHTS_4K = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_w48_l10_4k_bs4_r12.npz")
 TRAIN_KW = dict(block_step=4, bm_range=12)   # step-1 configuration the shipped pilot imitates
 TRAIN_SIGMAS = (5.0, 10.0, 15.0, 20.0, 25.0)
 
 
-def shipped(device: str = "cuda") -> PilotNet:
-    """The pilot trained by `python -m zb3d.pilot train` (weights next to this file)."""
-    return PilotNet.load(WEIGHTS, device=device)
+def shipped(device: str = "cuda", width: int = 32, layers: int = 8) -> PilotNet:
+    """A pilot trained by `python -m zb3d.pilot train` (weights next to this file): the
+    default 32 ch x 8 layers, or 48 ch x 10 layers."""
+    paths = {(32, 8): WEIGHTS, (48, 10): WEIGHTS_W48_L10}
+    if (width, layers) not in paths:
+        raise ValueError(f"no shipped pilot of {width} channels x {layers} layers")
+    return PilotNet.load(paths[(width, layers)], device=device)
 
 
 def evaluate(net: PilotNet, sigmas=TRAIN_SIGMAS, frames: int = 4, size: int = 384, seed: int = 77, **kw) -> list:

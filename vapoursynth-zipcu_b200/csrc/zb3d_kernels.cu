@@ -729,6 +729,9 @@ __global__ void __launch_bounds__(kFilterWarps * 32) zb_filter(FilterArgs a) {
     using T2 = typename TransformOf<T2D>::type;
     using T1 = typename TransformOf<T1D>::type;
     __shared__ float tbuf[kFilterWarps][8 * 4 * kTransStride];
+    // Wiener: the 64 coefficients of each thread, parked while its noisy group is transformed
+    // (dynamic shared memory [64][threads]; none for the hard-threshold pass)
+    extern __shared__ float cbuf[];
     const int lane = threadIdx.x & 31;
     const int j = lane & 7, g = lane >> 3;
     const unsigned gm = 0xffu << (lane & 24);
@@ -749,6 +752,33 @@ __global__ void __launch_bounds__(kFilterWarps * 32) zb_filter(FilterArgs a) {
     for (int p = 0; p < a.nplanes; ++p) {
         const float sigma = p == 0 ? a.sigma[0] : (p == 1 ? a.sigma[1] : a.sigma[2]);
         if (a.chroma && sigma < ZB_FLT_EPS) continue;
+        float k = 0.0f;
+        if constexpr (FINAL) {
+            // The reference (basic estimate) first: its 3D transform gives the Wiener
+            // coefficients r^2 / (r^2 + sigma^2), parked in shared memory, so that only one
+            // 64-value group is live in registers at a time.  The reference rounds r^2 once
+            // and adds sigma^2 (no fused multiply-add in the denominator); k accumulates by FMA.
+            float rf[64];
+            const float *rp = a.src + p * a.plane_stride;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const float *q = rp + pz[i] * a.frame_stride + (long long)py[i] * a.pitch + px[i] + j;
+#pragma unroll
+                for (int r = 0; r < 8; ++r) rf[i * 8 + r] = __ldg(q + r * a.pitch);
+            }
+            forward3<T2, T1>(rf, buf, g, j, gm);
+            const float s2 = sigma * sigma;
+#pragma unroll
+            for (int i = 0; i < 64; ++i) {
+                const float rv = rf[i];
+                const float r2 = __fmul_rn(rv, rv);
+                float coeff = r2 / __fadd_rn(r2, s2);
+                if (i == 0) coeff = j ? coeff : 1.0f;
+                k = __fmaf_rn(coeff, coeff, k);
+                cbuf[i * kFilterWarps * 32 + threadIdx.x] = coeff;
+            }
+            asm volatile("" ::: "memory");  // keep the noisy loads below: one group live at a time
+        }
         const float *sp = a.src + (FINAL ? a.clip_stride : 0) + p * a.plane_stride;
         float d[64];
 #pragma unroll
@@ -758,7 +788,6 @@ __global__ void __launch_bounds__(kFilterWarps * 32) zb_filter(FilterArgs a) {
             for (int r = 0; r < 8; ++r) d[i * 8 + r] = __ldg(q + r * a.pitch);
         }
         forward3<T2, T1>(d, buf, g, j, gm);
-        float k = 0.0f;
         if constexpr (!FINAL) {
 #pragma unroll
             for (int i = 0; i < 64; ++i) {
@@ -769,27 +798,10 @@ __global__ void __launch_bounds__(kFilterWarps * 32) zb_filter(FilterArgs a) {
                 d[i] = flag ? (val * (1.0f / 4096.0f)) : 0.0f;
             }
         } else {
-            float rf[64];
-            const float *rp = a.src + p * a.plane_stride;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const float *q = rp + pz[i] * a.frame_stride + (long long)py[i] * a.pitch + px[i] + j;
-#pragma unroll
-                for (int r = 0; r < 8; ++r) rf[i * 8 + r] = __ldg(q + r * a.pitch);
-            }
-            forward3<T2, T1>(rf, buf, g, j, gm);
-            // coeff = r^2 / (r^2 + sigma^2): the reference rounds r^2 once and adds
-            // sigma^2 (no fused multiply-add in the denominator); k accumulates by FMA
-            const float s2 = sigma * sigma;
 #pragma unroll
             for (int i = 0; i < 64; ++i) {
                 float val = d[i];
-                const float rv = rf[i];
-                const float r2 = __fmul_rn(rv, rv);
-                float coeff = r2 / __fadd_rn(r2, s2);
-                if (i == 0) coeff = j ? coeff : 1.0f;
-                val *= coeff;
-                k = __fmaf_rn(coeff, coeff, k);
+                val *= cbuf[i * kFilterWarps * 32 + threadIdx.x];
                 d[i] = val * (1.0f / 4096.0f);
             }
         }
@@ -1005,7 +1017,13 @@ template <bool FINAL, int T2D, int T1D>
 static cudaError_t launch_filter_t(const FilterArgs &a, cudaStream_t st) {
     const long long threads = (long long)a.nblocks * 8;
     const int tpb = kFilterWarps * 32;
-    zb_filter<FINAL, T2D, T1D><<<(unsigned)((threads + tpb - 1) / tpb), tpb, 0, st>>>(a);
+    const int dyn = FINAL ? 64 * tpb * (int)sizeof(float) : 0;  // Wiener coefficient buffer
+    auto k = zb_filter<FINAL, T2D, T1D>;
+    if (FINAL) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        if (e != cudaSuccess) return e;
+    }
+    k<<<(unsigned)((threads + tpb - 1) / tpb), tpb, dyn, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -289,9 +289,10 @@ int zb3d_pilot_conv3x3(const void *x, int n, int h, int w, int cin, const void *
  * becomes non-zero if a pipeline wait timed out. */
 int zb3d_pilot_conv3x3_tc(const void *x, int n, int h, int w, int cin, const void *wgt, const float *bias, int cout,
                           int relu, void *y, float *y0, const float *resid, int *status, void *stream);
-/* Grid of zb3d_pilot_conv3x3_tc for the whole process: ctas CTAs per SM (1 or 2; 2 by
- * default).  2 fills each SM's shared memory and is fastest alone; 1 leaves half of it to
- * kernels of other streams.  Returns 0, or -1 for an unsupported value. */
+/* Grid of zb3d_pilot_conv3x3_tc for the whole process: at most ctas CTAs per SM (1..3; 3
+ * by default, i.e. the layer's own count: 3 up to 32 channels, 2 with 48).  The default
+ * fills each SM and is fastest alone; 1 leaves room for kernels of other streams.
+ * Returns 0, or -1 for an unsupported value. */
 int zb3d_pilot_tc_ctas_per_sm(int ctas);
 /* The network input of zb3d_pilot_pack_input in the channel-blocked layout ([n][2][h][w][8]). */
 int zb3d_pilot_pack_input_blocked(const float *noisy, const float *sigma, int n, int h, int w, float level_scale,

@@ -28,12 +28,12 @@
 // A run of n output rows takes n + 2 input rows and n + 4 accumulators (the 4 at
 // its ends only collect halo contributions and are discarded).
 //
-// Two CTAs per SM, each owning a contiguous range of tiles in (image, strip, row)
-// order (balanced to one tile).  The row ring fills the shared memory the weights
-// leave (up to 16 slots).
+// Three CTAs per SM for layers of up to 32 channels, two with 48, each owning a
+// contiguous range of tiles in (image, strip, row) order (balanced to one tile).  The
+// row ring fills the shared memory the weights leave (up to 16 slots).
 //
-// Roles (384 threads): warp 0 lane 0 issues the TMA row loads, warp 1 lane 0
-// issues the MMAs, warp 2 owns the tensor-memory allocation, and two quads of
+// Roles (256 or 384 threads): warp 0 lane 0 issues the TMA row loads, warp 1 lane 0
+// issues the MMAs, warp 2 owns the tensor-memory allocation, and one or two quads of
 // epilogue warps (4-7 and 8-11, warp w on the 32-lane quarter w % 4 of tensor
 // memory) take the accumulators in turn, so that one quad's tensor-memory loads
 // and stores overlap the other's: bias, ReLU, BF16 store
@@ -58,11 +58,7 @@ constexpr int BOX_PIX = 130;             // TMA box of 130 single pixels (any wi
 constexpr int BOX_GROUPS = 18;           // TMA box of 18 groups of 8 pixels (width a multiple of 8)
 constexpr int CB_BYTES = BOX_GROUPS * 128;  // one channel block of a staged row (2304 bytes)
 constexpr int MAX_RING = 16;             // staged input row slots, at most
-constexpr int CTAS_PER_SM = 2;           // two independent pipelines per SM
-constexpr int SMEM_BUDGET = 112 * 1024;  // shared memory of the ring and the weights, per CTA
-constexpr int TMEM_COLS = 512 / CTAS_PER_SM;  // accumulator ring of each CTA
-constexpr int EPI_GROUPS = 2;            // epilogue warp quads, taking accumulators in turn
-constexpr int THREADS = 128 + 128 * EPI_GROUPS;
+constexpr int MAX_CTAS_PER_SM = 3;       // independent pipelines per SM, at most
 constexpr unsigned WAIT_LIMIT = 1u << 20;  // try_wait rounds on an mbarrier before giving up (about a second)
 
 struct Args {
@@ -81,8 +77,16 @@ template <int CIN, int COUT>
 struct Shape {
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && 3 * COUT <= 256, "unsupported layer shape");
     static constexpr int CB = CIN / 8;
+    // Pipelines per SM: 3 for layers up to 32 channels, 2 with 48 (their weights and rows
+    // need the shared memory).  With 3, each CTA has one epilogue warp quad and 128
+    // tensor-memory columns; with 2, two quads and 256 columns.
+    static constexpr int CTAS = (CIN <= 32 && COUT <= 32) ? 3 : 2;
+    static constexpr int EPI_GROUPS = CTAS == 3 ? 1 : 2;  // epilogue warp quads, taking accumulators in turn
+    static constexpr int THREADS = 128 + 128 * EPI_GROUPS;
+    static constexpr int TMEM_COLS = CTAS == 3 ? 128 : 256;
+    static constexpr int SMEM_BUDGET = CTAS == 3 ? 72 * 1024 : 112 * 1024;  // ring + weights, per CTA
     static constexpr int NACC = TMEM_COLS / COUT;  // accumulator slots
-    static_assert(NACC >= 5, "accumulator ring too small");
+    static_assert(NACC >= 4, "accumulator ring too small");
     static constexpr int KSTEPS = CIN / 16;
     static constexpr int ROW_BYTES = CB * CB_BYTES;
     static constexpr int W_BYTES = 9 * CB * COUT * 16;
@@ -231,7 +235,8 @@ __device__ __forceinline__ bool next_seg(const Args &p, long long &t, long long 
 }
 
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(THREADS, CTAS_PER_SM) conv3x3_tc(const __grid_constant__ CUtensorMap xmap, Args p) {
+__global__ void __launch_bounds__(Shape<CIN, COUT>::THREADS, Shape<CIN, COUT>::CTAS)
+    conv3x3_tc(const __grid_constant__ CUtensorMap xmap, Args p) {
     using S = Shape<CIN, COUT>;
     constexpr int RING = S::RING, NACC = S::NACC;
     extern __shared__ uint8_t smraw[];
@@ -254,7 +259,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) conv3x3_tc(const __grid_
     auto acc_slot = [](uint32_t g) { return (int)(NACC - 1 - g % NACC); };
 
     // weights as B operands [kx][channel block][ky][cout][8]: N = 3 COUT rows per (kx, block)
-    for (int i = threadIdx.x; i < 9 * S::CB * COUT; i += THREADS) {
+    for (int i = threadIdx.x; i < 9 * S::CB * COUT; i += S::THREADS) {
         const int co = i % COUT, r1 = i / COUT, ky = r1 % 3, r2 = r1 / 3, cb = r2 % S::CB, kx = r2 / S::CB;
         *reinterpret_cast<uint4 *>(sm + S::OFF_W + 16 * i) =
             __ldg(reinterpret_cast<const uint4 *>(p.wgt + ((size_t)co * 9 + ky * 3 + kx) * CIN + cb * 8));
@@ -274,7 +279,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) conv3x3_tc(const __grid_
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    if (warp == 2) tmem_alloc(smem_u32(tslot), TMEM_COLS);
+    if (warp == 2) tmem_alloc(smem_u32(tslot), S::TMEM_COLS);
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // weights: generic stores -> MMA reads
     fence_before_sync();
     __syncthreads();
@@ -387,7 +392,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) conv3x3_tc(const __grid_
         }
     } else if (warp >= 4) {
         // epilogue: warp w drains tensor-memory lanes 32 (w % 4) .. + 31 (pixels of the tile) of
-        // the accumulators g with g % EPI_GROUPS == its quad
+        // the accumulators g with g % S::EPI_GROUPS == its quad
         const int q = warp & 3, grp = (warp - 4) >> 2;
         uint32_t g = 0;
         bool ok = true;
@@ -397,7 +402,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) conv3x3_tc(const __grid_
             const int n = k.yb - k.ya;
             // accumulator j of the run = output row ya - 2 + j; rows ya .. yb - 1 are real
             for (int j = 0; j < n + 4; ++j, ++g) {
-                if ((int)(g % EPI_GROUPS) != grp) continue;
+                if ((int)(g % S::EPI_GROUPS) != grp) continue;
                 const int slot = acc_slot(g);
                 if (!wait_bar(acc_full + 8u * slot, (g / NACC) & 1, abort_flag, p.status, 4)) {
                     ok = false;
@@ -443,7 +448,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) conv3x3_tc(const __grid_
     __syncthreads();
     if (warp == 2) {
         fence_after_sync();
-        tmem_dealloc(tmem, TMEM_COLS);
+        tmem_dealloc(tmem, S::TMEM_COLS);
     }
 }
 
@@ -463,9 +468,9 @@ __global__ void pack_input_blocked(const float *noisy, const float *sigma, int n
 
 // ---- launcher ----------------------------------------------------------------------
 
-// CTAs per SM of the launch grid: 2 fills each SM's shared memory (fastest alone), 1
-// leaves half of it to kernels of other streams (step 2 of other frames)
-static std::atomic<int> g_conv_ctas_per_sm{pilot_tc::CTAS_PER_SM};
+// Cap on the CTAs per SM of the launch grid: the shape's own count (3 or 2) fills each
+// SM (fastest alone), 1 leaves room for kernels of other streams (step 2 of other frames)
+static std::atomic<int> g_conv_ctas_per_sm{pilot_tc::MAX_CTAS_PER_SM};
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -507,14 +512,15 @@ static cudaError_t conv_tc_t(const void *x, pilot_tc::Args a, cudaStream_t st) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     a.strips = (a.w + pilot_tc::TILE - 1) / pilot_tc::TILE;
-    // up to CTAS_PER_SM CTAs per SM (g_conv_ctas_per_sm), at least 4 tiles each
+    // S::CTAS CTAs per SM (capped by g_conv_ctas_per_sm), at least 4 tiles each
     const long long tiles = (long long)a.n * a.strips * a.h;
-    const long long want = (tiles + 3) / 4, slots = (long long)g_conv_ctas_per_sm.load() * sms;
+    const int per_sm = S::CTAS < g_conv_ctas_per_sm.load() ? S::CTAS : g_conv_ctas_per_sm.load();
+    const long long want = (tiles + 3) / 4, slots = (long long)per_sm * sms;
     const int grid = (int)(want < slots ? want : slots);
     auto k = pilot_tc::conv3x3_tc<CIN, COUT>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM);
     if (e != cudaSuccess) return e;
-    k<<<grid, pilot_tc::THREADS, S::SMEM, st>>>(map, a);
+    k<<<grid, S::THREADS, S::SMEM, st>>>(map, a);
     return cudaGetLastError();
 }
 
@@ -553,7 +559,7 @@ extern "C" int zb3d_pilot_conv3x3_tc(const void *x, int n, int h, int w, int cin
 }
 
 extern "C" int zb3d_pilot_tc_ctas_per_sm(int ctas) {
-    if (ctas < 1 || ctas > zb::pilot_tc::CTAS_PER_SM) return -1;
+    if (ctas < 1 || ctas > zb::pilot_tc::MAX_CTAS_PER_SM) return -1;
     zb::g_conv_ctas_per_sm.store(ctas);
     return 0;
 }

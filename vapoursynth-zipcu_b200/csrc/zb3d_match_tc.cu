@@ -38,9 +38,12 @@
 
 #include "zb3d_args.h"
 #include "zb3d_match.cuh"
+#include "zb3d_tcgen05.cuh"
 
 namespace zb {
 namespace tc {
+
+using namespace tc05;
 
 constexpr int BX = 8, BY = 16, M = BX * BY;  // reference blocks per tile
 constexpr int N = 128;                       // candidates per MMA chunk
@@ -95,9 +98,9 @@ __device__ __forceinline__ int core_off(int row, int kc) {
 }
 
 // ---------------------------------------------------------------------------
-// PTX wrappers (tcgen05, mbarrier), PTX ISA 8.6+ for sm_100a.
+// Operand descriptors and waits of this kernel (the generic tcgen05 / mbarrier
+// wrappers are in zb3d_tcgen05.cuh).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 // Shared-memory matrix descriptor, K-major with the 64-byte swizzle (layout type 4
 // at bits 61-63): start address and SBO (stride of 8-row groups, 1536 bytes) in
@@ -115,37 +118,7 @@ __device__ __forceinline__ uint32_t kstep_off(int kk) { return (uint32_t)((kk >>
 constexpr uint32_t IDESC = (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 
 __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.u32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate)
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t mbar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar)
-                 : "memory");
-}
-
-__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
-__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mbar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_test(uint32_t mbar, uint32_t parity) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(mbar), "r"(parity)
-        : "memory");
-    return done != 0;
+    mma_kind_f16(tmem_d, adesc, bdesc, IDESC, accumulate);
 }
 
 // Waits for phase `parity` of an mbarrier, at most WAIT_LIMIT polls; false on
@@ -159,34 +132,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, unsign
         if (i > 64) __nanosleep(64);
     }
     return false;
-}
-
-__device__ __forceinline__ void tmem_alloc(uint32_t slot_saddr, uint32_t ncols) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(slot_saddr), "r"(ncols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
-}
-
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols) : "memory");
-}
-
-// 32 consecutive FP32 columns of this warp's 32 lanes.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr)
-        : "memory");
-    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 __device__ __forceinline__ uint32_t h2u(__half a, __half b) {
@@ -355,9 +300,6 @@ __device__ __forceinline__ void list_fallback(const MatchArgs &a, int bi) {
     a.tc_ws[kTcWsList + k] = bi;
 }
 
-__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(mbar) : "memory");
-}
 
 // Asynchronous copy of the tile's FP32 region (union rows + 7, columns + 7) into
 // shared memory at pitch REG_COLS; columns beyond it are zero-filled.

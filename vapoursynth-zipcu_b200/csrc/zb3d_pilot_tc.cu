@@ -50,8 +50,12 @@
 #include <atomic>
 #include <cstdint>
 
+#include "zb3d_tcgen05.cuh"
+
 namespace zb {
 namespace pilot_tc {
+
+using namespace tc05;
 
 constexpr int TILE = 128;                // output pixels per tile (MMA M)
 constexpr int BOX_PIX = 130;             // TMA box of 130 single pixels (any width)
@@ -108,8 +112,6 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int n) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TILE >> 4) << 24);
 }
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
 // Shared-memory matrix descriptor, K-major without swizzle (layout type 0):
 // start address, LBO (the two 8-element K halves) and SBO (8-row groups) in
 // 16-byte units, version 1 at bits 46-47.
@@ -118,57 +120,13 @@ __device__ __forceinline__ uint64_t desc_k(uint32_t saddr, uint32_t lbo, uint32_
            ((uint64_t)((sbo >> 4) & 0x3fff) << 32) | (1ull << 46);
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                         uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.u32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t mbar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar)
-                 : "memory");
-}
-
-__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
-__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mbar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(mbar) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_tx(uint32_t mbar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(bytes) : "memory");
-}
-
-// try_wait suspends the thread until the phase completes or a hardware time limit
-// passes, so waiting threads take no issue slots from the working ones
-__device__ __forceinline__ bool mbar_test(uint32_t mbar, uint32_t parity) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(mbar), "r"(parity)
-        : "memory");
-    return done != 0;
-}
-
 // Waits for phase `parity` of an mbarrier.  Gives up when another role has
 // aborted, or after WAIT_LIMIT tries: then it raises the abort flag and records
 // `code` in the status word.
 __device__ __forceinline__ bool wait_bar(uint32_t mbar, uint32_t parity, volatile int *abort_flag, int *status,
                                          int code) {
     for (unsigned i = 0; i < WAIT_LIMIT; ++i) {
-        if (mbar_test(mbar, parity)) return true;
+        if (mbar_try(mbar, parity)) return true;
         if (*abort_flag) return false;
     }
     *abort_flag = 1;
@@ -176,7 +134,8 @@ __device__ __forceinline__ bool wait_bar(uint32_t mbar, uint32_t parity, volatil
     return false;
 }
 
-// 130 pixels from x of row y of channel-block plane `plane` (= image * CIN / 8 + block)
+// one TMA box (130 pixels, or 18 groups of 8 pixels, from x) of row y of channel-block
+// plane `plane` (= image * CIN / 8 + block)
 __device__ __forceinline__ void tma_row(uint32_t dst, const CUtensorMap *map, int c, int x, int y, int plane,
                                         uint32_t mbar) {
     asm volatile(
@@ -185,32 +144,6 @@ __device__ __forceinline__ void tma_row(uint32_t dst, const CUtensorMap *map, in
         "l"(reinterpret_cast<uint64_t>(map)), "r"(c), "r"(x), "r"(y), "r"(plane), "r"(mbar)
         : "memory");
 }
-
-__device__ __forceinline__ void tmem_alloc(uint32_t slot_saddr, uint32_t ncols) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(slot_saddr), "r"(ncols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
-}
-
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols) : "memory");
-}
-
-// 16 consecutive FP32 columns of this warp's 32 lanes (no wait)
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr)
-        : "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(lo)) |
@@ -280,7 +213,7 @@ __global__ void __launch_bounds__(Shape<CIN, COUT>::THREADS, Shape<CIN, COUT>::C
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     if (warp == 2) tmem_alloc(smem_u32(tslot), S::TMEM_COLS);
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // weights: generic stores -> MMA reads
+    fence_async_smem();  // weights: generic stores -> MMA reads
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
@@ -311,7 +244,7 @@ __global__ void __launch_bounds__(Shape<CIN, COUT>::THREADS, Shape<CIN, COUT>::C
         if (!ok) {
             // let the row loads already issued land before the CTA can end
             for (uint32_t q = e > RING ? e - RING : 0; q < e; ++q) {
-                for (unsigned i = 0; i < WAIT_LIMIT && !mbar_test(row_full + 8u * (q % RING), (q / RING) & 1); ++i) {
+                for (unsigned i = 0; i < WAIT_LIMIT && !mbar_try(row_full + 8u * (q % RING), (q / RING) & 1); ++i) {
                 }
             }
         }
@@ -356,25 +289,25 @@ __global__ void __launch_bounds__(Shape<CIN, COUT>::THREADS, Shape<CIN, COUT>::C
                         if (kx == 0 && ks == 0 && i > 0) {
                             // row r + 1's accumulator is fresh: its first product overwrites
                             const int s2 = s0 >= 2 ? s0 - 2 : s0 + NACC - 2;
-                            mma_bf16(tmem + (uint32_t)(s2 * COUT), ad, bd, idesc_bf16(COUT), 0);
+                            mma_kind_f16(tmem + (uint32_t)(s2 * COUT), ad, bd, idesc_bf16(COUT), 0);
                             if (s0 >= 1) {  // slots s0 - 1, s0 = rows r, r - 1
-                                mma_bf16(d0 - COUT, ad, bd + KY1, idesc_bf16(2 * COUT), 1);
+                                mma_kind_f16(d0 - COUT, ad, bd + KY1, idesc_bf16(2 * COUT), 1);
                             } else {
-                                mma_bf16(tmem + (uint32_t)((NACC - 1) * COUT), ad, bd + KY1, idesc_bf16(COUT), 1);
-                                mma_bf16(tmem, ad, bd + KY2, idesc_bf16(COUT), 1);
+                                mma_kind_f16(tmem + (uint32_t)((NACC - 1) * COUT), ad, bd + KY1, idesc_bf16(COUT), 1);
+                                mma_kind_f16(tmem, ad, bd + KY2, idesc_bf16(COUT), 1);
                             }
                             continue;
                         }
                         // a run's first row: all three accumulators are fresh
                         const uint32_t acc = (kx == 0 && ks == 0) ? 0u : 1u;
                         if (s0 >= 2) {  // slots s0 - 2, s0 - 1, s0 = rows r + 1, r, r - 1: one MMA
-                            mma_bf16(d0 - 2 * COUT, ad, bd, idesc_bf16(3 * COUT), acc);
+                            mma_kind_f16(d0 - 2 * COUT, ad, bd, idesc_bf16(3 * COUT), acc);
                         } else if (s0 == 1) {  // slots 0, 1 = rows r, r - 1; slot NACC - 1 = row r + 1
-                            mma_bf16(tmem, ad, bd + KY1, idesc_bf16(2 * COUT), acc);
-                            mma_bf16(tmem + (uint32_t)((NACC - 1) * COUT), ad, bd, idesc_bf16(COUT), acc);
+                            mma_kind_f16(tmem, ad, bd + KY1, idesc_bf16(2 * COUT), acc);
+                            mma_kind_f16(tmem + (uint32_t)((NACC - 1) * COUT), ad, bd, idesc_bf16(COUT), acc);
                         } else {  // slot 0 = row r - 1; slots NACC - 2, NACC - 1 = rows r + 1, r
-                            mma_bf16(tmem, ad, bd + KY2, idesc_bf16(COUT), acc);
-                            mma_bf16(tmem + (uint32_t)((NACC - 2) * COUT), ad, bd, idesc_bf16(2 * COUT), acc);
+                            mma_kind_f16(tmem, ad, bd + KY2, idesc_bf16(COUT), acc);
+                            mma_kind_f16(tmem + (uint32_t)((NACC - 2) * COUT), ad, bd, idesc_bf16(2 * COUT), acc);
                         }
                     }
                 mma_commit(row_free + 8u * (e % RING));  // the staged row is done
@@ -388,7 +321,7 @@ __global__ void __launch_bounds__(Shape<CIN, COUT>::THREADS, Shape<CIN, COUT>::C
         }
         // every MMA issued has completed before the CTA ends
         mma_commit(drain);
-        for (unsigned i = 0; i < WAIT_LIMIT && !mbar_test(drain, 0); ++i) {
+        for (unsigned i = 0; i < WAIT_LIMIT && !mbar_try(drain, 0); ++i) {
         }
     } else if (warp >= 4) {
         // epilogue: warp w drains tensor-memory lanes 32 (w % 4) .. + 31 (pixels of the tile) of

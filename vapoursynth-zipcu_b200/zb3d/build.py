@@ -31,7 +31,7 @@ UNITS = [
     ("zb3d_host.cpp", ARCH),
     ("zb3d_noalloc.cu", ARCH),
 ]
-HEADERS = ["zb3d_args.h", "zb3d_match.cuh", "zb3d_transforms.cuh"]
+HEADERS = ["zb3d_args.h", "zb3d_match.cuh", "zb3d_transforms.cuh", "zb3d_tcgen05.cuh"]
 
 
 def _stale(out, deps):

@@ -214,8 +214,12 @@ def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frame
                    weights: Optional[str] = None, conv_ctas_per_sm: int = 3):
     """Two-pass BM3Dv2 with the learned pilot (zb3d/pilot.py, shipped weights) as the
     step-2 reference in place of the step-1 estimate, on the same frames: device-resident
-    Mpix/s, and PSNR against the clean frames next to the plain two-pass form.  Frames
-    run on `nstreams` streams, each with its own step-2 filter and pilot buffers."""
+    Mpix/s, and PSNR against the clean frames next to the plain two-pass form.
+    The network runs batched on its own stream: one launch sequence for the luma planes
+    of a step's 8 frames and one for their 16 chroma planes, reading the noisy planes and
+    writing the references in place inside the frames' [reference | noisy] buffers.  The
+    exact step 2 of each frame then runs on one of `nstreams` streams once its batch's
+    network is done, overlapping the next batch's network."""
     from zb3d import _native as N
     from zb3d import pilot as P
     from zb3d import synth
@@ -228,61 +232,83 @@ def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frame
     basic = DeviceFilter(W, H, family=N.YUV, subsampling=(1, 1), num_streams=1, **KW)
     lay = finals[0].entries
     assert all(l.pitch == l.width for l in lay), "dense planes expected"
-    sig = torch.full((1,), SIGMA, dtype=torch.float32, device="cuda")
+    ly, lc = lay[0], lay[1]
+    assert (lay[2].width, lay[2].height) == (lc.width, lc.height)
     nf = len(frames)
-    bufs, outs = [], []  # per frame and plane: [reference | noisy] (the step-2 filter's input) and the output
+    assert nf % BATCH == 0
+    py, pc = ly.height * ly.width, lc.height * lc.width
+    # [frame][reference | noisy][luma plane] and [frame][U, V][reference | noisy][chroma plane]
+    ybuf = torch.zeros((nf, 2, py), dtype=torch.float32, device="cuda")
+    cbuf = torch.zeros((nf, 2, 2, pc), dtype=torch.float32, device="cuda")
     for i in range(nf):
-        fb, fo = [], []
-        for e, l in enumerate(lay):
-            pe = l.height * l.pitch
-            b = torch.zeros(2 * pe, dtype=torch.float32, device="cuda")
-            b[pe:].copy_(torch.from_numpy(np.ascontiguousarray(frames[i][l.plane[0]], np.float32).reshape(-1)))
-            fb.append(b)
-            fo.append(torch.empty(pe, dtype=torch.float32, device="cuda"))
-        bufs.append(fb)
-        outs.append(fo)
+        ybuf[i, 1].copy_(torch.from_numpy(np.ascontiguousarray(frames[i][0], np.float32).reshape(-1)))
+        for c in (1, 2):
+            cbuf[i, c - 1, 1].copy_(torch.from_numpy(np.ascontiguousarray(frames[i][c], np.float32).reshape(-1)))
+    outs = [[torch.empty(l.height * l.width, dtype=torch.float32, device="cuda") for l in lay] for _ in range(nf)]
+    net_stream = torch.cuda.Stream()
     streams = [torch.cuda.Stream() for _ in range(nstreams)]
+    sig_y = torch.full((BATCH,), SIGMA, dtype=torch.float32, device="cuda")
+    sig_c = torch.full((2 * BATCH,), SIGMA, dtype=torch.float32, device="cuda")
 
-    def frame(i, k=0, use_pilot=True):
+    def ref_ptr(i, e):  # the plane's [reference | noisy] pair, as step 2 reads it
+        return ybuf[i, 0].data_ptr() if e == 0 else cbuf[i, e - 1, 0].data_ptr()
+
+    def pilot_batch(f0, count):
+        """network over frames f0 .. f0 + count - 1 on the net stream; returns its event"""
+        with torch.cuda.stream(net_stream):
+            st = net_stream.cuda_stream
+            yv = ybuf[f0:f0 + count].view(count, 2, ly.height, ly.width)
+            net.forward(yv[:, 1], sig_y[:count], out=yv[:, 0], stream=st)
+            cv = cbuf[f0:f0 + count].view(2 * count, 2, lc.height, lc.width)
+            net.forward(cv[:, 1], sig_c[:2 * count], out=cv[:, 0], stream=st)
+        ev = torch.cuda.Event()
+        ev.record(net_stream)
+        return ev
+
+    def step2(i, k, after=None):
         s = streams[k]
-        st = s.cuda_stream
-        with torch.cuda.stream(s):
-            for e, l in enumerate(lay):
-                b, pe = bufs[i][e], l.height * l.pitch
-                if use_pilot:
-                    net.forward(b[pe:].view(1, l.height, l.width), sig, out=b[:pe].view(1, l.height, l.width),
-                                stream=st)
-                else:
-                    basic.run_entry(e, b.data_ptr() + 4 * pe, b.data_ptr(), st)
-                finals[k].run_entry(e, b.data_ptr(), outs[i][e].data_ptr(), st)
+        if after is not None:
+            s.wait_event(after)
+        for e in range(3):
+            finals[k].run_entry(e, ref_ptr(i, e), outs[i][e].data_ptr(), s.cuda_stream)
+
+    def plain_step1(i, k):
+        s = streams[k]
+        for e in range(3):
+            basic.run_entry(e, ref_ptr(i, e) + 4 * lay[e].height * lay[e].width, ref_ptr(i, e), s.cuda_stream)
 
     def psnrs(i):
+        torch.cuda.synchronize()
         return [synth.psnr(outs[i][e].view(l.height, l.width).cpu().numpy(),
                            synth.clean_plane(l.width, l.height, clip, i, l.plane[0])) for e, l in enumerate(lay)]
 
+    def batch(b):
+        f0 = (b * BATCH) % nf
+        ev = pilot_batch(f0, BATCH)
+        for j in range(BATCH):
+            step2(f0 + j, j % nstreams, ev)
+
     plain, piloted = [], []
     for i in range(min(psnr_frames, nf)):
-        frame(i, use_pilot=False)
-        torch.cuda.synchronize()
+        plain_step1(i, 0)
+        step2(i, 0)
         plain.append(psnrs(i))
-        frame(i, use_pilot=True)
-        torch.cuda.synchronize()
+        step2(i, 0, pilot_batch(i, 1))
         piloted.append(psnrs(i))
-    for j in range(max(warmup, nstreams)):
-        frame(j % nf, j % nstreams)
+    for b in range(max(warmup, 1)):
+        batch(b)
     torch.cuda.synchronize()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s0 = streams[0]
-    t0.record(s0)
-    for s in streams[1:]:
+    t0.record(net_stream)
+    for s in streams:
         s.wait_event(t0)
-    for j in range(steps * BATCH):
-        frame(j % nf, j % nstreams)
-    for s in streams[1:]:
+    for b in range(steps):
+        batch(b)
+    for s in streams:
         ev = torch.cuda.Event()
         ev.record(s)
-        s0.wait_event(ev)
-    t1.record(s0)
+        net_stream.wait_event(ev)
+    t1.record(net_stream)
     t1.synchronize()
     ms = t0.elapsed_time(t1)
     plain, piloted = np.array(plain), np.array(piloted)
@@ -295,8 +321,9 @@ def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frame
             "delta_psnr_db": delta, "delta_psnr_db_per_plane": [float(d) for d in np.mean(piloted - plain, 0)],
             "within_0_05_db": delta >= -0.05, "streams": nstreams, "conv_ctas_per_sm": conv_ctas_per_sm,
             "what": "pilot (%d x conv3x3, %d ch, BF16 tcgen05 kernels, FP32 accumulation in tensor memory) as step 1 "
-                    "on every plane, then the exact step 2; PSNR over the first %d frames against the clean frames"
-                    % (net.layers, net.width, min(psnr_frames, nf))}
+                    "on every plane, batched per step (8 luma, 16 chroma planes per launch) on its own stream, then "
+                    "the exact step 2 of each frame on %d streams; PSNR over the first %d frames against the clean "
+                    "frames" % (net.layers, net.width, nstreams, min(psnr_frames, nf))}
 
 
 def run_e2e(frames, steps: int, warmup: int, num_streams: int = 4):

@@ -285,18 +285,21 @@ int zb3d_pilot_conv3x3(const void *x, int n, int h, int w, int cin, const void *
 /* The same forward convolution (no mask) on the tensor cores, for inference: tcgen05.mma
  * with the accumulator in tensor memory, input rows staged by TMA, persistent CTAs down
  * 128-pixel column strips.  x and y use the channel-blocked layout [n][C/8][h][w][8]
- * (BF16); same shapes; x, wgt and y 16-byte aligned.  status (device int, may be NULL)
+ * (BF16); same shapes; x, wgt and y 16-byte aligned.  The images of y0 and resid are
+ * y0_stride and resid_stride floats apart (0: h * w).  status (device int, may be NULL)
  * becomes non-zero if a pipeline wait timed out. */
 int zb3d_pilot_conv3x3_tc(const void *x, int n, int h, int w, int cin, const void *wgt, const float *bias, int cout,
-                          int relu, void *y, float *y0, const float *resid, int *status, void *stream);
+                          int relu, void *y, float *y0, const float *resid, long long y0_stride,
+                          long long resid_stride, int *status, void *stream);
 /* Grid of zb3d_pilot_conv3x3_tc for the whole process: at most ctas CTAs per SM (1..3; 3
  * by default, i.e. the layer's own count: 3 up to 32 channels, 2 with 48).  The default
  * fills each SM and is fastest alone; 1 leaves room for kernels of other streams.
  * Returns 0, or -1 for an unsupported value. */
 int zb3d_pilot_tc_ctas_per_sm(int ctas);
-/* The network input of zb3d_pilot_pack_input in the channel-blocked layout ([n][2][h][w][8]). */
-int zb3d_pilot_pack_input_blocked(const float *noisy, const float *sigma, int n, int h, int w, float level_scale,
-                                  void *x0, void *stream);
+/* The network input of zb3d_pilot_pack_input in the channel-blocked layout ([n][2][h][w][8]);
+ * the noisy images are noisy_stride floats apart (0: h * w). */
+int zb3d_pilot_pack_input_blocked(const float *noisy, long long noisy_stride, const float *sigma, int n, int h,
+                                  int w, float level_scale, void *x0, void *stream);
 /* dw += dL/dw, db += dL/db of one layer from its input x and its pre-activation gradient dy. */
 int zb3d_pilot_conv3x3_wgrad(const void *x, const void *dy, int n, int h, int w, int cin, int cout, float *dw,
                              float *db, void *stream);

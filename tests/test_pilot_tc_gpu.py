@@ -47,8 +47,8 @@ def _conv(kind, x, w16, bias, n, h, w, cin, cout, relu, status=None):
         xb = blocked(x)
         yb = torch.empty((n, cout // 8, h, w, 8), dtype=torch.bfloat16, device="cuda")
         rc = lib.zb3d_pilot_conv3x3_tc(xb.data_ptr(), n, h, w, cin, w16.data_ptr(), bias.data_ptr(), cout, relu,
-                                       yb.data_ptr(), None, None, status.data_ptr() if status is not None else None,
-                                       None)
+                                       yb.data_ptr(), None, None, 0, 0,
+                                       status.data_ptr() if status is not None else None, None)
         assert rc == 0
         return nhwc(yb)
     else:
@@ -102,7 +102,7 @@ def test_tc_last_layer_fp32_output_and_residual():
         y0 = torch.full((n, h, w), np.nan, dtype=torch.float32, device="cuda")
         if kind == "tc":
             rc = lib.zb3d_pilot_conv3x3_tc(xb.data_ptr(), n, h, w, cin, w16.data_ptr(), bias.data_ptr(), cout, 0,
-                                           None, y0.data_ptr(), resid.data_ptr(), None, None)
+                                           None, y0.data_ptr(), resid.data_ptr(), 0, 0, None, None)
         else:
             rc = lib.zb3d_pilot_conv3x3(x.data_ptr(), n, h, w, cin, w16.data_ptr(), bias.data_ptr(), cout, 0, None,
                                         None, y0.data_ptr(), resid.data_ptr(), None)
@@ -132,3 +132,22 @@ def test_tc_network_forward_matches_mma_sync(width, layers):
     yt, ym = yt.cpu().numpy(), ym.cpu().numpy()
     rel = np.linalg.norm(yt - ym) / np.linalg.norm(ym - noisy.cpu().numpy())
     assert rel < 2e-2, rel  # one-step BF16 flips of hidden activations, relative to the net's output
+
+
+def test_tc_network_on_strided_frame_buffers():
+    """Images inside [reference | noisy] frame buffers (2 h w floats apart), as step 2 reads
+    them: the pilot reads the noisy halves and writes the reference halves in place."""
+    import torch
+    net = P.PilotNet(seed=5)
+    rng = np.random.default_rng(8)
+    n, h, w = 3, 40, 200
+    noisy = rng.uniform(0, 1, (n, h, w)).astype(np.float32)
+    sigma = torch.tensor([6.0, 12.0, 20.0], dtype=torch.float32, device="cuda")
+    dense, _ = net.forward(torch.from_numpy(noisy).cuda(), sigma, tc=True)
+    frames = torch.full((n, 2, h, w), np.nan, dtype=torch.float32, device="cuda")
+    frames[:, 1] = torch.from_numpy(noisy).cuda()
+    net.forward(frames[:, 1], sigma, out=frames[:, 0], tc=True)
+    assert torch.equal(frames[:, 0], dense)
+    assert torch.equal(frames[:, 1].cpu(), torch.from_numpy(noisy))
+    with pytest.raises(ValueError):
+        net.forward(frames[:, 1], sigma, tc=False)  # the NHWC path takes dense images only

@@ -69,8 +69,9 @@ struct Args {
     const __nv_bfloat16 *wgt;  // [cout][9][cin]
     const float *bias;         // [cout]
     __nv_bfloat16 *y;          // [n][cout / 8][h][w][8] or null
-    float *y0;                 // [n][h][w] or null: output channel 0 (+ resid) in FP32
-    const float *resid;        // [n][h][w] or null
+    float *y0;                 // [n][h][w] (images y0_stride apart) or null: channel 0 (+ resid) in FP32
+    const float *resid;        // [n][h][w] (images resid_stride apart) or null
+    long long y0_stride, resid_stride;
     int n, h, w, relu;
     int strips;                // ceil(w / 128)
     int grouped;               // boxes of 8-pixel groups (w % 8 == 0), else of single pixels
@@ -370,10 +371,9 @@ __global__ void __launch_bounds__(Shape<CIN, COUT>::THREADS, Shape<CIN, COUT>::C
                         dst[i * plane] = make_uint4(pack_bf16(v[8 * i], v[8 * i + 1]), pack_bf16(v[8 * i + 2], v[8 * i + 3]),
                                                     pack_bf16(v[8 * i + 4], v[8 * i + 5]), pack_bf16(v[8 * i + 6], v[8 * i + 7]));
                 }
-                if (p.y0) {
-                    const size_t o = (size_t)k.img * plane + pix;
-                    p.y0[o] = v[0] + (p.resid ? p.resid[o] : 0.0f);
-                }
+                if (p.y0)
+                    p.y0[(size_t)k.img * p.y0_stride + pix] =
+                        v[0] + (p.resid ? p.resid[(size_t)k.img * p.resid_stride + pix] : 0.0f);
             }
         }
     }
@@ -385,15 +385,17 @@ __global__ void __launch_bounds__(Shape<CIN, COUT>::THREADS, Shape<CIN, COUT>::C
     }
 }
 
-// x0 [n][2][h][w][8]: block 0 = (noisy, sigma / 255 * level_scale, 0 x 6), block 1 = 0
-__global__ void pack_input_blocked(const float *noisy, const float *sigma, int n, int h, int w, float level_scale,
-                                   __nv_bfloat16 *x0) {
+// x0 [n][2][h][w][8]: block 0 = (noisy, sigma / 255 * level_scale, 0 x 6), block 1 = 0;
+// the noisy images are noisy_stride floats apart
+__global__ void pack_input_blocked(const float *noisy, long long noisy_stride, const float *sigma, int n, int h, int w,
+                                   float level_scale, __nv_bfloat16 *x0) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long plane = (long long)h * w;
     if (i >= n * plane) return;
     const long long img = i / plane, pix = i - img * plane;
     uint4 *o = reinterpret_cast<uint4 *>(x0) + img * 2 * plane + pix;
-    o[0] = make_uint4(pack_bf16(noisy[i], sigma[img] * (1.0f / 255.0f) * level_scale), 0u, 0u, 0u);
+    o[0] = make_uint4(pack_bf16(noisy[img * noisy_stride + pix], sigma[img] * (1.0f / 255.0f) * level_scale), 0u, 0u,
+                      0u);
     o[plane] = make_uint4(0u, 0u, 0u, 0u);
 }
 
@@ -462,8 +464,8 @@ static cudaError_t conv_tc_t(const void *x, pilot_tc::Args a, cudaStream_t st) {
 // ---- C ABI (include/zb3d.h) ---------------------------------------------------------
 
 extern "C" int zb3d_pilot_conv3x3_tc(const void *x, int n, int h, int w, int cin, const void *wgt, const float *bias,
-                                     int cout, int relu, void *y, float *y0, const float *resid, int *status,
-                                     void *stream) {
+                                     int cout, int relu, void *y, float *y0, const float *resid, long long y0_stride,
+                                     long long resid_stride, int *status, void *stream) {
     if (n <= 0 || h <= 0 || w <= 0) return n == 0 ? 0 : -1;
     if ((reinterpret_cast<uintptr_t>(x) & 15) || (reinterpret_cast<uintptr_t>(wgt) & 15) ||
         (reinterpret_cast<uintptr_t>(y) & 15))
@@ -474,6 +476,9 @@ extern "C" int zb3d_pilot_conv3x3_tc(const void *x, int n, int h, int w, int cin
     a.y = static_cast<__nv_bfloat16 *>(y);
     a.y0 = y0;
     a.resid = resid;
+    a.y0_stride = y0_stride > 0 ? y0_stride : (long long)h * w;
+    a.resid_stride = resid_stride > 0 ? resid_stride : (long long)h * w;
+    if (a.y0_stride < (long long)h * w || a.resid_stride < (long long)h * w) return -1;
     a.n = n;
     a.h = h;
     a.w = w;
@@ -497,11 +502,13 @@ extern "C" int zb3d_pilot_tc_ctas_per_sm(int ctas) {
     return 0;
 }
 
-extern "C" int zb3d_pilot_pack_input_blocked(const float *noisy, const float *sigma, int n, int h, int w,
-                                             float level_scale, void *x0, void *stream) {
+extern "C" int zb3d_pilot_pack_input_blocked(const float *noisy, long long noisy_stride, const float *sigma, int n,
+                                             int h, int w, float level_scale, void *x0, void *stream) {
     const long long np = (long long)n * h * w;
     if (np <= 0) return np == 0 ? 0 : -1;
+    if (noisy_stride <= 0) noisy_stride = (long long)h * w;
+    if (noisy_stride < (long long)h * w) return -1;
     zb::pilot_tc::pack_input_blocked<<<(unsigned)((np + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
-        noisy, sigma, n, h, w, level_scale, static_cast<__nv_bfloat16 *>(x0));
+        noisy, noisy_stride, sigma, n, h, w, level_scale, static_cast<__nv_bfloat16 *>(x0));
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -126,6 +126,13 @@ class PilotNet:
         if tc is None:
             tc = not keep_acts
         n, h, w = noisy.shape
+        y = out if out is not None else torch.empty((n, h, w), dtype=torch.float32, device=self.dev)
+        for t, what in ((noisy, "noisy"), (y, "out")):
+            # images may sit any distance apart (e.g. inside [reference | noisy] frame buffers);
+            # each image must be dense, and strided images need the tensor-core path
+            if tuple(t.shape) != (n, h, w) or t.stride(1) != w or t.stride(2) != 1 or \
+                    (not tc and n > 1 and t.stride(0) != h * w):
+                raise ValueError(f"zb3d pilot: {what} must be [n][h][w] with dense images")
 
         def act(c):  # NHWC for the mma.sync kernels, channel-blocked [n][c/8][h][w][8] for tcgen05
             shape = (n, c // 8, h, w, 8) if tc else (n, h, w, c)
@@ -139,17 +146,21 @@ class PilotNet:
                 self._ws[key] = [act(16), act(self.width), act(self.width)]
             ws = self._ws[key]
         x = ws[0] if reuse else act(16)
-        pack = lib.zb3d_pilot_pack_input_blocked if tc else lib.zb3d_pilot_pack_input
-        _ok(pack(_p(noisy), _p(sigma), n, h, w, LEVEL_SCALE, _p(x), stream), "pack_input")
+        if tc:
+            rc = lib.zb3d_pilot_pack_input_blocked(_p(noisy), noisy.stride(0), _p(sigma), n, h, w, LEVEL_SCALE, _p(x),
+                                                   stream)
+        else:
+            rc = lib.zb3d_pilot_pack_input(_p(noisy), _p(sigma), n, h, w, LEVEL_SCALE, _p(x), stream)
+        _ok(rc, "pack_input")
         acts = [x]
-        y = out if out is not None else torch.empty((n, h, w), dtype=torch.float32, device=self.dev)
         last = len(self.shapes) - 1
 
         def conv(x_, l, relu, a_, y0_, resid_):
             cin, cout = self.shapes[l]
             if tc:
                 return lib.zb3d_pilot_conv3x3_tc(_p(x_), n, h, w, cin, _p(self.w16[l]), _p(self.b32[l]), cout, relu,
-                                                 _p(a_), _p(y0_), _p(resid_), None, stream)
+                                                 _p(a_), _p(y0_), _p(resid_), y.stride(0), noisy.stride(0), None,
+                                                 stream)
             return lib.zb3d_pilot_conv3x3(_p(x_), n, h, w, cin, _p(self.w16[l]), _p(self.b32[l]), cout, relu,
                                           None, _p(a_), _p(y0_), _p(resid_), stream)
 
@@ -385,7 +396,7 @@ def time_kernels(width_layers=((32, 8), (48, 10)), w: int = 1920, h: int = 1080,
         yn = torch.empty((1, h, w, cout), dtype=torch.bfloat16, device="cuda")
         st = torch.zeros(1, dtype=torch.int32, device="cuda")
         ttc = timeit(lambda: _ok(lib.zb3d_pilot_conv3x3_tc(_p(xb), 1, h, w, cin, _p(wt), _p(b), cout, 1, _p(yb), None,
-                                                           None, _p(st), None), "conv tc"), reps)
+                                                           None, 0, 0, _p(st), None), "conv tc"), reps)
         tmm = timeit(lambda: _ok(lib.zb3d_pilot_conv3x3(_p(xn), 1, h, w, cin, _p(wt), _p(b), cout, 1, None, _p(yn),
                                                         None, None, None), "conv"), reps)
         if int(st.item()) != 0:

@@ -211,7 +211,7 @@ class DevicePipeline:
 
 
 def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frames: int = 4, nstreams: int = 4,
-                   weights: Optional[str] = None, conv_ctas_per_sm: int = 3):
+                   weights: Optional[str] = None, conv_ctas_per_sm: int = 4):
     """Two-pass BM3Dv2 with the learned pilot (zb3d/pilot.py, shipped weights) as the
     step-2 reference in place of the step-1 estimate, on the same frames: device-resident
     Mpix/s, and PSNR against the clean frames next to the plain two-pass form.
@@ -798,7 +798,7 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other block-matching form")
     ap.add_argument("--no-pilot", action="store_true", help="skip the learned-pilot form")
     ap.add_argument("--pilot-weights", default=None, help="pilot weights (.npz) instead of the shipped ones")
-    ap.add_argument("--pilot-conv-ctas", type=int, default=3,
+    ap.add_argument("--pilot-conv-ctas", type=int, default=4,
                     help="cap on the CTAs per SM of the pilot's convolutions (1 leaves room for step 2 of "
                          "other frames)")
     ap.add_argument("--streams", type=int, default=4, help="CUDA streams the device pipeline spreads frames over")

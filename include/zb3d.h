@@ -291,8 +291,8 @@ int zb3d_pilot_conv3x3(const void *x, int n, int h, int w, int cin, const void *
 int zb3d_pilot_conv3x3_tc(const void *x, int n, int h, int w, int cin, const void *wgt, const float *bias, int cout,
                           int relu, void *y, float *y0, const float *resid, long long y0_stride,
                           long long resid_stride, int *status, void *stream);
-/* Grid of zb3d_pilot_conv3x3_tc for the whole process: at most ctas CTAs per SM (1..3; 3
- * by default, i.e. the layer's own count: 3 up to 32 channels, 2 with 48).  The default
+/* Grid of zb3d_pilot_conv3x3_tc for the whole process: at most ctas CTAs per SM (1..4; 4
+ * by default, i.e. the layer's own count: 4 up to 32 channels, 2 with 48).  The default
  * fills each SM and is fastest alone; 1 leaves room for kernels of other streams.
  * Returns 0, or -1 for an unsupported value. */
 int zb3d_pilot_tc_ctas_per_sm(int ctas);

@@ -28,15 +28,15 @@
 // A run of n output rows takes n + 2 input rows and n + 4 accumulators (the 4 at
 // its ends only collect halo contributions and are discarded).
 //
-// Three CTAs per SM for layers of up to 32 channels, two with 48, each owning a
+// Four CTAs per SM for layers of up to 32 channels, two with 48, each owning a
 // contiguous range of tiles in (image, strip, row) order (balanced to one tile).  The
 // row ring fills the shared memory the weights leave (up to 16 slots).
 //
-// Roles (256 or 384 threads): warp 0 lane 0 issues the TMA row loads, warp 1 lane 0
-// issues the MMAs, warp 2 owns the tensor-memory allocation, and one or two quads of
-// epilogue warps (4-7 and 8-11, warp w on the 32-lane quarter w % 4 of tensor
-// memory) take the accumulators in turn, so that one quad's tensor-memory loads
-// and stores overlap the other's: bias, ReLU, BF16 store
+// Roles (192 or 384 threads): warp 0 lane 0 issues the TMA row loads, warp 1 lane 0
+// issues the MMAs, warp 2 also owns the tensor-memory allocation, and one quad of
+// epilogue warps (2-5) or two (4-7 and 8-11) drain the accumulators, warp w on the
+// 32-lane quarter w % 4 of tensor memory; two quads take the accumulators in turn,
+// so that one quad's tensor-memory loads and stores overlap the other's: bias, ReLU, BF16 store
 // (16 bytes per channel block, 512 contiguous bytes per warp), or for the last
 // layer channel 0 plus the residual in FP32.  mbarriers link the roles; every wait
 // is bounded, and a timeout sets the status word and ends every role early.
@@ -62,7 +62,7 @@ constexpr int BOX_PIX = 130;             // TMA box of 130 single pixels (any wi
 constexpr int BOX_GROUPS = 18;           // TMA box of 18 groups of 8 pixels (width a multiple of 8)
 constexpr int CB_BYTES = BOX_GROUPS * 128;  // one channel block of a staged row (2304 bytes)
 constexpr int MAX_RING = 16;             // staged input row slots, at most
-constexpr int MAX_CTAS_PER_SM = 3;       // independent pipelines per SM, at most
+constexpr int MAX_CTAS_PER_SM = 4;       // independent pipelines per SM, at most
 constexpr unsigned WAIT_LIMIT = 1u << 20;  // try_wait rounds on an mbarrier before giving up (about a second)
 
 struct Args {
@@ -82,14 +82,16 @@ template <int CIN, int COUT>
 struct Shape {
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && 3 * COUT <= 256, "unsupported layer shape");
     static constexpr int CB = CIN / 8;
-    // Pipelines per SM: 3 for layers up to 32 channels, 2 with 48 (their weights and rows
-    // need the shared memory).  With 3, each CTA has one epilogue warp quad and 128
-    // tensor-memory columns; with 2, two quads and 256 columns.
-    static constexpr int CTAS = (CIN <= 32 && COUT <= 32) ? 3 : 2;
-    static constexpr int EPI_GROUPS = CTAS == 3 ? 1 : 2;  // epilogue warp quads, taking accumulators in turn
-    static constexpr int THREADS = 128 + 128 * EPI_GROUPS;
-    static constexpr int TMEM_COLS = CTAS == 3 ? 128 : 256;
-    static constexpr int SMEM_BUDGET = CTAS == 3 ? 72 * 1024 : 112 * 1024;  // ring + weights, per CTA
+    // Pipelines per SM: 4 for layers up to 32 channels, 2 with 48 (their weights and rows
+    // need the shared memory).  With 4, a CTA is 6 warps (producer, MMA, one epilogue quad
+    // in warps 2-5) with 128 tensor-memory columns; with 2, 12 warps (two epilogue quads in
+    // warps 4-11) with 256 columns.
+    static constexpr int CTAS = (CIN <= 32 && COUT <= 32) ? 4 : 2;
+    static constexpr int EPI_GROUPS = CTAS == 4 ? 1 : 2;  // epilogue warp quads, taking accumulators in turn
+    static constexpr int EPI_W0 = CTAS == 4 ? 2 : 4;       // first epilogue warp
+    static constexpr int THREADS = 32 * (EPI_W0 + 4 * EPI_GROUPS);
+    static constexpr int TMEM_COLS = 512 / CTAS;
+    static constexpr int SMEM_BUDGET = CTAS == 4 ? 54 * 1024 : 112 * 1024;  // ring + weights, per CTA
     static constexpr int NACC = TMEM_COLS / COUT;  // accumulator slots
     static_assert(NACC >= 4, "accumulator ring too small");
     static constexpr int KSTEPS = CIN / 16;
@@ -104,6 +106,7 @@ struct Shape {
     static constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
     static constexpr int OFF_BIAS = OFF_MISC + 16;    // after the tensor-memory address and abort flag
     static constexpr int SMEM = OFF_BIAS + COUT * 4 + 128;  // + alignment slack
+    static_assert(CTAS * (SMEM + 1024) <= 228 * 1024, "CTAs per SM exceed the shared memory");
     static constexpr int B_ROWS = 3 * COUT;          // stacked ky blocks of one (kx, channel block)
 };
 
@@ -324,10 +327,10 @@ __global__ void __launch_bounds__(Shape<CIN, COUT>::THREADS, Shape<CIN, COUT>::C
         mma_commit(drain);
         for (unsigned i = 0; i < WAIT_LIMIT && !mbar_try(drain, 0); ++i) {
         }
-    } else if (warp >= 4) {
+    } else if (warp >= S::EPI_W0) {
         // epilogue: warp w drains tensor-memory lanes 32 (w % 4) .. + 31 (pixels of the tile) of
         // the accumulators g with g % S::EPI_GROUPS == its quad
-        const int q = warp & 3, grp = (warp - 4) >> 2;
+        const int q = warp & 3, grp = (warp - S::EPI_W0) >> 2;
         uint32_t g = 0;
         bool ok = true;
         long long tt = t_begin;

@@ -88,23 +88,26 @@ class ClockSampler:
         self._stop = threading.Event()
         self._t = None
         self._nvml = None
+        self._h = None
 
     def _loop(self):
-        nv = self._nvml
-        h = nv.nvmlDeviceGetHandleByIndex(self.index)
-        self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
-        while not self._stop.is_set():
+        nv, h = self._nvml, self._h
+        while True:  # at least one sample, however short the timed region
             try:
                 self.samples.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
                 self.mask |= nv.nvmlDeviceGetCurrentClocksEventReasons(h)
             except Exception:
                 pass
-            self._stop.wait(0.01)
+            if self._stop.wait(0.01):
+                break
 
     def start(self):
+        # NVML set-up (slow on first use) happens here, before the timed region starts
         try:
             import pynvml as nv
             nv.nvmlInit()
+            self._h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(self._h, nv.NVML_CLOCK_SM)
             self._nvml = nv
         except Exception:
             self._nvml = None

@@ -151,3 +151,10 @@ def test_tc_network_on_strided_frame_buffers():
     assert torch.equal(frames[:, 1].cpu(), torch.from_numpy(noisy))
     with pytest.raises(ValueError):
         net.forward(frames[:, 1], sigma, tc=False)  # the NHWC path takes dense images only
+    # one image whose leading (size-1) dimension carries an arbitrary stride, as numpy gives it
+    padded = np.zeros((h, w + 3), np.float32)
+    padded[:, :w] = noisy[0]
+    one = torch.from_numpy(padded[:, :w][None].astype(np.float32)).cuda()
+    assert one.stride(0) != h * w
+    y1, _ = net.forward(one, sigma[:1], tc=True)
+    assert torch.equal(y1, dense[:1])

@@ -134,6 +134,9 @@ class PilotNet:
                     (not tc and n > 1 and t.stride(0) != h * w):
                 raise ValueError(f"zb3d pilot: {what} must be [n][h][w] with dense images")
 
+        def img_stride(t):  # floats between images (a single image's leading stride is arbitrary)
+            return t.stride(0) if n > 1 else h * w
+
         def act(c):  # NHWC for the mma.sync kernels, channel-blocked [n][c/8][h][w][8] for tcgen05
             shape = (n, c // 8, h, w, 8) if tc else (n, h, w, c)
             return torch.empty(shape, dtype=torch.bfloat16, device=self.dev)
@@ -147,8 +150,8 @@ class PilotNet:
             ws = self._ws[key]
         x = ws[0] if reuse else act(16)
         if tc:
-            rc = lib.zb3d_pilot_pack_input_blocked(_p(noisy), noisy.stride(0), _p(sigma), n, h, w, LEVEL_SCALE, _p(x),
-                                                   stream)
+            rc = lib.zb3d_pilot_pack_input_blocked(_p(noisy), img_stride(noisy), _p(sigma), n, h, w, LEVEL_SCALE,
+                                                   _p(x), stream)
         else:
             rc = lib.zb3d_pilot_pack_input(_p(noisy), _p(sigma), n, h, w, LEVEL_SCALE, _p(x), stream)
         _ok(rc, "pack_input")
@@ -159,7 +162,7 @@ class PilotNet:
             cin, cout = self.shapes[l]
             if tc:
                 return lib.zb3d_pilot_conv3x3_tc(_p(x_), n, h, w, cin, _p(self.w16[l]), _p(self.b32[l]), cout, relu,
-                                                 _p(a_), _p(y0_), _p(resid_), y.stride(0), noisy.stride(0), None,
+                                                 _p(a_), _p(y0_), _p(resid_), img_stride(y), img_stride(noisy), None,
                                                  stream)
             return lib.zb3d_pilot_conv3x3(_p(x_), n, h, w, cin, _p(self.w16[l]), _p(self.b32[l]), cout, relu,
                                           None, _p(a_), _p(y0_), _p(resid_), stream)

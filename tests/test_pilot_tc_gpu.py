@@ -158,3 +158,25 @@ def test_tc_network_on_strided_frame_buffers():
     assert one.stride(0) != h * w
     y1, _ = net.forward(one, sigma[:1], tc=True)
     assert torch.equal(y1, dense[:1])
+
+
+def test_pilot_runs_on_torchs_current_stream():
+    """Launches follow torch's current stream (its allocator orders the buffer reuse); a
+    different explicit stream is refused."""
+    import torch
+    net = P.PilotNet(seed=1)
+    x = torch.rand((1, 24, 160), device="cuda")
+    sig = torch.tensor([10.0], device="cuda")
+    ref, _ = net.forward(x, sig, tc=True)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        y, _ = net.forward(x, sig, tc=True)  # on s, with buffers of its own
+        y2, _ = net.forward(x, sig, tc=True, stream=s.cuda_stream)
+    torch.cuda.synchronize()
+    assert torch.equal(y, ref) and torch.equal(y2, ref)
+    with pytest.raises(ValueError):
+        net.forward(x, sig, tc=True, stream=s.cuda_stream)  # s is not the current stream here
+    # the buffer cache stays bounded across many shapes
+    for k in range(P.WS_KEEP + 4):
+        net.forward(torch.rand((1, 16, 64 + 8 * k), device="cuda"), sig, tc=True)
+    assert len(net._ws) <= P.WS_KEEP

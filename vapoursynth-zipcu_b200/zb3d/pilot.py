@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+from collections import OrderedDict
 from typing import Optional, Sequence
 
 import numpy as np
@@ -38,6 +39,7 @@ SHAPES = arch(32, 8)                                 # the default (and shipped)
 REAL_IN, REAL_OUT = 2, 1
 LEVEL_SCALE = 4.0                                    # noise-level plane = sigma / 255 * LEVEL_SCALE
 LOSS_SCALE = 1024.0                                  # keeps BF16 gradients clear of underflow
+WS_KEEP = 8                                          # inference buffer sets kept per network
 
 
 def _p(t) -> int:
@@ -74,7 +76,9 @@ class PilotNet:
             self.keep.append((torch.from_numpy(k).to(device), torch.from_numpy(kb).to(device)))
         self.w16 = [torch.empty(w.shape, dtype=torch.bfloat16, device=device) for w in self.w32]
         self.wt16 = [torch.empty((cin, 3, 3, cout), dtype=torch.bfloat16, device=device) for cin, cout in self.shapes]
-        self._ws = {}  # inference activation buffers per (n, h, w, stream), reused across calls
+        # inference activation buffers per (n, h, w, stream), reused across calls; the least
+        # recently used shapes are dropped beyond WS_KEEP
+        self._ws: "OrderedDict[tuple, list]" = OrderedDict()
         self.m = [(torch.zeros_like(w), torch.zeros_like(b)) for w, b in zip(self.w32, self.b32)]
         self.v = [(torch.zeros_like(w), torch.zeros_like(b)) for w, b in zip(self.w32, self.b32)]
         self.step_count = 0
@@ -119,12 +123,19 @@ class PilotNet:
         Returns y = noisy + net output (float32 [n][h][w], written to `out` if given)
         and, with keep_acts, the stored BF16 activations of every layer's input (NHWC, or
         channel-blocked [n][c/8][h][w][8] with tc).
-        `stream`: a CUDA stream handle (int) for every launch, or None for the default.
+        `stream`: a CUDA stream handle (int) for every launch, or None for torch's current
+        stream; it must be torch's current stream (e.g. inside `torch.cuda.stream(s)`), so
+        that the allocator orders the reuse of this call's buffers after its kernels.
         tc: convolutions on the tensor cores (tcgen05); default for inference (no keep_acts),
         while the training passes keep the mma.sync kernels their gradients are checked with."""
         torch, lib = self.torch, N.lib()
         if tc is None:
             tc = not keep_acts
+        current = torch.cuda.current_stream().cuda_stream
+        if stream is None:
+            stream = current or None  # the legacy default stream is NULL
+        elif stream != current:
+            raise ValueError("zb3d pilot: stream must be torch's current stream")
         n, h, w = noisy.shape
         y = out if out is not None else torch.empty((n, h, w), dtype=torch.float32, device=self.dev)
         for t, what in ((noisy, "noisy"), (y, "out")):
@@ -147,6 +158,11 @@ class PilotNet:
             key = (n, h, w, stream)
             if key not in self._ws:
                 self._ws[key] = [act(16), act(self.width), act(self.width)]
+                while len(self._ws) > WS_KEEP:
+                    # the dropped buffers were allocated on, and used on, the stream of their
+                    # key, so the allocator orders any reuse of their memory after their kernels
+                    self._ws.popitem(last=False)
+            self._ws.move_to_end(key)
             ws = self._ws[key]
         x = ws[0] if reuse else act(16)
         if tc:

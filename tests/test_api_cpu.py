@@ -147,3 +147,29 @@ def test_processed_planes_rule():
     assert zb3d._processed_planes(None, 3) == [True, True, True]
     assert zb3d._processed_planes([3.0, 0.0], 3) == [True, False, False]
     assert zb3d._processed_planes([0.0, 2.0], 3) == [False, True, True]
+
+
+def test_pilot_abi_argument_checks_need_no_gpu():
+    """The learned pilot's C entry points validate their arguments before any CUDA call."""
+    lib = N.lib()
+    # CTA cap of the tensor-core convolution: 1..4
+    for bad in (0, 5, -1):
+        assert lib.zb3d_pilot_tc_ctas_per_sm(bad) == -1
+    for ok in (1, 2, 3, 4):
+        assert lib.zb3d_pilot_tc_ctas_per_sm(ok) == 0
+    fake = 0x10000  # 16-byte aligned, never dereferenced: every call below fails its checks first
+    h, w = 32, 48
+    # image strides shorter than an image are refused
+    assert lib.zb3d_pilot_pack_input_blocked(fake, h * w - 1, fake, 2, h, w, 4.0, fake, None) == -1
+    assert lib.zb3d_pilot_conv3x3_tc(fake, 2, h, w, 32, fake, None, 16, 0, None, fake, fake, h * w - 1, 0, None,
+                                     None) == -1
+    assert lib.zb3d_pilot_conv3x3_tc(fake, 2, h, w, 32, fake, None, 16, 0, None, fake, fake, 0, h * w - 1, None,
+                                     None) == -1
+    # misaligned operands and unsupported layer shapes are refused
+    assert lib.zb3d_pilot_conv3x3_tc(fake + 4, 1, h, w, 32, fake, None, 32, 1, fake, None, None, 0, 0, None,
+                                     None) == -1
+    assert lib.zb3d_pilot_conv3x3_tc(fake, 1, h, w, 24, fake, None, 32, 1, fake, None, None, 0, 0, None, None) == -1
+    assert lib.zb3d_pilot_conv3x3_tc(fake, 1, h, w, 64, fake, None, 64, 1, fake, None, None, 0, 0, None, None) == -1
+    # empty batches are a no-op
+    assert lib.zb3d_pilot_pack_input_blocked(fake, 0, fake, 0, h, w, 4.0, fake, None) == 0
+    assert lib.zb3d_pilot_conv3x3_tc(fake, 0, h, w, 32, fake, None, 32, 1, fake, None, None, 0, 0, None, None) == 0

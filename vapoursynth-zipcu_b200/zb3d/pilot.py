@@ -30,12 +30,12 @@ from . import synth
 
 
 
-def arch(width: int = 32, layers: int = 8) -> list:
+def arch(width: int = 32, layers: int = 6) -> list:
     """(cin, cout) of each layer; the 2 input and 1 output channels are padded to 16."""
     return [(16, width)] + [(width, width)] * (layers - 2) + [(width, 16)]
 
 
-SHAPES = arch(32, 8)                                 # the default (and shipped) architecture
+SHAPES = arch(32, 6)                                 # the default (and shipped) architecture
 REAL_IN, REAL_OUT = 2, 1
 LEVEL_SCALE = 4.0                                    # noise-level plane = sigma / 255 * LEVEL_SCALE
 LOSS_SCALE = 1024.0                                  # keeps BF16 gradients clear of underflow
@@ -54,7 +54,7 @@ def _ok(rc: int, what: str):
 class PilotNet:
     """The network, its FP32 master weights and Adam state, on one CUDA device."""
 
-    def __init__(self, seed: int = 0, device: str = "cuda", width: int = 32, layers: int = 8):
+    def __init__(self, seed: int = 0, device: str = "cuda", width: int = 32, layers: int = 6):
         import torch
         self.torch, self.dev = torch, device
         self.width, self.layers = width, layers
@@ -349,20 +349,22 @@ class PilotGate:
 # ---------------------------------------------------------------------------------------
 import os as _os
 
-WEIGHTS = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_bs4_r12.npz")  # 32 ch x 8 layers
-# the 48-channel, 10-layer net, trained by `python -m zb3d.pilot train --width 48 --layers 10`
+# 32 ch x 6 layers, trained by `python -m zb3d.pilot train` with its defaults
+WEIGHTS = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_bs4_r12.npz")
+# the 48-channel, 10-layer net, trained by
+# `python -m zb3d.pilot train --width 48 --layers 10 --frames 6 --dims 1920x1080,960x540 --steps 12500`
 WEIGHTS_W48_L10 = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_w48_l10_bs4_r12.npz")
 # 48 ch x 10 layers trained on 3840x2160 planes:
-# `python -m zb3d.pilot train --width 48 --layers 10 --dims 3840x2160 --frames 4`
+# `python -m zb3d.pilot train --width 48 --layers 10 --dims 3840x2160 --frames 4 --steps 12500`
 WEIGHTS_4K = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_w48_l10_4k_bs4_r12.npz")
 TRAIN_KW = dict(block_step=4, bm_range=12)   # step-1 configuration the shipped pilot imitates
 TRAIN_SIGMAS = (5.0, 10.0, 15.0, 20.0, 25.0)
 
 
-def shipped(device: str = "cuda", width: int = 32, layers: int = 8) -> PilotNet:
+def shipped(device: str = "cuda", width: int = 32, layers: int = 6) -> PilotNet:
     """A pilot trained by `python -m zb3d.pilot train` (weights next to this file): the
-    default 32 ch x 8 layers, or 48 ch x 10 layers."""
-    paths = {(32, 8): WEIGHTS, (48, 10): WEIGHTS_W48_L10}
+    default 32 ch x 6 layers, or 48 ch x 10 layers."""
+    paths = {(32, 6): WEIGHTS, (48, 10): WEIGHTS_W48_L10}
     if (width, layers) not in paths:
         raise ValueError(f"no shipped pilot of {width} channels x {layers} layers")
     return PilotNet.load(paths[(width, layers)], device=device)
@@ -385,7 +387,7 @@ def evaluate(net: PilotNet, sigmas=TRAIN_SIGMAS, frames: int = 4, size: int = 38
     return rows
 
 
-def time_kernels(width_layers=((32, 8), (48, 10)), w: int = 1920, h: int = 1080, reps: int = 20) -> list:
+def time_kernels(width_layers=((32, 6), (48, 10)), w: int = 1920, h: int = 1080, reps: int = 20) -> list:
     """CUDA-event times of the inference convolution per layer shape on one w x h plane
     (tcgen05 and mma.sync), and of whole nets on a YUV420 frame (the plane plus two
     half-size planes).  Lines of text."""
@@ -442,12 +444,14 @@ def main(argv=None):
     import argparse
     ap = argparse.ArgumentParser(prog="python -m zb3d.pilot")
     ap.add_argument("cmd", choices=["train", "eval", "time"])
-    ap.add_argument("--frames", type=int, default=6, help="training frames per noise level and frame size")
-    ap.add_argument("--dims", default="1920x1080,960x540", help="training frame sizes (the 1080p YUV420 planes)")
-    ap.add_argument("--steps", type=int, default=6250, help="Adam steps of 32 crops (6250 = 200k crops)")
+    ap.add_argument("--frames", type=int, default=16, help="training frames per noise level and frame size")
+    ap.add_argument("--dims", default="1920x1080,1920x1080,1920x1080,960x540",
+                    help="training frame sizes of the 1080p YUV420 planes; a size listed k times contributes k "
+                         "sets of frames (luma-sized planes weigh 3:1 by default)")
+    ap.add_argument("--steps", type=int, default=25000, help="Adam steps of 32 crops (25000 = 800k crops)")
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--width", type=int, default=32, help="channels of the hidden layers (16, 32 or 48)")
-    ap.add_argument("--layers", type=int, default=8, help="number of 3x3 convolutions")
+    ap.add_argument("--layers", type=int, default=6, help="number of 3x3 convolutions")
     ap.add_argument("--out", default=WEIGHTS)
     a = ap.parse_args(argv)
     import time

@@ -939,12 +939,13 @@ def main():
         if pipe is not None:
             pipe.close()
             pipe = None
-        out["pilot_form"] = run_pilot_form(torch, frames, rank, max(1, args.steps // 4), 1,
+        # timed over the same K steps as the plain form (8 frames each)
+        out["pilot_form"] = run_pilot_form(torch, frames, rank, args.steps, 1,
                                            weights=args.pilot_weights, conv_ctas_per_sm=args.pilot_conv_ctas)
         if args.pilot_weights is None:
             # the 48-channel, 10-layer net of the learned-pilot configuration, on the same frames
             from zb3d import pilot as P
-            out["pilot_form_w48_l10"] = run_pilot_form(torch, frames, rank, max(1, args.steps // 4), 1,
+            out["pilot_form_w48_l10"] = run_pilot_form(torch, frames, rank, args.steps, 1,
                                                        weights=P.WEIGHTS_W48_L10,
                                                        conv_ctas_per_sm=args.pilot_conv_ctas)
     if rank == 0 and not args.no_ref_cuda:

@@ -306,12 +306,19 @@ __global__ void __launch_bounds__(128) zb_match_tiled(MatchArgs a) {
 // and odd-row partial sums, which advance together: acc = fma2(d, d, acc)
 // computes the reference's e0 and e1 chains in one instruction and acc.x + acc.y
 // is their join.  d = n + (-c) = -(c - n) exactly, so d*d is the reference's
-// square.  Pair rows are padded by 4 floats every 32 so the lanes' float4 loads
-// do not collide on banks.
+// square.  A pair row is a run of 16-byte chunks (two columns each), 128-byte
+// aligned; chunk c sits at c ^ ((c >> 3) & 1), so in the odd 128-byte lines of a
+// row the chunks of a pair swap places.  Eight lanes reading every second chunk
+// from any start then hit eight distinct bank quads: their float4 loads do not
+// collide on banks.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int pair_off(int col) {  // float offset of column `col` in a pair row
-    const int f = 2 * col;
-    return f + (f >> 5) * 4;
+    const int c = col >> 1;
+    return 4 * (c ^ ((c >> 3) & 1)) + 2 * (col & 1);
+}
+
+__host__ __device__ constexpr int pair_pitch(int tile_pitch) {  // floats per pair row
+    return (2 * tile_pitch + 31) & ~31;
 }
 
 __device__ __forceinline__ float2 f4lo(const float4 &v) { return make_float2(v.x, v.y); }
@@ -359,7 +366,7 @@ __global__ void __launch_bounds__(128) zb_match_tiled2(MatchArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     constexpr int NBW = SHARED ? 31 : 16;
     const int R = a.range, W = a.w, H = a.h, tp = a.tile_pitch;
-    const int pp = pair_off(tp) + 4;  // pair-row pitch in floats (multiple of 4)
+    const int pp = pair_pitch(tp);
     const int kx0 = blockIdx.x * NBW;
     const int x0 = kx0 * BS;
     const int by0 = blockIdx.y * nw;
@@ -910,9 +917,7 @@ static cudaError_t launch_tiled_t(const MatchArgs &a, int rows_per_cta, cudaStre
 
 // packed FP32x2 SSD kernel: two pair-interleaved copies of the tile
 static size_t match_tile2_bytes(const MatchArgs &a, int rows_per_cta) {
-    const int f = 2 * a.tile_pitch;
-    const int pp = f + (f >> 5) * 4 + 4;
-    return (size_t)((rows_per_cta - 1) * a.bs + 2 * a.range + 8) * pp * sizeof(float);
+    return (size_t)((rows_per_cta - 1) * a.bs + 2 * a.range + 8) * pair_pitch(a.tile_pitch) * sizeof(float);
 }
 
 template <bool SHARED, int BS>

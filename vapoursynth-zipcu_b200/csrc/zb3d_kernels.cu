@@ -915,7 +915,7 @@ static cudaError_t launch_tiled_t(const MatchArgs &a, int rows_per_cta, cudaStre
     return cudaGetLastError();
 }
 
-// packed FP32x2 SSD kernel: two pair-interleaved copies of the tile
+// packed FP32x2 SSD kernel: two pair-interleaved copies of the tile (swizzled pair rows)
 static size_t match_tile2_bytes(const MatchArgs &a, int rows_per_cta) {
     return (size_t)((rows_per_cta - 1) * a.bs + 2 * a.range + 8) * pair_pitch(a.tile_pitch) * sizeof(float);
 }

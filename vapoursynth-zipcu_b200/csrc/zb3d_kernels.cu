@@ -657,186 +657,240 @@ __global__ void __launch_bounds__(128) zb_match_temporal(MatchArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Collaborative filtering (vszipcu src/bm3d.cu:392-546) and aggregation.
-// 8 lanes per group, lane j holds column j of every patch (64 values).  The
-// forward 3D transform runs vertical, horizontal (between two transposes), then
-// across the 8 patches; the inverse runs in the reference's order too, so every
-// coefficient and every keep/drop decision equals the reference's.
+// Collaborative filtering (vszipcu src/bm3d.cu:392-546) and aggregation into
+// signed 64-bit fixed point.
 // ---------------------------------------------------------------------------
 static constexpr int kFilterWarps = 4;
-static constexpr int kTransStride = 72;  // 8 rows x 9 (padded) floats per group and patch
-
-// 8x8 transpose of each patch inside the lane group, through shared memory.
-// Lane j's value i moves to lane i, value j.  Bank-conflict free: a group is 8
-// consecutive banks at a stride of 8 per group, rows padded to 9.
-__device__ __forceinline__ void group_transpose(float (&d)[64], float *buf, int g, int j, unsigned gm) {
-    __syncwarp(gm);
-#pragma unroll
-    for (int p = 0; p < 8; ++p)
-#pragma unroll
-        for (int i = 0; i < 8; ++i) buf[(p * 4 + g) * kTransStride + i * 9 + j] = d[p * 8 + i];
-    __syncwarp(gm);
-#pragma unroll
-    for (int p = 0; p < 8; ++p)
-#pragma unroll
-        for (int i = 0; i < 8; ++i) d[p * 8 + i] = buf[(p * 4 + g) * kTransStride + j * 9 + i];
-}
-
-template <class T2, class T1>
-__device__ __forceinline__ void forward3(float (&d)[64], float *buf, int g, int j, unsigned gm) {
-#pragma unroll
-    for (int p = 0; p < 8; ++p) T2::fwd(&d[p * 8]);
-    group_transpose(d, buf, g, j, gm);
-#pragma unroll
-    for (int p = 0; p < 8; ++p) T2::fwd(&d[p * 8]);
-    group_transpose(d, buf, g, j, gm);
-#pragma unroll
-    for (int v = 0; v < 8; ++v) {
-        float t[8];
-#pragma unroll
-        for (int p = 0; p < 8; ++p) t[p] = d[p * 8 + v];
-        T1::fwd(t);
-#pragma unroll
-        for (int p = 0; p < 8; ++p) d[p * 8 + v] = t[p];
-    }
-}
-
-template <class T2, class T1>
-__device__ __forceinline__ void inverse3(float (&d)[64], float *buf, int g, int j, unsigned gm) {
-#pragma unroll
-    for (int p = 0; p < 8; ++p) T2::inv(&d[p * 8]);
-    group_transpose(d, buf, g, j, gm);
-#pragma unroll
-    for (int p = 0; p < 8; ++p) T2::inv(&d[p * 8]);
-    group_transpose(d, buf, g, j, gm);
-#pragma unroll
-    for (int v = 0; v < 8; ++v) {
-        float t[8];
-#pragma unroll
-        for (int p = 0; p < 8; ++p) t[p] = d[p * 8 + v];
-        T1::inv(t);
-#pragma unroll
-        for (int p = 0; p < 8; ++p) d[p * 8 + v] = t[p];
-    }
-}
-
-__device__ __forceinline__ float group_sum(float k, unsigned gm) {
-    k += __shfl_xor_sync(gm, k, 1, 8);
-    k += __shfl_xor_sync(gm, k, 2, 8);
-    k += __shfl_xor_sync(gm, k, 4, 8);
-    return k;
-}
 
 __device__ __forceinline__ unsigned long long to_fix(float v) {
     return (unsigned long long)__float2ll_rn(v * kFixScale);
 }
 
+// ---------------------------------------------------------------------------
+// Collaborative filtering with 16 lanes per group.  Lane (j, h), j = 0..7,
+// h = 0..1, holds 32 of the group's 512 values, half of what a lane of an
+// 8-lane group holds, so twice as many groups are resident per SM.  Every 1-D
+// transform still runs on 8 values inside one lane, in the reference's order;
+// between transforms the values move through shared memory.  The layouts
+// (q, t = 0..3; the half h takes the interleaved indices 2q + h, 2t + h):
+//   A  column x = j of patches 2q + h, all rows          gather, vertical forward
+//   B  row fy = j of patches 2q + h, all columns         horizontal forward
+//   C  column fx = j, rows fy = 2t + h, all patches      across patches (Wiener coefficients)
+//   D  column fx = j of spectra 2q + h, all rows         shrinkage, vertical inverse
+//   E  row y = j of spectra 2q + h, all columns          horizontal inverse
+//   F  column x = j, rows y = 2t + h, all patches        inverse across patches, aggregation
+// Registers: A, B, D, E as d[q * 8 + i]; C, F as d[p * 4 + t].  The strides of the
+// three kinds of move (A->B and D->E, B->C and E->F, C->D) were chosen so that the
+// 32 lanes of a warp (two groups) touch 32 distinct banks on every store and load.
+// The shrinkage runs in layout D with the vertical inverse directly after it in
+// registers, the same code shape as the reference (src/bm3d.cu:445, 457-478): its
+// transforms write a * b + c and leave the fusing into FMAs to the compiler, and
+// the compiler fuses this stage the reference's way only in that shape.
+// ---------------------------------------------------------------------------
+static constexpr int kGroupBuf = 592;    // floats per group in the move buffer
+static constexpr int kCoeffBuf = 592;    // floats per group in the Wiener coefficient buffer
+
+// A -> B and D -> E: 8x8 transpose of each of the lane's four patches
+__device__ __forceinline__ void move_tr(float (&d)[32], float *gb, int h, int j, unsigned gm) {
+    __syncwarp(gm);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) gb[(2 * q + h) * 72 + i + 9 * j] = d[q * 8 + i];
+    __syncwarp(gm);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) d[q * 8 + i] = gb[(2 * q + h) * 72 + j + 9 * i];
+}
+
+// B -> C and E -> F: (patch 2q + h, row j, column i) -> (patch p, row 2t + h, column j)
+__device__ __forceinline__ void move_bc(float (&d)[32], float *gb, int h, int j, unsigned gm) {
+    __syncwarp(gm);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) gb[(2 * q + h) * 72 + 9 * j + 2 * i] = d[q * 8 + i];
+    __syncwarp(gm);
+#pragma unroll
+    for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) d[p * 4 + t] = gb[p * 72 + 9 * (2 * t + h) + 2 * j];
+}
+
+// C -> D: (spectrum p, row 2t + h, column j) -> (spectrum 2q + h, row i, column j)
+__device__ __forceinline__ void move_cd(float (&d)[32], float *gb, int h, int j, unsigned gm) {
+    __syncwarp(gm);
+#pragma unroll
+    for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) gb[p * 72 + 8 * (2 * t + h) + j] = d[p * 4 + t];
+    __syncwarp(gm);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) d[q * 8 + i] = gb[(2 * q + h) * 72 + 8 * i + j];
+}
+
+// layout A -> layout C through the forward 3D transform
+template <class T2, class T1>
+__device__ __forceinline__ void forward3_16(float (&d)[32], float *gb, int h, int j, unsigned gm) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) T2::fwd(&d[q * 8]);
+    move_tr(d, gb, h, j, gm);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) T2::fwd(&d[q * 8]);
+    move_bc(d, gb, h, j, gm);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        float v[8];
+#pragma unroll
+        for (int p = 0; p < 8; ++p) v[p] = d[p * 4 + t];
+        T1::fwd(v);
+#pragma unroll
+        for (int p = 0; p < 8; ++p) d[p * 4 + t] = v[p];
+    }
+}
+
+// layout D (after the shrinkage) -> layout F through the rest of the inverse 3D
+// transform: vertical, horizontal, then across patches
+template <class T2, class T1>
+__device__ __forceinline__ void inverse3_16(float (&d)[32], float *gb, int h, int j, unsigned gm) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) T2::inv(&d[q * 8]);
+    move_tr(d, gb, h, j, gm);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) T2::inv(&d[q * 8]);
+    move_bc(d, gb, h, j, gm);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        float v[8];
+#pragma unroll
+        for (int p = 0; p < 8; ++p) v[p] = d[p * 4 + t];
+        T1::inv(v);
+#pragma unroll
+        for (int p = 0; p < 8; ++p) d[p * 4 + t] = v[p];
+    }
+}
+
+// the lane's four patches 2q + h, column j, into layout A
+__device__ __forceinline__ void gather16(float (&d)[32], const float *plane, const FilterArgs &a, long long grp,
+                                         int h, int j) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int2 v = a.list[grp * 8 + 2 * q + h];
+        const float *s = plane + ((unsigned)v.y >> 24) * a.frame_stride + (long long)(v.y & 0xffffff) * a.pitch + v.x + j;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) d[q * 8 + i] = __ldg(s + i * a.pitch);
+    }
+}
+
 template <bool FINAL, int T2D, int T1D>
-__global__ void __launch_bounds__(kFilterWarps * 32) zb_filter(FilterArgs a) {
+__global__ void __launch_bounds__(kFilterWarps * 32) zb_filter16(FilterArgs a) {
     using T2 = typename TransformOf<T2D>::type;
     using T1 = typename TransformOf<T1D>::type;
-    __shared__ float tbuf[kFilterWarps][8 * 4 * kTransStride];
-    // Wiener: the 64 coefficients of each thread, parked while its noisy group is transformed
-    // (dynamic shared memory [64][threads]; none for the hard-threshold pass)
+    __shared__ float tbuf[kFilterWarps * 2 * kGroupBuf];
+    // Wiener: the group's 512 coefficients at [spectrum * 72 + row * 8 + column]
     extern __shared__ float cbuf[];
     const int lane = threadIdx.x & 31;
-    const int j = lane & 7, g = lane >> 3;
-    const unsigned gm = 0xffu << (lane & 24);
-    const long long grp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+    const int j = lane & 7, h = (lane >> 3) & 1, gw = lane >> 4;
+    const unsigned gm = 0xffffu << (lane & 16);
+    const long long grp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
     if (grp >= a.nblocks) return;
-    float *buf = tbuf[threadIdx.x >> 5];
-
-    int px[8], py[8], pz[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int2 v = a.list[grp * 8 + i];
-        px[i] = v.x;
-        py[i] = v.y & 0xffffff;
-        pz[i] = (unsigned)v.y >> 24;
-    }
+    float *gb = tbuf + ((threadIdx.x >> 5) * 2 + gw) * kGroupBuf;
+    float *cb = cbuf + (threadIdx.x >> 4) * kCoeffBuf;
     const float E = a.extractor;
 
-    for (int p = 0; p < a.nplanes; ++p) {
-        const float sigma = p == 0 ? a.sigma[0] : (p == 1 ? a.sigma[1] : a.sigma[2]);
+    for (int pl = 0; pl < a.nplanes; ++pl) {
+        const float sigma = pl == 0 ? a.sigma[0] : (pl == 1 ? a.sigma[1] : a.sigma[2]);
         if (a.chroma && sigma < ZB_FLT_EPS) continue;
+        float d[32];
         float k = 0.0f;
         if constexpr (FINAL) {
-            // The reference (basic estimate) first: its 3D transform gives the Wiener
-            // coefficients r^2 / (r^2 + sigma^2), parked in shared memory, so that only one
-            // 64-value group is live in registers at a time.  The reference rounds r^2 once
-            // and adds sigma^2 (no fused multiply-add in the denominator); k accumulates by FMA.
-            float rf[64];
-            const float *rp = a.src + p * a.plane_stride;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const float *q = rp + pz[i] * a.frame_stride + (long long)py[i] * a.pitch + px[i] + j;
-#pragma unroll
-                for (int r = 0; r < 8; ++r) rf[i * 8 + r] = __ldg(q + r * a.pitch);
-            }
-            forward3<T2, T1>(rf, buf, g, j, gm);
+            // Wiener coefficients r^2 / (r^2 + sigma^2) of the basic estimate's spectrum (the
+            // reference rounds r^2 once and adds sigma^2 without FMA), then the weight's sum of
+            // squared coefficients, accumulated by FMA over spectrum and row for column j in
+            // the reference's order: every lane runs the full chain of its column
+            gather16(d, a.src + pl * a.plane_stride, a, grp, h, j);
+            forward3_16<T2, T1>(d, gb, h, j, gm);
             const float s2 = sigma * sigma;
 #pragma unroll
-            for (int i = 0; i < 64; ++i) {
-                const float rv = rf[i];
-                const float r2 = __fmul_rn(rv, rv);
-                float coeff = r2 / __fadd_rn(r2, s2);
-                if (i == 0) coeff = j ? coeff : 1.0f;
-                k = __fmaf_rn(coeff, coeff, k);
-                cbuf[i * kFilterWarps * 32 + threadIdx.x] = coeff;
-            }
-            asm volatile("" ::: "memory");  // keep the noisy loads below: one group live at a time
-        }
-        const float *sp = a.src + (FINAL ? a.clip_stride : 0) + p * a.plane_stride;
-        float d[64];
+            for (int p = 0; p < 8; ++p)
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const float *q = sp + pz[i] * a.frame_stride + (long long)py[i] * a.pitch + px[i] + j;
+                for (int t = 0; t < 4; ++t) {
+                    const float rv = d[p * 4 + t];
+                    const float r2 = __fmul_rn(rv, rv);
+                    float coeff = r2 / __fadd_rn(r2, s2);
+                    if (p == 0 && t == 0 && h == 0 && j == 0) coeff = 1.0f;
+                    cb[p * 72 + (2 * t + h) * 8 + j] = coeff;
+                }
+            __syncwarp(gm);
+#pragma unroll 8
+            for (int p = 0; p < 8; ++p)
 #pragma unroll
-            for (int r = 0; r < 8; ++r) d[i * 8 + r] = __ldg(q + r * a.pitch);
+                for (int r = 0; r < 8; ++r) {
+                    const float c = cb[p * 72 + r * 8 + j];
+                    k = __fmaf_rn(c, c, k);
+                }
+            k += __shfl_xor_sync(gm, k, 1, 8);
+            k += __shfl_xor_sync(gm, k, 2, 8);
+            k += __shfl_xor_sync(gm, k, 4, 8);
         }
-        forward3<T2, T1>(d, buf, g, j, gm);
+        gather16(d, a.src + (FINAL ? a.clip_stride : 0) + pl * a.plane_stride, a, grp, h, j);
+        forward3_16<T2, T1>(d, gb, h, j, gm);
+        // shrinkage in layout D, right before the vertical inverse: d[q * 8 + i] is
+        // spectrum 2q + h, row i, column j
+        move_cd(d, gb, h, j, gm);
         if constexpr (!FINAL) {
 #pragma unroll
-            for (int i = 0; i < 64; ++i) {
-                const float val = d[i];
-                const float thr = (i == 0 && j == 0) ? 0.0f : sigma;
-                const float flag = fabsf(val) >= thr;
-                k += flag;
-                d[i] = flag ? (val * (1.0f / 4096.0f)) : 0.0f;
-            }
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const float val = d[q * 8 + i];
+                    const float thr = (q == 0 && i == 0 && h == 0 && j == 0) ? 0.0f : sigma;
+                    const float flag = fabsf(val) >= thr;
+                    k += flag;
+                    d[q * 8 + i] = flag ? (val * (1.0f / 4096.0f)) : 0.0f;
+                }
+            // kept-coefficient count: integer-valued, exact in any order
+            k += __shfl_xor_sync(gm, k, 1, 16);
+            k += __shfl_xor_sync(gm, k, 2, 16);
+            k += __shfl_xor_sync(gm, k, 4, 16);
+            k += __shfl_xor_sync(gm, k, 8, 16);
         } else {
 #pragma unroll
-            for (int i = 0; i < 64; ++i) {
-                float val = d[i];
-                val *= cbuf[i * kFilterWarps * 32 + threadIdx.x];
-                d[i] = val * (1.0f / 4096.0f);
-            }
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    float val = d[q * 8 + i];
+                    val *= cb[(2 * q + h) * 72 + i * 8 + j];
+                    d[q * 8 + i] = val * (1.0f / 4096.0f);
+                }
         }
-        k = group_sum(k, gm);
         const float w = 1.0f / k;
-        inverse3<T2, T1>(d, buf, g, j, gm);
+        inverse3_16<T2, T1>(d, gb, h, j, gm);
 
-        unsigned long long *num = a.num + p * a.acc_plane_stride;
+        unsigned long long *num = a.num + pl * a.acc_plane_stride;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            unsigned long long *q = num + pz[i] * a.acc_frame_stride + (long long)py[i] * a.pitch + px[i] + j;
+        for (int p = 0; p < 8; ++p) {
+            const int2 v = a.list[grp * 8 + p];
+            unsigned long long *q = num + ((unsigned)v.y >> 24) * a.acc_frame_stride +
+                                    (long long)(v.y & 0xffffff) * a.pitch + v.x + j;
 #pragma unroll
-            for (int r = 0; r < 8; ++r) {
-                const float v = __fmaf_rn(w, d[i * 8 + r], E) - E;
-                atomicAdd(q + r * a.pitch, to_fix(v));
+            for (int t = 0; t < 4; ++t) {
+                const float val = __fmaf_rn(w, d[p * 4 + t], E) - E;
+                atomicAdd(q + (2 * t + h) * a.pitch, to_fix(val));
             }
         }
-        const float wq = (w + E) - E;
-        // lane j books the weight of patch j once, at its origin
-        int zx = px[0], zy = py[0], zz = pz[0];
-#pragma unroll
-        for (int i = 1; i < 8; ++i)
-            if (i == j) {
-                zx = px[i];
-                zy = py[i];
-                zz = pz[i];
-            }
-        atomicAdd(a.den + p * a.acc_plane_stride + zz * a.acc_frame_stride + (long long)zy * a.pitch + zx, to_fix(wq));
+        if (h == 0) {
+            // lane j books the weight of patch j once, at its origin
+            const float wq = (w + E) - E;
+            const int2 v = a.list[grp * 8 + j];
+            atomicAdd(a.den + pl * a.acc_plane_stride + ((unsigned)v.y >> 24) * a.acc_frame_stride +
+                          (long long)(v.y & 0xffffff) * a.pitch + v.x,
+                      to_fix(wq));
+        }
+        __syncwarp(gm);  // the coefficient buffer is rewritten by the next plane
     }
 }
 
@@ -1020,10 +1074,10 @@ temporal:
 
 template <bool FINAL, int T2D, int T1D>
 static cudaError_t launch_filter_t(const FilterArgs &a, cudaStream_t st) {
-    const long long threads = (long long)a.nblocks * 8;
+    const long long threads = (long long)a.nblocks * 16;
     const int tpb = kFilterWarps * 32;
-    const int dyn = FINAL ? 64 * tpb * (int)sizeof(float) : 0;  // Wiener coefficient buffer
-    auto k = zb_filter<FINAL, T2D, T1D>;
+    const int dyn = FINAL ? (tpb / 16) * kCoeffBuf * (int)sizeof(float) : 0;  // Wiener coefficient buffer
+    auto k = zb_filter16<FINAL, T2D, T1D>;
     if (FINAL) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
         if (e != cudaSuccess) return e;

@@ -810,34 +810,40 @@ __global__ void __launch_bounds__(kFilterWarps * 32) zb_filter16(FilterArgs a) {
             // Wiener coefficients r^2 / (r^2 + sigma^2) of the basic estimate's spectrum (the
             // reference rounds r^2 once and adds sigma^2 without FMA), then the weight's sum of
             // squared coefficients, accumulated by FMA over spectrum and row for column j in
-            // the reference's order: every lane runs the full chain of its column
+            // the reference's order: every lane runs the full chain of its column.  The basic
+            // estimate and the noisy patches share one copy of the forward transform's code.
+            const float s2 = sigma * sigma;
+#pragma unroll 1
+            for (int pass = 0; pass < 2; ++pass) {
+                gather16(d, a.src + (pass ? a.clip_stride : 0) + pl * a.plane_stride, a, grp, h, j);
+                forward3_16<T2, T1>(d, gb, h, j, gm);
+                if (pass) break;
+#pragma unroll
+                for (int p = 0; p < 8; ++p)
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) {
+                        const float rv = d[p * 4 + t];
+                        const float r2 = __fmul_rn(rv, rv);
+                        float coeff = r2 / __fadd_rn(r2, s2);
+                        if (p == 0 && t == 0 && h == 0 && j == 0) coeff = 1.0f;
+                        cb[p * 72 + (2 * t + h) * 8 + j] = coeff;
+                    }
+                __syncwarp(gm);
+#pragma unroll 8
+                for (int p = 0; p < 8; ++p)
+#pragma unroll
+                    for (int r = 0; r < 8; ++r) {
+                        const float c = cb[p * 72 + r * 8 + j];
+                        k = __fmaf_rn(c, c, k);
+                    }
+                k += __shfl_xor_sync(gm, k, 1, 8);
+                k += __shfl_xor_sync(gm, k, 2, 8);
+                k += __shfl_xor_sync(gm, k, 4, 8);
+            }
+        } else {
             gather16(d, a.src + pl * a.plane_stride, a, grp, h, j);
             forward3_16<T2, T1>(d, gb, h, j, gm);
-            const float s2 = sigma * sigma;
-#pragma unroll
-            for (int p = 0; p < 8; ++p)
-#pragma unroll
-                for (int t = 0; t < 4; ++t) {
-                    const float rv = d[p * 4 + t];
-                    const float r2 = __fmul_rn(rv, rv);
-                    float coeff = r2 / __fadd_rn(r2, s2);
-                    if (p == 0 && t == 0 && h == 0 && j == 0) coeff = 1.0f;
-                    cb[p * 72 + (2 * t + h) * 8 + j] = coeff;
-                }
-            __syncwarp(gm);
-#pragma unroll 8
-            for (int p = 0; p < 8; ++p)
-#pragma unroll
-                for (int r = 0; r < 8; ++r) {
-                    const float c = cb[p * 72 + r * 8 + j];
-                    k = __fmaf_rn(c, c, k);
-                }
-            k += __shfl_xor_sync(gm, k, 1, 8);
-            k += __shfl_xor_sync(gm, k, 2, 8);
-            k += __shfl_xor_sync(gm, k, 4, 8);
         }
-        gather16(d, a.src + (FINAL ? a.clip_stride : 0) + pl * a.plane_stride, a, grp, h, j);
-        forward3_16<T2, T1>(d, gb, h, j, gm);
         // shrinkage in layout D, right before the vertical inverse: d[q * 8 + i] is
         // spectrum 2q + h, row i, column j
         move_cd(d, gb, h, j, gm);

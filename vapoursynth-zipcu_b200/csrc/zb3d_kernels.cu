@@ -16,7 +16,7 @@
 //    read as float4 (bank-conflict free, no shuffles in the inner loop except one
 //    to join the two halves).  The top-8 list lives in registers and follows the
 //    reference's insertion rule in scan order, so the lists are bit-identical.
-//  * Filtering: 8 lanes per group, the reference's transform order, FP32.
+//  * Filtering: 16 lanes per group (32 values each), the reference's transform order, FP32.
 //  * Aggregation: signed 64-bit fixed point (2^32 = 1.0) with integer atomics,
 //    which is exact and order independent; the weight sum is accumulated once
 //    per patch at its origin and expanded by an 8x8 box sum in the finish pass.

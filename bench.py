@@ -876,6 +876,11 @@ def main():
     props = torch.cuda.get_device_properties(local)
     peak_fp32 = props.multi_processor_count * 128 * 2 * sm_max * 1e6 / 1e12
     achieved = match_flops_total / (match_ms / 1e3) / 1e12 if match_ms > 0 else None
+    # DRAM bytes per matching launch: ncu measured 8.32 MB read and 0 written for the
+    # 1920x1080 Y launch, which is the plane read once (4 B per pixel); scaled by plane
+    # size to the average of the batch's Y, U and V launches
+    plane_px = [w * h for (w, h) in plane_dims()]
+    traffic = 8.32e6 * (sum(plane_px) / len(plane_px)) / plane_px[0]
 
     out = {"metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -889,7 +894,10 @@ def main():
                       "streams": pipe.ns},
            "gpu_launches": pipe.launches_per_frame() * args.steps * BATCH,
            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
-                        "frac": (achieved / peak_fp32) if achieved else None, "traffic": None,
+                        "frac": (achieved / peak_fp32) if achieved else None, "traffic": traffic,
+                        "traffic_how": "DRAM read + write bytes per launch from the ncu capture of the Y launch "
+                                       "(profiles/zb_match_tiled2_ssd_bs4_1080p_Y.md), scaled by plane size to the "
+                                       "average launch; algorithmically the plane is read once",
                         "kernel": "zb_match_tiled2<shared, bs4> (block matching, packed FP32x2)",
                         "per_launch_ms": match_ms / max(match_n, 1), "launches": match_n,
                         "how": "algorithmic FLOP (192 per candidate, all clipped windows) of one batch's "
@@ -952,12 +960,12 @@ def main():
             pipe.close()
             pipe = None
         # timed over the same K steps as the plain form (8 frames each)
-        out["pilot_form"] = run_pilot_form(torch, frames, rank, args.steps, 1,
+        out["pilot_form"] = run_pilot_form(torch, frames, rank, args.steps, 1, nstreams=args.streams,
                                            weights=args.pilot_weights, conv_ctas_per_sm=args.pilot_conv_ctas)
         if args.pilot_weights is None:
             # the 48-channel, 10-layer net of the learned-pilot configuration, on the same frames
             from zb3d import pilot as P
-            out["pilot_form_w48_l10"] = run_pilot_form(torch, frames, rank, args.steps, 1,
+            out["pilot_form_w48_l10"] = run_pilot_form(torch, frames, rank, args.steps, 1, nstreams=args.streams,
                                                        weights=P.WEIGHTS_W48_L10,
                                                        conv_ctas_per_sm=args.pilot_conv_ctas)
     if rank == 0 and not args.no_ref_cuda:

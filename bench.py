@@ -697,6 +697,68 @@ def run_gray640(torch, steps: int, warmup: int):
                                    "extractor_exp 3, single pass"}}
 
 
+def run_dct_tf32(torch, steps: int, warmup: int):
+    """Precision form of the patch transform (zb3d_dct2d_tf32): the 2D DCT of the group stack
+    of one 1920x1080 luma plane at block_step 4 (128,851 groups x 8 patches) on the tcgen05
+    tensor cores in TF32, with the hi/lo split and without it; the error of each against an
+    FP64 transform of a 4096-patch sample, relative to the sample's largest coefficient."""
+    from zb3d import _native as N
+    from zb3d import synth
+    lib = N.lib()
+    npat = 128851 * 8
+    plane = synth.noisy_plane(W, H, SIGMA, frame=0)
+    rng = np.random.default_rng(0)
+    ys = rng.integers(0, H - 8, npat)
+    xs = rng.integers(0, W - 8, npat)
+    pl = torch.from_numpy(np.ascontiguousarray(plane[:, :W])).cuda()
+    iy = torch.from_numpy(ys).cuda()[:, None, None] + torch.arange(8, device="cuda")[None, :, None]
+    ix = torch.from_numpy(xs).cuda()[:, None, None] + torch.arange(8, device="cuda")[None, None, :]
+    x = pl[iy, ix].reshape(npat, 64).contiguous()
+    y = torch.empty_like(x)
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = torch.cuda.Stream()
+    k = np.arange(8)[:, None]
+    T = 4.0 * np.where(k == 0, np.sqrt(1 / 8), np.sqrt(2 / 8)) * np.cos(np.pi * (2 * np.arange(8)[None, :] + 1) * k / 16)
+    K = np.kron(T, T)
+    out = {"metric": "2D DCT of 8x8 patches, tcgen05 TF32 (GB/s of patches in + out)", "unit": "GB/s",
+           "steps": steps, "warmup": warmup,
+           "config": {"workload": f"{npat} patches (the block_step 4 group stack of a 1920x1080 Y plane), "
+                                  "[n][64] FP32 in device memory, inputs larger than L2 (528 MB per call)"}}
+    for split in (1, 0):
+        def call():
+            rc = lib.zb3d_dct2d_tf32(x.data_ptr(), y.data_ptr(), npat, split, status.data_ptr(), st.cuda_stream)
+            if rc:
+                raise RuntimeError(f"zb3d_dct2d_tf32 returned {rc}")
+        for _ in range(warmup):
+            call()
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        for _ in range(steps):
+            call()
+        z.record(st)
+        z.synchronize()
+        ms = a.elapsed_time(z) / steps
+        if int(status.item()):
+            raise RuntimeError("zb3d_dct2d_tf32: a wait timed out")
+        xs_ = x[:4096].cpu().numpy().astype(np.float64)
+        ref = xs_ @ K.T
+        err = float(np.abs(y[:4096].cpu().numpy() - ref).max() / np.abs(ref).max())
+        key = "split" if split else "single_tf32"
+        out[key] = {"ms_per_call": ms, "GB_per_s": npat * 512 / ms / 1e6,
+                    "tensor_TFLOP_per_s": npat * 8192 * (3 if split else 1) / ms / 1e9,
+                    "rel_max_error_vs_fp64": err}
+    out["value"] = out["split"]["GB_per_s"]
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        src = "measured copy bandwidth (MEASURED_PEAKS.json)"
+    except Exception:
+        peak, src = 6650.0, "fallback copy bandwidth"
+    out["roofline"] = {"bound": "hbm", "achieved": out["value"], "peak": peak, "unit": "GB/s",
+                       "frac": out["value"] / peak, "traffic": None, "peak_source": src,
+                       "how": "algorithmic bytes (256 B read + 256 B written per patch) / CUDA-event time per call"}
+    return out
+
+
 def run_batched(torch, steps: int, warmup: int, nstreams: int = 4):
     """Uneven batch: 720x480, 1280x720 and 3840x2160 clips of 16 frames, YUV420 per plane or
     YUV444 CBM3D (chroma=1, matched on Y), radius 0 or 1 (stacked output), sigma drawn per
@@ -808,7 +870,7 @@ def main():
     ap.add_argument("--match-form", type=int, choices=[-1, 0, 1], default=-1,
                     help="block matching: -1 = the library's autotuned choice per plane, 0 = FP32 scan of every "
                          "candidate, 1 = tensor-core bound + exact re-rank")
-    ap.add_argument("--workload", choices=["twopass1080", "vbm3d", "gray640", "batched", "pilot4k"],
+    ap.add_argument("--workload", choices=["twopass1080", "vbm3d", "gray640", "batched", "pilot4k", "dct_tf32"],
                     default="twopass1080",
                     help="twopass1080 is the metric's workload; the others print their own line")
     args = ap.parse_args()
@@ -825,7 +887,8 @@ def main():
     import torch
     torch.cuda.set_device(local)
     if args.workload != "twopass1080":
-        fn = {"vbm3d": run_vbm3d, "gray640": run_gray640, "batched": run_batched, "pilot4k": run_pilot4k}[args.workload]
+        fn = {"vbm3d": run_vbm3d, "gray640": run_gray640, "batched": run_batched, "pilot4k": run_pilot4k,
+              "dct_tf32": run_dct_tf32}[args.workload]
         out = fn(torch, args.steps, args.warmup)
         for k, v in {"n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic"}.items():
             out.setdefault(k, v)

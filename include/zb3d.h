@@ -296,6 +296,15 @@ int zb3d_pilot_conv3x3_tc(const void *x, int n, int h, int w, int cin, const voi
  * fills each SM and is fastest alone; 1 leaves room for kernels of other streams.
  * Returns 0, or -1 for an unsupported value. */
 int zb3d_pilot_tc_ctas_per_sm(int ctas);
+/* Precision form of the patch transform (no counterpart in the reference, whose 2D
+ * transform is FP32 SIMT code, src/bm3d.cu:32-110 and :392-413): the 2D DCT of npatches
+ * row-major 8x8 FP32 patches (d_x, d_y: [npatches][64] in device memory, d_y 16-byte
+ * aligned) on the tcgen05 tensor cores in TF32 with FP32 accumulation.  split = 1 adds
+ * the hi/lo products that win the accuracy back (Xl.Kh + Xh.Kl + Xh.Kh), split = 0 is
+ * one TF32 product.  The first call on a device copies the transform matrix to it
+ * (synchronous).  *d_status (device) becomes non-zero if a wait for the products timed
+ * out.  Returns 0, 1 for bad arguments, 2 for a CUDA error. */
+int zb3d_dct2d_tf32(const float *d_x, float *d_y, long long npatches, int split, int *d_status, void *stream);
 /* The network input of zb3d_pilot_pack_input in the channel-blocked layout ([n][2][h][w][8]);
  * the noisy images are noisy_stride floats apart (0: h * w). */
 int zb3d_pilot_pack_input_blocked(const float *noisy, long long noisy_stride, const float *sigma, int n, int h,

@@ -173,3 +173,13 @@ def test_pilot_abi_argument_checks_need_no_gpu():
     # empty batches are a no-op
     assert lib.zb3d_pilot_pack_input_blocked(fake, 0, fake, 0, h, w, 4.0, fake, None) == 0
     assert lib.zb3d_pilot_conv3x3_tc(fake, 0, h, w, 32, fake, None, 32, 1, fake, None, None, 0, 0, None, None) == 0
+
+
+def test_dct2d_tf32_argument_checks_need_no_gpu():
+    """The precision-form transform rejects bad arguments before any CUDA call."""
+    from zb3d import _native as N
+    lib = N.lib()
+    assert lib.zb3d_dct2d_tf32(None, None, 0, 1, None, None) == 0    # nothing to do
+    assert lib.zb3d_dct2d_tf32(None, None, 5, 1, None, None) == 1    # missing buffers
+    assert lib.zb3d_dct2d_tf32(None, None, -1, 1, None, None) == 1   # negative count
+    assert lib.zb3d_dct2d_tf32(16, 20, 5, 1, 32, None) == 1          # output not 16-byte aligned

@@ -98,6 +98,7 @@ EXPORTS = {
                                       c_void_p, c_void_p, c_void_p, ctypes.c_longlong, ctypes.c_longlong, c_void_p,
                                       c_void_p]),
     "zb3d_pilot_tc_ctas_per_sm": (c_int, [c_int]),
+    "zb3d_dct2d_tf32": (c_int, [c_void_p, c_void_p, ctypes.c_longlong, c_int, c_void_p, c_void_p]),
     "zb3d_pilot_pack_input_blocked": (c_int, [c_void_p, ctypes.c_longlong, c_void_p, c_int, c_int, c_int, c_float,
                                               c_void_p, c_void_p]),
     "zb3d_pilot_conv3x3_wgrad": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p,

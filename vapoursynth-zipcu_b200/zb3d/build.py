@@ -28,6 +28,7 @@ UNITS = [
     ("zb3d_vagg.cu", ARCH),
     ("zb3d_pilot.cu", ARCH),
     ("zb3d_pilot_tc.cu", ARCH),
+    ("zb3d_dct_tc.cu", ARCH),
     ("zb3d_host.cpp", ARCH),
     ("zb3d_noalloc.cu", ARCH),
 ]

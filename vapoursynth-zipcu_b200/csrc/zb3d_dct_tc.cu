@@ -100,14 +100,16 @@ __global__ void __launch_bounds__(128) dct2d_tf32(const float *__restrict__ x, f
     uint32_t phase = 0;
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const long long p0 = t * TILE;
-        // the tile's patches, split into TF32 high parts and FP32 remainders
-        for (int i = tid; i < TILE * 64; i += 128) {
-            const int row = i >> 6, k = i & 63;
+        // the tile's patches, split into TF32 high parts and FP32 remainders, written in
+        // shared-memory order: a warp fills 128 contiguous bytes (8 patches x one 4-pixel
+        // chunk) per store, conflict-free, and reads 8 runs of 16 bytes from global memory
+        for (int s = tid; s < TILE * 64; s += 128) {
+            const int kk = s & 3, row = (s >> 2) & (TILE - 1), kc = s >> 9;  // s = kmaj(row, 4 kc + kk) / 4
             const long long p = p0 + row;
-            const float v = p < n ? __ldg(x + p * 64 + k) : 0.0f;
+            const float v = p < n ? __ldg(x + p * 64 + kc * 4 + kk) : 0.0f;
             const float hi = tf32_high(v);
-            *reinterpret_cast<float *>(a_hi + kmaj(row, k, TILE)) = hi;
-            *reinterpret_cast<float *>(a_lo + kmaj(row, k, TILE)) = v - hi;
+            reinterpret_cast<float *>(a_hi)[s] = hi;
+            reinterpret_cast<float *>(a_lo)[s] = v - hi;
         }
         fence_async_smem();
         fence_before_sync();

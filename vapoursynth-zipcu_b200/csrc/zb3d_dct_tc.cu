@@ -29,6 +29,7 @@ constexpr int A_BYTES = TILE * 64 * 4;           // one A operand copy: 32 KB
 constexpr int B_BYTES = 64 * 64 * 4;             // one B operand copy: 16 KB
 constexpr int SMEM = 2 * A_BYTES + 2 * B_BYTES + 64;
 constexpr unsigned WAIT_LIMIT = 1u << 22;
+constexpr int THREADS = 256;                     // 8 warps: all stage, two per tensor-memory lane quarter drain
 // kind::tf32: FP32 accumulator (bit 4), TF32 A (bits 7-9 = 2) and B (bits 10-12 = 2),
 // both K-major, N = 64 (bits 17-22 = N >> 3), M = 128 (bits 24-28 = M >> 4)
 constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((uint32_t)(TILE >> 4) << 24);
@@ -71,8 +72,8 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64
         : "memory");
 }
 
-// 128 threads; each CTA stages the matrix once and walks tiles of 128 patches
-__global__ void __launch_bounds__(128) dct2d_tf32(const float *__restrict__ x, float *__restrict__ y, long long n,
+// each CTA stages the matrix once and walks tiles of 128 patches
+__global__ void __launch_bounds__(THREADS) dct2d_tf32(const float *__restrict__ x, float *__restrict__ y, long long n,
                                                   int split, int *status) {
     extern __shared__ __align__(1024) uint8_t sm[];
     uint8_t *a_hi = sm, *a_lo = sm + A_BYTES, *b_hi = sm + 2 * A_BYTES, *b_lo = b_hi + B_BYTES;
@@ -80,7 +81,7 @@ __global__ void __launch_bounds__(128) dct2d_tf32(const float *__restrict__ x, f
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    for (int i = tid; i < 64 * 64; i += 128) {
+    for (int i = tid; i < 64 * 64; i += THREADS) {
         const int row = i >> 6, k = i & 63;
         *reinterpret_cast<float *>(b_hi + kmaj(row, k, 64)) = g_kron[0][i];
         *reinterpret_cast<float *>(b_lo + kmaj(row, k, 64)) = g_kron[1][i];
@@ -103,7 +104,7 @@ __global__ void __launch_bounds__(128) dct2d_tf32(const float *__restrict__ x, f
         // the tile's patches, split into TF32 high parts and FP32 remainders, written in
         // shared-memory order: a warp fills 128 contiguous bytes (8 patches x one 4-pixel
         // chunk) per store, conflict-free, and reads 8 runs of 16 bytes from global memory
-        for (int s = tid; s < TILE * 64; s += 128) {
+        for (int s = tid; s < TILE * 64; s += THREADS) {
             const int kk = s & 3, row = (s >> 2) & (TILE - 1), kc = s >> 9;  // s = kmaj(row, 4 kc + kk) / 4
             const long long p = p0 + row;
             const float v = p < n ? __ldg(x + p * 64 + kc * 4 + kk) : 0.0f;
@@ -141,12 +142,13 @@ __global__ void __launch_bounds__(128) dct2d_tf32(const float *__restrict__ x, f
             break;
         }
         fence_after_sync();
-        // warp w reads tensor-memory lanes 32w .. 32w + 31: one patch per thread
-        const long long p = p0 + warp * 32 + lane;
-#pragma unroll
-        for (int half = 0; half < 2; ++half) {
+        // warp w reads tensor-memory lanes 32 (w % 4) .. + 31 (one patch per thread), columns
+        // 32 (w / 4) .. + 31 (half of its coefficients)
+        {
+            const int quarter = warp & 3, half = warp >> 2;
+            const long long p = p0 + quarter * 32 + lane;
             float v[32];
-            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(half * 32), v);
+            tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * 32), v);
             if (p < n) {
                 float4 *dst = reinterpret_cast<float4 *>(y + p * 64 + half * 32);
 #pragma unroll
@@ -206,6 +208,6 @@ extern "C" int zb3d_dct2d_tf32(const float *d_x, float *d_y, long long npatches,
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long ntiles = (npatches + TILE - 1) / TILE;
     const int grid = (int)(ntiles < 2LL * sms ? ntiles : 2LL * sms);
-    dct2d_tf32<<<grid, 128, SMEM, (cudaStream_t)stream>>>(d_x, d_y, npatches, split, d_status);
+    dct2d_tf32<<<grid, THREADS, SMEM, (cudaStream_t)stream>>>(d_x, d_y, npatches, split, d_status);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }

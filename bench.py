@@ -958,9 +958,9 @@ def main():
            "gpu_launches": pipe.launches_per_frame() * args.steps * BATCH,
            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                         "frac": (achieved / peak_fp32) if achieved else None, "traffic": traffic,
-                        "traffic_how": "DRAM read + write bytes per launch from the ncu capture of the Y launch "
-                                       "(profiles/zb_match_tiled2_ssd_bs4_1080p_Y.md), scaled by plane size to the "
-                                       "average launch; algorithmically the plane is read once",
+                        "traffic_how": "DRAM read + write bytes per launch from an ncu capture of the 1920x1080 Y "
+                                       "launch (8.32 MB read, 0 written), scaled by plane size to the average "
+                                       "launch; algorithmically the plane is read once",
                         "kernel": "zb_match_tiled2<shared, bs4> (block matching, packed FP32x2)",
                         "per_launch_ms": match_ms / max(match_n, 1), "launches": match_n,
                         "how": "algorithmic FLOP (192 per candidate, all clipped windows) of one batch's "

@@ -6,7 +6,7 @@ C ABI's get_frame) against the reference's own kernels on the same GPU.
 * BM3D with radius > 0 emits the reference's stacked accumulators for the
   clamped window of every frame (src/bm3d.zig:684-699), bitwise;
 * BM3Dv2 radius > 0 equals the reference's vaggregate over those stacks, and
-  the fused and composed forms are byte-identical (README.md:77-79);
+  the fused and composed forms are byte-identical (vszipcu README.md:77-79);
 * CBM3D (YUV444, chroma=1); concurrent get_frame calls; frame-range errors.
 """
 from concurrent.futures import ThreadPoolExecutor

@@ -378,7 +378,9 @@ def run_e2e(frames, steps: int, warmup: int, num_streams: int = 4):
 # ---------------------------------------------------------------------------
 # the reference's own kernels on the same GPU (drop-in comparison)
 # ---------------------------------------------------------------------------
-def run_ref_cuda(torch, frames, steps: int, warmup: int):
+def run_ref_cuda(torch, frames, steps: int, warmup: int, nstreams: int = 4):
+    """The reference's kernels, each frame's launch sequence on one of `nstreams` streams
+    in turn (the reference host's default is 4 stream slots, vszipcu src/bm3d.zig:1077-1081)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     try:
         import ref_configs as rc
@@ -393,7 +395,7 @@ def run_ref_cuda(torch, frames, steps: int, warmup: int):
             if not (refh.available() and refh.has_cubin(s)):
                 return None
             specs[(final, w)] = s
-    ns = 2
+    ns = nstreams
     kernels = [{k: refh.RefKernel(s) for k, s in specs.items()} for _ in range(ns)]
     streams = [torch.cuda.Stream() for _ in range(ns)]
     dims = plane_dims()
@@ -422,13 +424,15 @@ def run_ref_cuda(torch, frames, steps: int, warmup: int):
         s0 = streams[0]
         a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(s0)
-        streams[1].wait_event(a)
+        for st in streams[1:]:
+            st.wait_event(a)
         for s in range(nsteps):
             for j in range(BATCH):
                 frame(j, (first + s * BATCH + j) % FRAMES_PER_GPU)
-        ev = torch.cuda.Event()
-        ev.record(streams[1])
-        s0.wait_event(ev)
+        for st in streams[1:]:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            s0.wait_event(ev)
         z.record(s0)
         z.synchronize()
         return a.elapsed_time(z)
@@ -1032,13 +1036,33 @@ def main():
                                                        weights=P.WEIGHTS_W48_L10,
                                                        conv_ctas_per_sm=args.pilot_conv_ctas)
     if rank == 0 and not args.no_ref_cuda:
-        rms = run_ref_cuda(torch, frames, args.steps, args.warmup)
-        if rms:
-            rv = W * H * args.steps * BATCH / (rms / 1e3) / 1e6
-            out["ref_cuda"] = {"value": rv, "unit": "Mpix/s", "ms_per_step": rms / args.steps,
+        if pipe is not None:
+            pipe.close()
+            pipe = None
+        by_ns = {}
+        for ns in (4, 2):
+            rms = run_ref_cuda(torch, frames, args.steps, args.warmup, nstreams=ns)
+            if rms:
+                by_ns[ns] = (W * H * args.steps * BATCH / (rms / 1e3) / 1e6, rms / args.steps)
+        if by_ns:
+            rv = by_ns[max(by_ns)][0]
+            out["ref_cuda"] = {"value": rv, "unit": "Mpix/s", "ms_per_step": by_ns[max(by_ns)][1],
+                               "streams": max(by_ns),
+                               "value_by_streams": {str(k): v[0] for k, v in sorted(by_ns.items())},
                                "what": "the reference's own bm3d.cu kernels (NVRTC-built, -use_fast_math) on "
-                                       "this GPU, same frames, same two-pass chaining, device-resident",
+                                       "this GPU, same frames, same two-pass chaining, device-resident; frames "
+                                       "spread over the reference host's default 4 stream slots (2 shown too)",
                                "speedup_ours": value / world / rv}
+            # the drop-in comparison in one place: this build's forms over the reference's kernels
+            # (4 streams, device-resident on both sides; e2e runs through the public API)
+            vs = {"ref_cuda_mpix_s": rv, "ref_cuda_streams": max(by_ns), "plain_x": value / world / rv}
+            if "pilot_form" in out and out["pilot_form"].get("value"):
+                vs["pilot_x"] = out["pilot_form"]["value"] / rv
+            if "e2e" in out:
+                vs["e2e_pinned_x"] = out["e2e"]["value"] / world / rv
+                if out["e2e"].get("pageable"):
+                    vs["e2e_pageable_x"] = out["e2e"]["pageable"]["value"] / world / rv
+            out["vs_reference_cuda"] = vs
     if pipe is not None:
         pipe.close()
     if rank == 0 and not args.no_cpu:

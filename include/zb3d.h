@@ -230,9 +230,13 @@ int zb3d_vaggregate_device(const float *const *stacks, const int *z, int tw, int
  *           basic estimate (matched on, Wiener reference) followed by the noisy plane
  *   d_dst   [height][pitch] denoised output
  *   sigma   8-bit-scale sigma as in zb3d_args (scaled internally like BM3D)
+ * A sigma below FLT_EPSILON leaves the plane unprocessed, as BM3D does: the noisy
+ * plane is copied to d_dst.
  * Limits: height*pitch <= 1048576 and at most 131072 reference blocks; larger
  * planes are rejected with an error.  The first call on a device looks up the
- * array's device address (make that first call before any stream capture).
+ * array's device address (make that first call before any stream capture); the
+ * address is kept for the life of the process, so a device that was reset
+ * (cudaDeviceReset) must not be given to this entry point again.
  * Every call reuses the same array, so calls that overlap on the GPU race.
  * Returns 0, or -1 with the reason in err.
  */
@@ -302,8 +306,10 @@ int zb3d_pilot_tc_ctas_per_sm(int ctas);
  * aligned) on the tcgen05 tensor cores in TF32 with FP32 accumulation.  split = 1 adds
  * the hi/lo products that win the accuracy back (Xl.Kh + Xh.Kl + Xh.Kh), split = 0 is
  * one TF32 product.  The first call on a device copies the transform matrix to it
- * (synchronous).  *d_status (device) becomes non-zero if a wait for the products timed
- * out.  Returns 0, 1 for bad arguments, 2 for a CUDA error. */
+ * (synchronous).  *d_status (device) becomes 1 if a wait for the products timed out and
+ * they then landed, 2 if they had not landed even after a second wait: the device is then
+ * unhealthy (tensor memory was released under a running MMA) and the call must not be
+ * retried.  Returns 0, 1 for bad arguments, 2 for a CUDA error. */
 int zb3d_dct2d_tf32(const float *d_x, float *d_y, long long npatches, int split, int *d_status, void *stream);
 /* The network input of zb3d_pilot_pack_input in the channel-blocked layout ([n][2][h][w][8]);
  * the noisy images are noisy_stride floats apart (0: h * w). */
@@ -315,9 +321,10 @@ int zb3d_pilot_conv3x3_wgrad(const void *x, const void *dy, int n, int h, int w,
 /* network input: channel 0 = noisy, 1 = sigma[image] / 255 * level_scale, others 0 (16 channels). */
 int zb3d_pilot_pack_input(const float *noisy, const float *sigma, int n, int h, int w, float level_scale, void *x0,
                           void *stream);
-/* dy (16 channels) = scale * dMSE/dy in channel 0; *loss += sum of squared errors. */
-int zb3d_pilot_mse_grad(const float *y, const float *t, long long count, float scale, void *dy, double *loss,
-                        void *stream);
+/* dy (16 channels) = scale * dMSE/dy in channel 0; loss_partials[k] (may be NULL; ceil(count / 256)
+ * floats) = the FP32 sum of squared errors of elements [256 k, 256 k + 256), for the host to add up. */
+int zb3d_pilot_mse_grad(const float *y, const float *t, long long count, float scale, void *dy,
+                        float *loss_partials, void *stream);
 /* Adam step (step >= 1) on FP32 weights w with loss-scaled gradient g / gscale; keep (may be NULL)
  * pins entries to 0 where keep == 0; w16 (may be NULL) receives the BF16 copy. */
 int zb3d_pilot_adam(float *w, float *m, float *v, const float *g, long long count, float lr, float b1, float b2,

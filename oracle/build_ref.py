@@ -27,7 +27,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 import ref_configs as rc  # noqa: E402
 
-REF_ROOT = os.environ.get("ZB3D_REFERENCE_ROOT", "/root/reference")
+# the reference source tree (its src/bm3d.cu); there is no default location
+REF_ROOT = os.environ.get("ZB3D_REFERENCE_ROOT", "")
 OUT = os.path.join(HERE, "_ref")
 GEN = os.path.join(OUT, "gen")
 
@@ -96,6 +97,9 @@ VAGG_OPTS = ["-arch=sm_100", "-std=c++17", "-modify-stack-limit=false"]
 
 
 def build(force: bool = False, jobs: int = 8, verbose: bool = True) -> int:
+    if not REF_ROOT:
+        raise RuntimeError("build_ref: set ZB3D_REFERENCE_ROOT to the reference source tree (the directory "
+                           "holding src/bm3d.cu)")
     if not os.path.isfile(os.path.join(REF_ROOT, "src", "bm3d.cu")):
         if verbose:
             print(f"build_ref: reference sources not found under {REF_ROOT}; skipped")

@@ -132,11 +132,14 @@ __global__ void __launch_bounds__(THREADS) dct2d_tf32(const float *__restrict__ 
         for (unsigned i = 0; i < WAIT_LIMIT && !done; ++i) done = mbar_try(smem_u32(bar), phase);
         phase ^= 1u;
         if (!__syncthreads_and(done)) {
-            // the products did not complete in time: record it, let them land, stop
+            // the products did not complete in time: record it (1), let them land, stop.  If
+            // they still have not landed, the status is 2: tensor memory is freed while an MMA
+            // may still write it, so the caller must treat the device as unhealthy and not retry.
             if (tid == 0) {
                 atomicExch(status, 1);
-                for (unsigned i = 0; i < WAIT_LIMIT && !mbar_try(smem_u32(bar), phase ^ 1u); ++i) {
-                }
+                bool landed = false;
+                for (unsigned i = 0; i < WAIT_LIMIT && !landed; ++i) landed = mbar_try(smem_u32(bar), phase ^ 1u);
+                if (!landed) atomicExch(status, 2);
             }
             __syncthreads();
             break;
@@ -163,30 +166,33 @@ __global__ void __launch_bounds__(THREADS) dct2d_tf32(const float *__restrict__ 
     if (warp == 0) tmem_dealloc(tmem, 64);
 }
 
+std::once_flag g_host_once;
+float g_host_kron[2][64 * 64];
 std::once_flag g_dev_once[64];
 cudaError_t g_dev_err[64];
 
-// (T (x) T) from the closed form of T in double on the host, split into float parts,
-// copied once per device
+// (T (x) T) from the closed form of T in double on the host, split into float parts:
+// built once per process, then copied once per device
 cudaError_t init_matrix(int dev) {
-    std::call_once(g_dev_once[dev], [dev] {
+    std::call_once(g_host_once, [] {
         const double pi = 3.14159265358979323846264338327950288;
         double T[8][8];
         for (int k = 0; k < 8; ++k)
             for (int m = 0; m < 8; ++m)
                 T[k][m] = 4.0 * (k == 0 ? std::sqrt(1.0 / 8.0) : std::sqrt(2.0 / 8.0)) *
                           std::cos(pi * (2 * m + 1) * k / 16.0);
-        static float h[2][64 * 64];
         for (int r = 0; r < 8; ++r)
             for (int c = 0; c < 8; ++c)
                 for (int i = 0; i < 8; ++i)
                     for (int j = 0; j < 8; ++j) {
                         const float v = (float)(T[r][i] * T[c][j]);
                         const float hi = tf32_high(v);
-                        h[0][(r * 8 + c) * 64 + i * 8 + j] = hi;
-                        h[1][(r * 8 + c) * 64 + i * 8 + j] = v - hi;
+                        g_host_kron[0][(r * 8 + c) * 64 + i * 8 + j] = hi;
+                        g_host_kron[1][(r * 8 + c) * 64 + i * 8 + j] = v - hi;
                     }
-        g_dev_err[dev] = cudaMemcpyToSymbol(g_kron, h, sizeof(h));
+    });
+    std::call_once(g_dev_once[dev], [dev] {
+        g_dev_err[dev] = cudaMemcpyToSymbol(g_kron, g_host_kron, sizeof(g_host_kron));
         if (g_dev_err[dev] == cudaSuccess) g_dev_err[dev] = cudaFuncSetAttribute(dct2d_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
     });
     return g_dev_err[dev];

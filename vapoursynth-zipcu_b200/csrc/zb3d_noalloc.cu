@@ -26,6 +26,7 @@
 #define ZB_NOALLOC_ACC_PIXELS (size_t(1) << 20)
 #define ZB_NOALLOC_LIST_BLOCKS (size_t(1) << 17)
 #define ZB_NOALLOC_BYTES (2 * ZB_NOALLOC_ACC_PIXELS * 8 + ZB_NOALLOC_LIST_BLOCKS * 64)
+#define ZB_NOALLOC_FLT_EPSILON 1.19209290e-7f
 
 static __device__ __align__(256) unsigned char zb_noalloc_scratch[ZB_NOALLOC_BYTES];
 
@@ -57,7 +58,9 @@ void set_err(char *err, size_t n, const char *msg) {
 
 // Device address of the scratch array on the current device.  The name of a
 // __device__ array is only a host-side handle; the address comes from the
-// runtime, looked up once per device with that device current.
+// runtime, looked up once per device with that device current, and kept for the
+// life of the process: a caller that resets a device (cudaDeviceReset) must not
+// call this entry point on that device again.
 unsigned char *scratch_for_current_device(char *err, size_t errlen) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
@@ -104,12 +107,26 @@ extern "C" int zb3d_bm3d_plane_noalloc(const float *d_src, float *d_dst, int wid
                      pixels, nblocks, kAccPixels, kListBlocks);
         return -1;
     }
+    cudaStream_t st = (cudaStream_t)stream;
+    // sigma below FLT_EPSILON: the plane is not processed and the output is the noisy
+    // plane itself, as the reference's output frame keeps unprocessed planes of the
+    // noisy clip (vszipcu src/bm3d.zig:1017, :702-703)
+    if (sigma < ZB_NOALLOC_FLT_EPSILON) {
+        const float *noisy = d_src + (final_ ? pixels : 0);
+        const cudaError_t ce = cudaMemcpy2DAsync(d_dst, (size_t)pitch * 4, noisy, (size_t)pitch * 4,
+                                                 (size_t)width * 4, (size_t)height, cudaMemcpyDeviceToDevice, st);
+        if (ce != cudaSuccess) {
+            if (err && errlen)
+                snprintf(err, errlen, "zb3d_bm3d_plane_noalloc: copy failed (%s).", cudaGetErrorString(ce));
+            return -1;
+        }
+        return 0;
+    }
     unsigned char *base = scratch_for_current_device(err, errlen);
     if (!base) return -1;
     unsigned long long *num = reinterpret_cast<unsigned long long *>(base);
     unsigned long long *den = reinterpret_cast<unsigned long long *>(base + kAccBytes);
     int2 *list = reinterpret_cast<int2 *>(base + 2 * kAccBytes);
-    cudaStream_t st = (cudaStream_t)stream;
 
     // the array keeps the previous call's sums: both accumulators start from zero
     cudaError_t e = cudaMemsetAsync(num, 0, pixels * sizeof(unsigned long long), st);

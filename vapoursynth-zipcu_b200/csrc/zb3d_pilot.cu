@@ -272,9 +272,10 @@ __global__ void pack_input(const float *noisy, const float *sigma, int n, int h,
     for (int k = 1; k < 8; ++k) o[k] = 0;
 }
 
-// dy[p][16] = scale * 2 (y - t) / count in channel 0; loss += sum (y - t)^2.
-__global__ void mse_grad(const float *y, const float *t, long long count, float scale, __nv_bfloat16 *dy,
-                         double *loss) {
+// dy[p][16] = scale * 2 (y - t) / count in channel 0; partial[blockIdx.x] = the CTA's
+// sum of (y - t)^2 in FP32 (the caller adds the partials up on the host).
+__global__ void __launch_bounds__(256) mse_grad(const float *y, const float *t, long long count, float scale,
+                                               __nv_bfloat16 *dy, float *partial) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     float e2 = 0.0f;
     if (i < count) {
@@ -287,7 +288,11 @@ __global__ void mse_grad(const float *y, const float *t, long long count, float 
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) e2 += __shfl_xor_sync(0xffffffffu, e2, o);
-    if ((threadIdx.x & 31) == 0 && loss) atomicAdd(loss, (double)e2);
+    __shared__ float ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = e2;
+    __syncthreads();
+    if (threadIdx.x == 0 && partial)
+        partial[blockIdx.x] = ((ws[0] + ws[1]) + (ws[2] + ws[3])) + ((ws[4] + ws[5]) + (ws[6] + ws[7]));
 }
 
 // Adam on FP32 master weights; g is the loss-scaled gradient (divided by gscale here);
@@ -416,10 +421,10 @@ int zb3d_pilot_pack_input(const float *noisy, const float *sigma, int n, int h, 
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
-int zb3d_pilot_mse_grad(const float *y, const float *t, long long count, float scale, void *dy, double *loss,
-                        void *stream) {
+int zb3d_pilot_mse_grad(const float *y, const float *t, long long count, float scale, void *dy,
+                        float *loss_partials, void *stream) {
     zb::pilot::mse_grad<<<(unsigned)((count + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
-        y, t, count, scale, static_cast<__nv_bfloat16 *>(dy), loss);
+        y, t, count, scale, static_cast<__nv_bfloat16 *>(dy), loss_partials);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -200,9 +200,11 @@ class PilotNet:
         torch, lib = self.torch, N.lib()
         n, h, w = noisy.shape
         y, acts = self.forward(noisy, sigma, keep_acts=True)
-        loss = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        # per-CTA FP32 sums of squared errors, added up on the host (no FP64 on the GPU)
+        partials = torch.empty((y.numel() + 255) // 256, dtype=torch.float32, device=self.dev)
         d = torch.empty((n, h, w, 16), dtype=torch.bfloat16, device=self.dev)
-        _ok(lib.zb3d_pilot_mse_grad(_p(y), _p(target), y.numel(), LOSS_SCALE, _p(d), _p(loss), None), "mse_grad")
+        _ok(lib.zb3d_pilot_mse_grad(_p(y), _p(target), y.numel(), LOSS_SCALE, _p(d), _p(partials), None),
+            "mse_grad")
         dws = [torch.zeros_like(wt) for wt in self.w32]
         dbs = [torch.zeros_like(b) for b in self.b32]
         for l in range(len(self.shapes) - 1, -1, -1):
@@ -217,7 +219,8 @@ class PilotNet:
             _ok(lib.zb3d_pilot_conv3x3(_p(d), n, h, w, cout, _p(self.wt16[l]), None, cin, 0, _p(acts[l]), _p(dx),
                                        None, None, None), f"dgrad {l}")
             d = dx
-        return dws, dbs, float(loss.item()) / y.numel(), y
+        loss = float(partials.cpu().numpy().astype(np.float64).sum())
+        return dws, dbs, loss / y.numel(), y
 
     def train_step(self, noisy, target, sigma, lr: float = 1e-3) -> float:
         lib = N.lib()

@@ -163,7 +163,10 @@ __global__ void __launch_bounds__(THREADS) dct2d_tf32(const float *__restrict__ 
         fence_after_sync();
     }
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, 64);
+    if (warp == 0) {
+        __syncwarp();  // lane 0 issued the MMAs alone; tcgen05.dealloc is .sync.aligned
+        tmem_dealloc(tmem, 64);
+    }
 }
 
 std::once_flag g_host_once;

@@ -2,31 +2,40 @@
 //
 // The plain matcher evaluates every candidate's SSD in the reference's FP32
 // operation order (vszipcu src/bm3d.cu:282-302, 614-660).  This form gets the
-// same lists with far less FP32 work:
+// same lists with the distances bounded on the tensor cores:
 //
-//  1. Per tile of 8 x 16 reference blocks (M = 128 rows), the candidate
-//     positions of the union of their search windows are streamed through
-//     tcgen05.mma (kind::f16, FP32 accumulation in tensor memory) in chunks of
-//     N = 256 candidates.  Row m of the product is, for block m and candidate c,
-//         d(m, c) = |b_c - c0|^2 - 2 (mu_m - c0) S_c - 2 (a_m - mu_m) . (b_c - c0)
-//     (c0 a tile constant, mu_m the block mean, S_c the candidate sum), which
-//     equals SSD(a_m, b_c) - |a_m - c0|^2.  The pixel cross term runs on FP16
-//     operands; the norm terms enter as FP16 hi/lo pairs; candidates outside
-//     block m's window get +16384 through one-hot window terms.  K = 96.
-//  2. Pass 1 keeps, per block, the minimum of d over 16 groups of candidates.
-//     The eighth smallest group minimum U comes from eight distinct window
-//     candidates, so the reference's eighth-best FP32 error is at most
-//     U + |a - c0|^2 + eps, where eps bounds |d - (SSD_ref - |a - c0|^2)|.
-//  3. Pass 2 recomputes the chunks and collects every candidate with
-//     d <= U + 2 eps: a superset of the exact top 8 (ties included).
-//  4. The collected candidates (in scan order) get the exact FP32 SSD in the
-//     reference's order and go through the reference's insertion rule and self
-//     inclusion, so the list is bit-identical to the plain matcher's.
+//  1. A tile is 8 x 16 reference blocks (M = 128 rows of the MMA, TMEM lane m =
+//     block m).  The candidate positions of the union of their search windows,
+//     nur rows x nuc columns, are numbered row-major: flat f = r * nuc + c.  They
+//     stream through tcgen05.mma (kind::f16, FP32 accumulation in tensor memory)
+//     in chunks of N = 256 consecutive f.  Row m of the product is, for block m
+//     and candidate f,
+//         d(m, f) = |b_f - c0|^2 - 2 (mu_m - c0) S_f - 2 (a_m - mu_m) . (b_f - c0)
+//     (c0 a tile constant, mu_m the block mean, S_f the candidate sum), which
+//     equals SSD(a_m, b_f) - |a_m - c0|^2.  The pixel cross term runs on FP16
+//     operands, the norm terms enter as FP16 hi/lo pairs in a fifth K step.
+//  2. Operand B needs no per-chunk build: the tile's region is expanded once into
+//     E[y][x] = the 8 FP16 pixels (y, x .. x + 7) - c0, 16 bytes per position, at
+//     a row pitch of nuc positions.  Patch row i of candidate f is then E entry
+//     f + i * nuc, so one shared-memory descriptor (8-row core matrices 128 bytes
+//     apart, K chunks one E row apart) walks 256 consecutive candidates and the
+//     8 patch rows.  The norm terms sit in a per-candidate table read the same way.
+//  3. Pass 1 keeps, per block, the minimum of d over 16 groups of its window
+//     candidates (flat index mod 16).  The eighth smallest group minimum U comes
+//     from eight distinct window candidates, so the reference's eighth-best FP32
+//     error is at most U + |a - c0|^2 + eps, where eps bounds
+//     |d - (SSD_ref - |a - c0|^2)|.  Pass 2 recomputes the chunks and collects
+//     every window candidate with d <= U + 2 eps: a superset of the exact top 8,
+//     ties included.
+//  4. The collected candidates get the exact FP32 SSD in the reference's order
+//     and the eight smallest by (error, scan position) are kept, which is the list
+//     the reference's strict-less insertion builds in scan order; then self
+//     inclusion.  The list is bit-identical to the plain matcher's.
 //
-// A block whose collection overflows, or a tile whose pixels leave the range
-// the FP16 terms are sized for (|x| <= 4), is listed for the exact matcher
-// (zb_match_global, gen_mode 2), so the result never depends on the bound
-// being tight.
+// A block whose collection overflows, or a tile whose pixels leave the range the
+// FP16 terms are sized for (|x| <= 4), is listed for the exact matcher
+// (zb_match_global, gen_mode 2), so the result never depends on the bound being
+// tight.
 //
 // Compiled with -use_fast_math like the other matching kernels: the exact
 // re-rank uses explicit __fmul_rn / __fmaf_rn, so its arithmetic is fixed.
@@ -46,80 +55,57 @@ namespace tc {
 using namespace tc05;
 
 constexpr int BX = 8, BY = 16, M = BX * BY;  // reference blocks per tile
-constexpr int N = 128;                       // candidates per MMA chunk
-constexpr int NSLOT = 4;                     // chunks in flight: slabs, TMEM accumulators (NSLOT * N = 512 columns)
-constexpr int K = 96;                        // 64 pixels + 5 norm terms + 8 + 16 window one-hots + 3 zero
-constexpr int KSTEPS = K / 16;
+constexpr int N = 256;                       // candidates per MMA chunk = TMEM columns of one slot
+constexpr int KSTEPS = 5;                    // patch rows (0,1) (2,3) (4,5) (6,7), then the norm terms
 constexpr int MAX_UC = 56, MAX_UR = 88;      // candidate union of a tile: columns, rows
 constexpr int REG_ROWS = MAX_UR + 7;
-constexpr int REG_COLS = 64;                 // staged region columns (union + 7, padded)
-constexpr int R16_PITCH = 33;                // 32-bit words per FP16 region row (+1 against bank conflicts)
+constexpr int REG_COLS = 64;                 // staged FP32 region: columns (union + 7, padded)
+constexpr int E_ENTRIES = REG_ROWS * MAX_UC + N;   // + the tail the last chunk reads
+constexpr int T_ENTRIES = MAX_UR * MAX_UC + N + 16;
 constexpr int CAP = 48;                      // collected candidates per block and job parity
-constexpr int THREADS = 416;                 // warps 0-7: blocks (two per block: even / odd jobs), 8-11: operand
-                                             // builders, 12: MMA issuer
+constexpr int THREADS = 384;                 // warps 0-7: blocks (two per lane quarter: even / odd
+                                             // jobs), warp 8: TMEM owner and MMA issuer, 9-11: setup
 constexpr int NWARPS = THREADS / 32;
-constexpr float BIG = 16384.0f;              // window penalty (exact in FP16)
 constexpr float RANGE = 4.0f;                // pixel magnitude the FP16 terms are sized for
 constexpr unsigned WAIT_LIMIT = 1u << 22;    // polls of an mbarrier before giving up (~0.5 s)
 
-// shared memory plan (bytes); core-matrix layouts need 16-byte alignment
-constexpr int SZ_A = M * K * 2;                              // operand A: 128 x 96 FP16
-constexpr int SZ_B = N * K * 2;                              // one operand-B slab: 128 x 96 FP16
-constexpr int OFF_A = 0;
-constexpr int OFF_B = OFF_A + SZ_A;                          // NSLOT slabs
-constexpr int OFF_R16E = OFF_B + NSLOT * SZ_B;               // FP16 region, pairs from even columns
-constexpr int SZ_R16 = ((REG_ROWS * R16_PITCH * 4 + 15) / 16) * 16;
-constexpr int OFF_R16O = OFF_R16E + SZ_R16 + 64;             // pairs from odd columns (16 banks apart)
-constexpr int OFF_SP = OFF_R16O + SZ_R16;                    // per candidate: S hi, S lo, p hi, p lo (FP16)
-constexpr int SZ_SP = MAX_UR * MAX_UC * 8;
-constexpr int OFF_XP = OFF_SP + SZ_SP;                       // per union column: 8 x-window penalties
-constexpr int SZ_XP = (MAX_UC + 1) * 16;
-constexpr int OFF_YP = OFF_XP + SZ_XP;                       // per union row: 16 y-window penalties
-constexpr int SZ_YP = MAX_UR * 32;
-constexpr int OFF_BUF = OFF_YP + SZ_YP;                      // [2][CAP][128] collected flat indices per job parity
-constexpr int SZ_BUF = 2 * CAP * M * 2;
-constexpr int OFF_ROWMAX = OFF_BUF + SZ_BUF;                 // per union row: max candidate |b - c0|^2
-constexpr int OFF_XCH = OFF_ROWMAX + MAX_UR * 4;              // pass-boundary exchange: minima [128][17], T, eps, counts
-constexpr int SZ_XCH = (M * 17 + 5 * M) * 4;
-constexpr int OFF_MISC = OFF_XCH + SZ_XCH;                    // mbarriers, TMEM address, reductions
-constexpr int SMEM_BYTES = OFF_MISC + 160;  // 3 x NSLOT mbarriers, TMEM address, flags, reductions
+// shared memory plan (bytes)
+constexpr int OFF_E = 0;                                     // expanded region, FP16 x 8 per position
+constexpr int SZ_E = E_ENTRIES * 16;
+constexpr int OFF_T = OFF_E + SZ_E;                          // per candidate: S hi, S lo, S hi, p hi, p lo, 0, 0, 0
+constexpr int SZ_T = T_ENTRIES * 16;
+constexpr int OFF_A = OFF_T + SZ_T;                          // operand A: 10 K chunks x 128 rows x 16 bytes
+constexpr int A_KCHUNK = M * 16;
+constexpr int SZ_A = 10 * A_KCHUNK;
+constexpr int OFF_BUF = OFF_A + SZ_A;                        // setup: FP32 region; stream: collected candidates
+constexpr int SZ_REG = REG_ROWS * REG_COLS * 4;
+constexpr int SZ_LIST = 2 * CAP * M * 2;                     // [2][CAP][128] flat indices (16 bits)
+constexpr int SZ_BUF = SZ_REG > SZ_LIST ? SZ_REG : SZ_LIST;
+constexpr int OFF_GMX = OFF_BUF + SZ_BUF;                    // [16][128] odd-parity group minima at the pass boundary
+constexpr int OFF_EPS = OFF_GMX + 16 * M * 4;                // [128] 2 eps
+constexpr int OFF_TX = OFF_EPS + M * 4;                      // [128] collection bound U + 2 eps
+constexpr int OFF_CNT = OFF_TX + M * 4;                      // [2][128] collection counts
+constexpr int OFF_ROWMAX = OFF_CNT + 2 * M * 4;              // [MAX_UR] max |b - c0|^2 per union row
+constexpr int OFF_MISC = OFF_ROWMAX + MAX_UR * 4;            // mbarriers, TMEM address, flags, reductions
+constexpr int SMEM_BYTES = OFF_MISC + 96;
 static_assert(SMEM_BYTES <= 227 * 1024, "tensor-core matcher exceeds shared memory");
-// during setup the slab area holds the FP32 region and the horizontal sums
-constexpr int OFF_REG32 = OFF_B;
-constexpr int OFF_HS = OFF_B + REG_ROWS * REG_COLS * 4;
-static_assert(REG_ROWS * REG_COLS * 4 + 2 * REG_ROWS * MAX_UC * 4 <= NSLOT * SZ_B, "setup scratch exceeds slabs");
+static_assert(OFF_T % 16 == 0 && OFF_A % 128 == 0 && OFF_BUF % 16 == 0 && OFF_MISC % 16 == 0,
+              "shared-memory regions must stay aligned");
+// during setup the E area holds the horizontal sums; during the re-rank the FP32 region
+// (E area) and the exact errors (T area)
+static_assert(2 * REG_ROWS * MAX_UC * 4 <= SZ_E && SZ_REG <= SZ_E && 2 * CAP * M * 4 <= SZ_T, "scratch reuse");
 
-// Operands are K-major with the 64-byte swizzle: per 8-row group, K = 96 is three
-// 512-byte atoms of 8 rows x 32 elements; in row r of an atom the 16-byte chunk
-// c (8 elements) sits at chunk c ^ ((r >> 1) & 3).  core_off = byte offset of the
-// 16-byte piece kc (K elements 8 kc .. 8 kc + 7) of a row.
-__device__ __forceinline__ int core_off(int row, int kc) {
-    return (row >> 3) * 1536 + (kc >> 2) * 512 + (row & 7) * 64 + (((kc & 3) ^ ((row >> 1) & 3)) << 4);
+// Shared-memory matrix descriptor, K-major without swizzle (layout type 0): start
+// address, LBO (distance of K-adjacent core matrices) and SBO (distance of 8-row
+// groups) in 16-byte units, version 1 at bits 46-47 as tcgen05 requires.
+__device__ __forceinline__ uint64_t desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3fff) | ((uint64_t)((lbo >> 4) & 0x3fff) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3fff) << 32) | (1ull << 46);
 }
-
-// ---------------------------------------------------------------------------
-// Operand descriptors and waits of this kernel (the generic tcgen05 / mbarrier
-// wrappers are in zb3d_tcgen05.cuh).
-// ---------------------------------------------------------------------------
-
-// Shared-memory matrix descriptor, K-major with the 64-byte swizzle (layout type 4
-// at bits 61-63): start address and SBO (stride of 8-row groups, 1536 bytes) in
-// 16-byte units, LBO 1 (unused by swizzled K-major layouts), version 1 at bits
-// 46-47 as tcgen05 requires, base offset 0 (atoms are 512-byte aligned).  K step
-// kk (16 elements) starts at atom kk / 2, byte 32 (kk % 2).
-__device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
-    return (uint64_t)((saddr >> 4) & 0x3fff) | (1ull << 16) | ((uint64_t)(1536 >> 4) << 32) | (1ull << 46) |
-           (4ull << 61);
-}
-__device__ __forceinline__ uint32_t kstep_off(int kk) { return (uint32_t)((kk >> 1) * 512 + (kk & 1) * 32); }
 
 // Instruction descriptor of kind::f16: FP16 A and B (both the same type), FP32
 // accumulator, both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
 constexpr uint32_t IDESC = (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-
-__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-    mma_kind_f16(tmem_d, adesc, bdesc, IDESC, accumulate);
-}
 
 // Waits for phase `parity` of an mbarrier, at most WAIT_LIMIT polls; false on
 // timeout.  `polls` counts the unsuccessful polls.
@@ -147,14 +133,12 @@ __device__ __forceinline__ void split_h(float x, __half &hi, __half &lo) {
 // ---------------------------------------------------------------------------
 // Tile geometry.  Tile (blockIdx.x, blockIdx.y) holds reference blocks
 // kx0 + [0, 8) x ky0 + [0, 16); block m = 8 * row + column is TMEM lane m.
-// The candidate union is [ux0, ux0 + nuc) x [uy0, uy0 + nur), enumerated
-// row-major with an odd row stride (flat index f = row * stride + column), so
-// that the 16 groups f mod 16 mix rows and columns; an even nuc gets one padded
-// column.  Chunk c of the MMA stream is the flat range [256 c, 256 c + 256).
+// The candidate union is [ux0, ux0 + nuc) x [uy0, uy0 + nur), flat f = r * nuc + c;
+// chunk c is the flat range [256 c, 256 c + 256).
 // ---------------------------------------------------------------------------
 struct Geom {
     int kx0, ky0, nvx, nvy;
-    int ux0, uy0, nuc, nur, stride, flat, nch;
+    int ux0, uy0, nuc, nur, flat, nch;
 };
 
 __device__ __forceinline__ int block_x(const MatchArgs &a, int kx) { return min(a.bs * kx, a.w - 8); }
@@ -171,8 +155,7 @@ __device__ __forceinline__ Geom tile_geom(const MatchArgs &a) {
     g.uy0 = max(block_y(a, g.ky0) - R, 0);
     g.nuc = min(block_x(a, g.kx0 + g.nvx - 1) + R, a.w - 8) - g.ux0 + 1;
     g.nur = min(block_y(a, g.ky0 + g.nvy - 1) + R, a.h - 8) - g.uy0 + 1;
-    g.stride = g.nuc | 1;
-    g.flat = g.nur * g.stride;
+    g.flat = g.nur * g.nuc;
     g.nch = (g.flat + N - 1) / N;
     return g;
 }
@@ -205,6 +188,23 @@ __device__ __forceinline__ float exact_ssd2(const float2 (&nc)[8][4], const floa
     return ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
 }
 
+// three-operand minimum (sm_100)
+__device__ __forceinline__ float min3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// minimum of 32 values, depth 4
+__device__ __forceinline__ float min32(const float (&v)[32]) {
+    float a[11];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) a[k] = min3(v[3 * k], v[3 * k + 1], v[3 * k + 2]);
+    a[10] = fminf(v[30], v[31]);
+    const float b0 = min3(a[0], a[1], a[2]), b1 = min3(a[3], a[4], a[5]), b2 = min3(a[6], a[7], a[8]);
+    return fminf(min3(b0, b1, b2), fminf(a[9], a[10]));
+}
+
 // Eighth smallest of 16 values (bitonic sort of a register copy).
 __device__ __forceinline__ float eighth_smallest(const float (&g)[16]) {
     float v[16];
@@ -227,79 +227,49 @@ __device__ __forceinline__ float eighth_smallest(const float (&g)[16]) {
     return v[7];
 }
 
-__device__ __forceinline__ uint32_t fsh(uint32_t lo, uint32_t hi) { return __funnelshift_r(lo, hi, 16); }
-
-// three-operand minimum (sm_100)
-__device__ __forceinline__ float min3(float a, float b, float c) {
-    float r;
-    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-}
-
 // floor(f / s) for f < 2^16, s < 2^10: multiply by 2^32 / s rounded up (error < 2^-16)
 __device__ __forceinline__ int div_small(unsigned f, unsigned long long inv) { return (int)((f * inv) >> 32); }
 
-// Operand-B slab of chunk c: candidate n of the chunk is row n; its 96 K entries
-// are the 64 centred FP16 pixels (patch row i = K core matrix i), then
-// [S hi, S lo, S hi, p hi, p lo], the 8 x-window and 16 y-window penalties, 0.
-// Run by the 128 builder threads (b = 0..127), one candidate each.
-__device__ __forceinline__ void build_slab(unsigned char *smem, const Geom &g, int c, int slab, int b) {
-    unsigned char *S = smem + OFF_B + slab * SZ_B;
-    const uint32_t *r16e = reinterpret_cast<const uint32_t *>(smem + OFF_R16E);
-    const uint32_t *r16o = reinterpret_cast<const uint32_t *>(smem + OFF_R16O);
-    const uint2 *sp = reinterpret_cast<const uint2 *>(smem + OFF_SP);
-    const uint4 *xpt = reinterpret_cast<const uint4 *>(smem + OFF_XP);
-    const uint4 *ypt = reinterpret_cast<const uint4 *>(smem + OFF_YP);
-    const uint32_t hb = (uint32_t)__half_as_ushort(__float2half_rn(BIG));
-    const unsigned long long inv = (0x100000000ull + g.stride - 1) / g.stride;
-#pragma unroll 2
-    for (int n = b; n < N; n += 128) {
-        const int f = c * N + n;
-        uint4 pc[12];
-        bool pad = f >= g.flat;
-        int r = 0, cc = 0;
-        if (!pad) {
-            r = div_small((unsigned)f, inv);
-            cc = f - r * g.stride;
-            pad = cc >= g.nuc;
+// Bits j (0..31) of the flat candidates g0 + j that lie in a block's window,
+// union rows [r0, r1] x columns [c0, c1].
+__device__ __forceinline__ uint32_t window_mask(int g0, int nuc, unsigned long long inv, int r0, int r1, int c0,
+                                                int c1) {
+    int r = div_small((unsigned)g0, inv);
+    int off = r * nuc - g0;  // bit index of column 0 of row r (<= 0 for the first row)
+    uint32_t mask = 0;
+    while (off < 32) {
+        if (r >= r0 && r <= r1) {
+            const int jl = max(off + c0, 0), jh = min(off + c1, 31);
+            if (jl <= jh) mask |= (0xffffffffu >> (31 - jh)) & (0xffffffffu << jl);
         }
-        if (pad) {  // not a candidate: every x penalty set
-#pragma unroll
-            for (int i = 0; i < 8; ++i) pc[i] = make_uint4(0, 0, 0, 0);
-            pc[8] = make_uint4(0, 0, hb << 16, hb | (hb << 16));
-            pc[9] = make_uint4(hb | (hb << 16), hb | (hb << 16), hb, 0);
-            pc[10] = make_uint4(0, 0, 0, 0);
-            pc[11] = make_uint4(0, 0, 0, 0);
-        } else {
-            const uint32_t *src = (cc & 1) ? r16o : r16e;
-            const int w0 = cc >> 1;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const uint32_t *rp = src + (r + i) * R16_PITCH + w0;
-                pc[i] = make_uint4(rp[0], rp[1], rp[2], rp[3]);
-            }
-            const uint2 s = sp[r * MAX_UC + cc];
-            const uint4 x = xpt[cc];
-            const uint4 y0 = ypt[2 * r], y1 = ypt[2 * r + 1];
-            pc[8] = make_uint4(s.x, (s.x & 0xffffu) | (s.y << 16), (s.y >> 16) | (x.x << 16), fsh(x.x, x.y));
-            pc[9] = make_uint4(fsh(x.y, x.z), fsh(x.z, x.w), fsh(x.w, y0.x), fsh(y0.x, y0.y));
-            pc[10] = make_uint4(fsh(y0.y, y0.z), fsh(y0.z, y0.w), fsh(y0.w, y1.x), fsh(y1.x, y1.y));
-            pc[11] = make_uint4(fsh(y1.y, y1.z), fsh(y1.z, y1.w), y1.w >> 16, 0);
-        }
-#pragma unroll
-        for (int kc = 0; kc < 12; ++kc) *reinterpret_cast<uint4 *>(S + core_off(n, kc)) = pc[kc];
+        ++r;
+        off += nuc;
     }
+    return mask;
 }
 
-static_assert(OFF_MISC % 16 == 0 && OFF_B % 512 == 0 && SZ_B % 512 == 0 && OFF_SP % 16 == 0 && OFF_XP % 16 == 0 &&
-                  OFF_YP % 16 == 0 && OFF_R16O % 16 == 0,
-              "shared-memory regions must stay 16-byte aligned");
+// (error, scan position) order: the reference's strict-less insertion over a
+// row-major scan keeps, among equal errors, the one scanned first
+__device__ __forceinline__ bool lex_less(float e1, int p1, float e2, int p2) { return e1 < e2 || (e1 == e2 && p1 < p2); }
+
+__device__ __forceinline__ void top8_insert_lex(float (&e)[8], int (&q)[8], float err, int pos) {
+#pragma unroll
+    for (int i = 7; i > 0; --i) {
+        const bool ci = lex_less(err, pos, e[i], q[i]);
+        const bool cp = lex_less(err, pos, e[i - 1], q[i - 1]);
+        e[i] = cp ? e[i - 1] : (ci ? err : e[i]);
+        q[i] = cp ? q[i - 1] : (ci ? pos : q[i]);
+    }
+    if (lex_less(err, pos, e[0], q[0])) {
+        e[0] = err;
+        q[0] = pos;
+    }
+}
 
 __device__ __forceinline__ void list_fallback(const MatchArgs &a, int bi) {
     const int k = atomicAdd(a.tc_ws, 1);
     a.tc_ws[kTcWsList + k] = bi;
 }
-
 
 // Asynchronous copy of the tile's FP32 region (union rows + 7, columns + 7) into
 // shared memory at pitch REG_COLS; columns beyond it are zero-filled.
@@ -318,40 +288,45 @@ __device__ __forceinline__ void stage_region(float *reg, const float *plane, int
 
 // One CTA per tile of 8 x 16 reference blocks.  Warps 0-7 own the blocks: warp w
 // reads TMEM lanes 32 (w mod 4) .. + 31 (block m = lane index) for the jobs of
-// parity w / 4.  Warps 8-11 build the operand-B slabs, lane 0 of warp 12 issues
-// the MMAs.  Jobs j = 0 .. 2 nch - 1 are (pass j / nch, chunk
-// j mod nch) and use slot s = j mod NSLOT: slab s, TMEM columns [128 s, 128 s + 128).
-// The roles meet only at mbarriers: full[s] (slab built, 4 builder warps),
-// done[s] (MMAs of the job complete, tcgen05.commit) and free[s] (TMEM slot read,
-// the 4 warps of the job's parity); job j waits for phase j / NSLOT, and every producer of
-// phase u + 1 first waits for a consumer of phase u, so parities never alias.
+// parity w / 4, which use TMEM slot w / 4 (columns [256 s, 256 s + 256)).  Lane 0 of
+// warp 8 issues the MMAs.  The roles meet at mbarriers: done[s] (MMAs of the job
+// complete, tcgen05.commit) and free[s] (the slot read by the 4 warps of its
+// parity); job j waits for phase (j / 2) mod 2 of both.
 __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const Geom g = tile_geom(a);
-    const int H = a.h, R = a.range, P = a.pitch;
+    const int H = a.h, W = a.w, R = a.range, P = a.pitch;
+    const int nuc = g.nuc;
     const float *plane = a.frames + (long long)a.radius * a.fstride;
 
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + OFF_MISC);    // full[NSLOT], done[NSLOT], free[NSLOT]
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + OFF_MISC + 96);
-    int *oor = reinterpret_cast<int *>(smem + OFF_MISC + 100);
-    int *tmax = reinterpret_cast<int *>(smem + OFF_MISC + 104);        // max |S|, bits of a non-negative float
-    float *red = reinterpret_cast<float *>(smem + OFF_MISC + 112);     // [0..3] mean sums, [4..7] counts
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + OFF_MISC);  // done[2], free[2]
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + OFF_MISC + 32);
+    int *oor = reinterpret_cast<int *>(smem + OFF_MISC + 36);
+    int *tmax = reinterpret_cast<int *>(smem + OFF_MISC + 40);        // max |S|, bits of a non-negative float
+    float *red = reinterpret_cast<float *>(smem + OFF_MISC + 48);     // [0..3] mean sums, [4..7] counts
     float *rowmax = reinterpret_cast<float *>(smem + OFF_ROWMAX);
-    float *reg = reinterpret_cast<float *>(smem + OFF_REG32);
-    float *hs = reinterpret_cast<float *>(smem + OFF_HS);
+    float *reg = reinterpret_cast<float *>(smem + OFF_BUF);           // setup: FP32 region
+    float *hs = reinterpret_cast<float *>(smem + OFF_E);              // setup: horizontal sums
     float *hp = hs + REG_ROWS * MAX_UC;
-    uint16_t *buf = reinterpret_cast<uint16_t *>(smem + OFF_BUF);
+    uint16_t *lists = reinterpret_cast<uint16_t *>(smem + OFF_BUF);   // [2][CAP][128]
+    float *gmx = reinterpret_cast<float *>(smem + OFF_GMX);           // [16][128]
+    float *eps2x = reinterpret_cast<float *>(smem + OFF_EPS);
+    float *tx = reinterpret_cast<float *>(smem + OFF_TX);
+    int *cntx = reinterpret_cast<int *>(smem + OFF_CNT);
     const uint32_t mb = smem_u32(mbar);
-    const uint32_t full0 = mb, done0 = mb + 8 * NSLOT, free0 = mb + 16 * NSLOT;  // slot s at +8 s
+    const uint32_t done0 = mb, free0 = mb + 16;  // slot s at +8 s
+    const unsigned long long inv = (0x100000000ull + nuc - 1) / nuc;
 
     unsigned long long *prof = a.tc_prof ? a.tc_prof + 16 * (blockIdx.y * gridDim.x + blockIdx.x) : nullptr;
     unsigned polls = 0;
     if (prof && tid == 0) prof[0] = clock64();
-    if (warp == 0) tmem_alloc(smem_u32(tslot), 512);
+    if (warp == 8) {
+        __syncwarp();  // tcgen05.alloc is .sync.aligned
+        tmem_alloc(smem_u32(tslot), 512);
+    }
     if (tid == 0) {
-        for (int k = 0; k < NSLOT; ++k) {
-            mbar_init(full0 + 8 * k, 4);
+        for (int k = 0; k < 2; ++k) {
             mbar_init(done0 + 8 * k, 1);
             mbar_init(free0 + 8 * k, 4);
         }
@@ -395,23 +370,14 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     __syncthreads();
     const float c0 = ((red[0] + red[1]) + (red[2] + red[3])) / fmaxf((red[4] + red[5]) + (red[6] + red[7]), 1.0f);
 
-    // ---- FP16 centred region (even / odd pair copies), range check, row sums --
-    // one warp per region row: lane = 32-bit word of the FP16 copies / union column
-    const int rr = g.nur + 7, rc = g.nuc + 7;
-    uint32_t *r16e = reinterpret_cast<uint32_t *>(smem + OFF_R16E);
-    uint32_t *r16o = reinterpret_cast<uint32_t *>(smem + OFF_R16O);
+    // ---- range check, horizontal 8-sums of (x - c0) and (x - c0)^2 ---------------
+    const int rr = g.nur + 7, rc = nuc + 7;
     bool bad = false;
     for (int row = warp; row < rr; row += NWARPS) {
         const float *rp = reg + row * REG_COLS;
-        const int c = 2 * lane;
-        const float x0 = rp[c], x1 = rp[c + 1], x2 = lane < 31 ? rp[c + 2] : 0.0f;
-        const __half h0 = __float2half_rn(c < rc ? x0 - c0 : 0.0f);
-        const __half h1 = __float2half_rn(c + 1 < rc ? x1 - c0 : 0.0f);
-        const __half h2 = __float2half_rn(c + 2 < rc ? x2 - c0 : 0.0f);
-        r16e[row * R16_PITCH + lane] = h2u(h0, h1);
-        r16o[row * R16_PITCH + lane] = h2u(h1, h2);
-        bad |= (c < rc && !(fabsf(x0) <= RANGE)) || (c + 1 < rc && !(fabsf(x1) <= RANGE));
-        for (int cc = lane; cc < g.nuc; cc += 32) {
+        const float x0 = rp[lane], x1 = rp[lane + 32];
+        bad |= (lane < rc && !(fabsf(x0) <= RANGE)) || (lane + 32 < rc && !(fabsf(x1) <= RANGE));
+        for (int cc = lane; cc < nuc; cc += 32) {
             float s = 0.0f, q = 0.0f;
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
@@ -427,12 +393,12 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     __syncthreads();
     if (prof && tid == 0) prof[2] = clock64();
 
-    // ---- per-candidate S, p as FP16 hi/lo, row maxima of p; penalty tables ----
-    uint2 *sp = reinterpret_cast<uint2 *>(smem + OFF_SP);
+    // ---- norm table: per candidate S and p as FP16 hi/lo, row maxima of p ------
+    uint4 *tt = reinterpret_cast<uint4 *>(smem + OFF_T);
     float smax = 0.0f;
     for (int r = warp; r < g.nur; r += NWARPS) {
         float mx = 0.0f;
-        for (int c = lane; c < g.nuc; c += 32) {
+        for (int c = lane; c < nuc; c += 32) {
             float s = 0.0f, q = 0.0f;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
@@ -442,7 +408,7 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
             __half sh, sl, ph, pl;
             split_h(s, sh, sl);
             split_h(q, ph, pl);
-            sp[r * MAX_UC + c] = make_uint2(h2u(sh, sl), h2u(ph, pl));
+            tt[r * nuc + c] = make_uint4(h2u(sh, sl), h2u(sh, ph), h2u(pl, __float2half_rn(0.0f)), 0u);
             smax = fmaxf(smax, fabsf(s));
             mx = fmaxf(mx, q);
         }
@@ -453,35 +419,27 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) smax = fmaxf(smax, __shfl_xor_sync(0xffffffffu, smax, o));
     if (lane == 0) atomicMax(tmax, __float_as_int(smax));
-    const __half hbig = __float2half_rn(BIG), hzero = __float2half_rn(0.0f), hone = __float2half_rn(1.0f);
-    for (int c = tid; c < g.stride; c += THREADS) {
-        __half p[8];
+    for (int i = g.flat + tid; i < T_ENTRIES; i += THREADS) tt[i] = make_uint4(0, 0, 0, 0);
+    __syncthreads();  // the horizontal sums are dead from here on
+
+    // ---- expanded region: E[y][x] = FP16 (x + j, j < 8) - c0 of region row y -----
+    uint4 *ee = reinterpret_cast<uint4 *>(smem + OFF_E);
+    const int ne = rr * nuc;
+    for (int i = tid; i < ne; i += THREADS) {
+        const int y = div_small((unsigned)i, inv), x = i - y * nuc;
+        const float *rp = reg + y * REG_COLS + x;
+        __half h[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const bool out = c >= g.nuc || (j < g.nvx && abs(g.ux0 + c - block_x(a, g.kx0 + j)) > R);
-            p[j] = out ? hbig : hzero;
-        }
-        reinterpret_cast<uint4 *>(smem + OFF_XP)[c] = make_uint4(h2u(p[0], p[1]), h2u(p[2], p[3]), h2u(p[4], p[5]),
-                                                                 h2u(p[6], p[7]));
+        for (int j = 0; j < 8; ++j) h[j] = __float2half_rn(rp[j] - c0);
+        ee[i] = make_uint4(h2u(h[0], h[1]), h2u(h[2], h[3]), h2u(h[4], h[5]), h2u(h[6], h[7]));
     }
-    for (int r = tid; r < g.nur; r += THREADS) {
-        __half p[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const bool out = i < g.nvy && abs(g.uy0 + r - block_y(a, g.ky0 + i)) > R;
-            p[i] = out ? hbig : hzero;
-        }
-        uint4 *yp = reinterpret_cast<uint4 *>(smem + OFF_YP) + 2 * r;
-        yp[0] = make_uint4(h2u(p[0], p[1]), h2u(p[2], p[3]), h2u(p[4], p[5]), h2u(p[6], p[7]));
-        yp[1] = make_uint4(h2u(p[8], p[9]), h2u(p[10], p[11]), h2u(p[12], p[13]), h2u(p[14], p[15]));
-    }
-    __syncthreads();
+    for (int i = ne + tid; i < ne + N; i += THREADS) ee[i] = make_uint4(0, 0, 0, 0);
     if (prof && tid == 0) prof[3] = clock64();
 
     // ---- operand A (one row per block) and the block's error bound ------------
-    float eps = 0.0f;
     if (tid < M) {
-        uint4 pa[12];
+        uint4 pa[10];
+        float eps = 0.0f;
         if (valid) {
             float an2 = 0.0f, ah2 = 0.0f;
 #pragma unroll
@@ -500,23 +458,15 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
             const float nu = mu - c0;
             __half nh, nl;
             split_h(nu, nh, nl);
-            __half e[32];
-            e[0] = __float2half_rn(-2.0f * __half2float(nh));
-            e[1] = e[0];
-            e[2] = __float2half_rn(-2.0f * __half2float(nl));
-            e[3] = e[4] = hone;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) e[5 + j] = j == bxl ? hone : hzero;
-#pragma unroll
-            for (int i = 0; i < 16; ++i) e[13 + i] = i == byl ? hone : hzero;
-            e[29] = e[30] = e[31] = hzero;
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                pa[8 + k] = make_uint4(h2u(e[8 * k], e[8 * k + 1]), h2u(e[8 * k + 2], e[8 * k + 3]),
-                                       h2u(e[8 * k + 4], e[8 * k + 5]), h2u(e[8 * k + 6], e[8 * k + 7]));
+            const __half m2h = __float2half_rn(-2.0f * __half2float(nh));
+            const __half m2l = __float2half_rn(-2.0f * __half2float(nl));
+            const __half one = __float2half_rn(1.0f), zero = __float2half_rn(0.0f);
+            // [S hi, S lo, S hi, p hi, p lo] . [-2 nh, -2 nh, -2 nl, 1, 1]
+            pa[8] = make_uint4(h2u(m2h, m2h), h2u(m2l, one), h2u(one, zero), 0u);
+            pa[9] = make_uint4(0, 0, 0, 0);
             // eps bounds |d - (SSD_ref - |a - c0|^2)| over the block's window:
             // FP16 rounding of both cross-term operands (2^-11 each, x2 for the factor 2),
-            // FP32 accumulation of 96 terms and the hi/lo splits (2^-15 of the term sizes).
+            // FP32 accumulation and the hi/lo splits (2^-15 of the term sizes).
             const int r0 = max(yb - R, 0) - g.uy0, r1 = min(yb + R, H - 8) - g.uy0;
             float pm = 0.0f;
             for (int r = r0; r <= r1; ++r) pm = fmaxf(pm, rowmax[r]);
@@ -526,106 +476,114 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
                   3.0517578125e-05f * (2.0f * an * bm + 2.0f * fabsf(nu) * sm + pm + ah2 + 1.0f);
         } else {
 #pragma unroll
-            for (int k = 0; k < 12; ++k) pa[k] = make_uint4(0, 0, 0, 0);
+            for (int k = 0; k < 10; ++k) pa[k] = make_uint4(0, 0, 0, 0);
         }
 #pragma unroll
-        for (int kc = 0; kc < 12; ++kc) *reinterpret_cast<uint4 *>(smem + OFF_A + core_off(tid, kc)) = pa[kc];
-        fence_async_smem();
+        for (int kc = 0; kc < 10; ++kc)
+            *reinterpret_cast<uint4 *>(smem + OFF_A + kc * A_KCHUNK + (tid >> 3) * 128 + (tid & 7) * 16) = pa[kc];
+        eps2x[tid] = 2.0f * eps;
     }
-    __syncthreads();  // the FP32 region in the slab area is dead from here on
+    fence_async_smem();
+    fence_before_sync();
+    __syncthreads();  // the FP32 region in the list area is dead from here on
+    fence_after_sync();
+    const bool bad_tile = *oor != 0;
+    if (prof && tid == 0) prof[4] = clock64();
 
     // ---- the MMA stream ------------------------------------------------------------
+    // jobs j = 0 .. 2 nch - 1 are (pass j / nch, chunk j mod nch) on TMEM slot j mod 2
     const int nch = g.nch, J = 2 * nch;
-    float *gmx = reinterpret_cast<float *>(smem + OFF_XCH);  // [128][17] odd-parity minima
-    float *Tx = gmx + M * 17, *epsx = Tx + M;
-    int *cntx = reinterpret_cast<int *>(epsx + M);           // [2][128] collection counts per job parity
-    int *okx = cntx + 2 * M;                                 // [128] bound usable
-    if (tid < M) epsx[tid] = eps;
-    __syncthreads();
-    if (prof && tid == 0) prof[4] = clock64();
     int timeout = 0, last = -1;
-    long long t_ld = 0;  // profiling: cycles in TMEM loads (block warps) or slab builds (builders)
+    long long t_ld = 0;  // profiling: cycles in TMEM loads
     int n_ld = 0;
-    if (warp < 8) {
+    if (bad_tile) {
+        // pixels beyond the FP16 sizing: every block of the tile goes to the FP32 scan
+    } else if (warp < 8) {
         const int q = warp & 3, par = warp >> 2, m = 32 * q + lane;
         const int mbx = m & 7, mby = m >> 3;
         const bool mvalid = mbx < g.nvx && mby < g.nvy;
-        uint16_t *mybuf = buf + par * CAP * M;
+        uint16_t *mylist = lists + par * CAP * M;
         // the quarter's blocks need the flat range [flo, fhi)
         int flo = 0, fhi = 0;
         const int by0 = 4 * q, nr = min(4, g.nvy - by0);
         if (nr > 0) {
-            flo = (max(block_y(a, g.ky0 + by0) - R, 0) - g.uy0) * g.stride;
-            fhi = (min(block_y(a, g.ky0 + by0 + nr - 1) + R, H - 8) - g.uy0 + 1) * g.stride;
+            flo = (max(block_y(a, g.ky0 + by0) - R, 0) - g.uy0) * nuc;
+            fhi = (min(block_y(a, g.ky0 + by0 + nr - 1) + R, H - 8) - g.uy0 + 1) * nuc;
         }
+        // the block's window in union coordinates (empty for idle lanes)
+        const int mx = block_x(a, g.kx0 + mbx), my = block_y(a, g.ky0 + mby);
+        const int wr0 = mvalid ? max(my - R, 0) - g.uy0 : 1, wr1 = mvalid ? min(my + R, H - 8) - g.uy0 : 0;
+        const int wc0 = max(mx - R, 0) - g.ux0, wc1 = min(mx + R, W - 8) - g.ux0;
         float gm[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) gm[i] = __int_as_float(0x7f800000);
-        float T = -__int_as_float(0x7f800000);  // collection threshold (stays -inf for idle lanes)
+        float T = -__int_as_float(0x7f800000);  // collection bound (stays -inf for idle lanes)
         int cnt = 0;
         bool have_t = false;
         // pass boundary: the pair (warps q, q + 4) merges its minima and agrees on T
         auto exchange = [&]() {
             if (par == 1) {
 #pragma unroll
-                for (int i = 0; i < 16; ++i) gmx[m * 17 + i] = gm[i];
+                for (int i = 0; i < 16; ++i) gmx[i * M + m] = gm[i];
             }
             asm volatile("bar.sync %0, 64;\n" ::"r"(1 + q) : "memory");
             if (par == 0) {
 #pragma unroll
-                for (int i = 0; i < 16; ++i) gm[i] = fminf(gm[i], gmx[m * 17 + i]);
-                if (mvalid) T = eighth_smallest(gm) + 2.0f * epsx[m];
-                Tx[m] = T;
+                for (int i = 0; i < 16; ++i) gm[i] = fminf(gm[i], gmx[i * M + m]);
+                if (mvalid) T = eighth_smallest(gm) + eps2x[m];
+                tx[m] = T;
             }
             asm volatile("bar.sync %0, 64;\n" ::"r"(1 + q) : "memory");
-            if (par == 1) T = Tx[m];
+            if (par == 1) T = tx[m];
             have_t = true;
         };
         const bool dbg = a.tc_dbg != nullptr && blockIdx.x == 0 && blockIdx.y == 0;
+        const int s = par;
         for (int j = par; j < J; j += 2) {
-            if (j >= nch && !have_t) exchange();
-            const int s = j % NSLOT, base = (j % nch) * N;
-            if (!mbar_wait(done0 + 8 * s, (j / NSLOT) & 1, polls)) {
+            const bool pass2 = j >= nch;
+            if (pass2 && !have_t) exchange();
+            if (!mbar_wait(done0 + 8 * s, (j >> 1) & 1, polls)) {
                 timeout = 1;
                 break;
             }
             fence_after_sync();
-            const bool pass2 = j >= nch;
-            const int s0 = max(flo - base, 0) >> 5;
-            const int s1 = (min(fhi - base, N) + 31) >> 5;
+            const int base = (pass2 ? j - nch : j) * N;
+            const int g_lo = max(flo - base, 0) >> 5;
+            const int g_hi = (min(fhi - base, N) + 31) >> 5;
             const uint32_t tl = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(s * N);
-            for (int sc = s0; sc < s1; ++sc) {
+            for (int gg = g_lo; gg < g_hi; ++gg) {
                 float v[32];
-                __syncwarp();  // tcgen05.ld is warp-collective: reconverge after the collection loop
+                __syncwarp();  // tcgen05.ld is warp-collective: reconverge after the collection code
                 const long long t0 = prof ? clock64() : 0;
-                tmem_ld32(tl + 32 * sc, v);
+                tmem_ld32(tl + 32 * gg, v);
                 if (prof) {
                     t_ld += clock64() - t0;
                     ++n_ld;
                 }
+                const int g0 = base + 32 * gg;
                 if (!pass2) {
-#pragma unroll
-                    for (int r = 0; r < 16; ++r) gm[r] = min3(gm[r], v[r], v[r + 16]);
                     if (dbg) {
-                        float *o = a.tc_dbg + (size_t)m * (nch * N) + base + 32 * sc;
+                        float *o = a.tc_dbg + (size_t)m * (nch * N) + g0;
 #pragma unroll
                         for (int r = 0; r < 32; ++r) o[r] = v[r];
                     }
-                } else {
-                    unsigned h0 = 0, h1 = 0, h2 = 0, h3 = 0;  // four independent chains
+                    // group minima over the block's own window candidates
+                    const uint32_t wm = window_mask(g0, nuc, inv, wr0, wr1, wc0, wc1);
 #pragma unroll
-                    for (int r = 0; r < 8; ++r) {
-                        h0 |= (v[r] <= T ? 1u : 0u) << r;
-                        h1 |= (v[r + 8] <= T ? 1u : 0u) << r;
-                        h2 |= (v[r + 16] <= T ? 1u : 0u) << r;
-                        h3 |= (v[r + 24] <= T ? 1u : 0u) << r;
-                    }
-                    unsigned hit = h0 | (h1 << 8) | (h2 << 16) | (h3 << 24);
-                    while (hit) {
-                        const int r = __ffs(hit) - 1;
-                        hit &= hit - 1;
-                        if (cnt < CAP) mybuf[cnt * M + m] = (uint16_t)(base + 32 * sc + r);
-                        ++cnt;
+                    for (int r = 0; r < 32; ++r)
+                        if (!((wm >> r) & 1u)) v[r] = __int_as_float(0x7f800000);
+#pragma unroll
+                    for (int r = 0; r < 16; ++r) gm[r] = min3(gm[r], v[r], v[r + 16]);
+                } else if (min32(v) <= T) {
+                    const uint32_t wm = window_mask(g0, nuc, inv, wr0, wr1, wc0, wc1);
+                    if (wm) {
+#pragma unroll
+                        for (int r = 0; r < 32; ++r) {
+                            if (((wm >> r) & 1u) && v[r] <= T) {
+                                if (cnt < CAP) mylist[cnt * M + m] = (uint16_t)(g0 + r);
+                                ++cnt;
+                            }
+                        }
                     }
                 }
             }
@@ -635,37 +593,28 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
         }
         if (!have_t) exchange();  // both warps of a pair pass the boundary exactly once
         cntx[par * M + m] = cnt;
-        if (par == 0) okx[m] = T < 0.5f * BIG;  // a bound at penalty level: the window was not covered
-    } else if (warp < 12) {
-        const int b = tid - 256;
+        if (par == 0) tx[m] = T;
+    } else if (warp == 8 && lane == 0) {
+        const uint32_t a_saddr = smem_u32(smem + OFF_A), e_saddr = smem_u32(smem + OFF_E),
+                       t_saddr = smem_u32(smem + OFF_T);
+        const uint32_t row_bytes = 16u * (uint32_t)nuc;
         for (int j = 0; j < J; ++j) {
-            const int s = j % NSLOT;
-            // slab s was last read by job j - NSLOT
-            if (j >= NSLOT && !mbar_wait(done0 + 8 * s, ((j - NSLOT) / NSLOT) & 1, polls)) {
-                timeout = 1;
-                break;
-            }
-            const long long t0 = prof ? clock64() : 0;
-            build_slab(smem, g, j % nch, s, b);
-            if (prof) t_ld += clock64() - t0;
-            fence_async_smem();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(full0 + 8 * s);
-        }
-    } else if (lane == 0) {
-        const uint32_t a_saddr = smem_u32(smem + OFF_A), b_saddr = smem_u32(smem + OFF_B);
-        for (int j = 0; j < J; ++j) {
-            const int s = j % NSLOT;
-            if (!mbar_wait(full0 + 8 * s, (j / NSLOT) & 1, polls) ||
-                (j >= NSLOT && !mbar_wait(free0 + 8 * s, ((j - NSLOT) / NSLOT) & 1, polls))) {
+            const int s = j & 1, c = j < nch ? j : j - nch;
+            if (j >= 2 && !mbar_wait(free0 + 8 * s, ((j - 2) >> 1) & 1, polls)) {
                 timeout = 1;
                 break;
             }
             fence_after_sync();
-            const uint32_t d = tbase + (uint32_t)(s * N), bsa = b_saddr + s * SZ_B;
+            const uint32_t d = tbase + (uint32_t)(s * N);
+            const uint32_t eb = e_saddr + 16u * (uint32_t)(c * N);
 #pragma unroll
-            for (int kk = 0; kk < KSTEPS; ++kk)
-                mma_f16(d, make_desc(a_saddr + kstep_off(kk)), make_desc(bsa + kstep_off(kk)), kk);
+            for (int kk = 0; kk < KSTEPS - 1; ++kk)
+                mma_kind_f16(d, desc(a_saddr + 2 * kk * A_KCHUNK, A_KCHUNK, 128),
+                             desc(eb + 2 * kk * row_bytes, row_bytes, 128), IDESC, kk);
+            // norm terms: one 16-byte table row per candidate; the K step's second 8-element
+            // chunk (A entries zero) reads the next candidate's row
+            mma_kind_f16(d, desc(a_saddr + 8 * A_KCHUNK, A_KCHUNK, 128),
+                         desc(t_saddr + 16u * (uint32_t)(c * N), 16, 128), IDESC, 1);
             mma_commit(done0 + 8 * s);
             last = j;
         }
@@ -674,51 +623,54 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     if (prof) {
         const unsigned wp = __reduce_add_sync(0xffffffffu, polls);
         if (lane == 0) {
-            atomicAdd(prof + (warp < 8 ? 8 : warp < 12 ? 9 : 10), (unsigned long long)wp);
-            if (warp < 12) atomicAdd(prof + (warp < 8 ? 11 : 12), (unsigned long long)t_ld);
-            if (warp < 8) atomicAdd(prof + 13, (unsigned long long)n_ld);
+            atomicAdd(prof + (warp < 8 ? 8 : 10), (unsigned long long)wp);
+            if (warp < 8) {
+                atomicAdd(prof + 11, (unsigned long long)t_ld);
+                atomicAdd(prof + 13, (unsigned long long)n_ld);
+            }
         }
     }
     // ---- drain and release tensor memory -------------------------------------------
-    if (stop && warp == 12 && lane == 0 && last >= 0)
-        mbar_wait(done0 + 8 * (last % NSLOT), (last / NSLOT) & 1, polls);
+    if (stop && warp == 8 && lane == 0 && last >= 0)
+        mbar_wait(done0 + 8 * (last & 1), (last >> 1) & 1, polls);
     if (stop && tid == 0) a.tc_ws[1] = 1;
     fence_before_sync();
     __syncthreads();
-    if (warp == 0) {
+    if (warp == 8) {
+        // lane 0 of this warp ran the MMA loop alone: tcgen05.dealloc is .sync.aligned, so
+        // the warp must be converged before it
+        __syncwarp();
         fence_after_sync();
         tmem_dealloc(tbase, 512);
     }
+    if (prof && tid == 0) prof[5] = clock64();
 
     // ---- exact re-rank of the collected candidates from the FP32 region ------------
     // Three threads per block compute the exact errors of its collected candidates
     // (entries k = grp, grp + 3, ... of [even-job list, odd-job list]); then the
-    // block's thread merges both lists in flat order (= the reference's scan order)
-    // into the reference's insertion rule.
-    stage_region(reg, plane, P, g, tid);
+    // block's thread keeps the eight smallest by (error, scan position).
+    const bool skip_tile = stop || bad_tile;
+    float *reg2 = reinterpret_cast<float *>(smem + OFF_E);  // the FP32 region again
+    float *errs = reinterpret_cast<float *>(smem + OFF_T);  // [2][CAP][128]
+    if (!skip_tile) stage_region(reg2, plane, P, g, tid);
     __syncthreads();
-    if (prof && tid == 0) prof[5] = clock64();
-    float *errs = reg + REG_ROWS * REG_COLS;  // [2][CAP][128], after the region in the slab area
-    const bool bad_tile = stop || *oor;
-    const unsigned long long inv = (0x100000000ull + g.stride - 1) / g.stride;
-    if (tid < 3 * M && !bad_tile) {
+    if (!skip_tile && tid < 3 * M) {
         const int m = tid & 127, grp = tid >> 7;
         const int mbx = m & 7, mby = m >> 3;
         const int c0n = cntx[m], c1n = cntx[M + m];
-        if (mbx < g.nvx && mby < g.nvy && okx[m] && c0n <= CAP && c1n <= CAP) {
+        if (mbx < g.nvx && mby < g.nvy && c0n <= CAP && c1n <= CAP && tx[m] < __int_as_float(0x7f800000)) {
             const int moff = (block_y(a, g.ky0 + mby) - g.uy0) * REG_COLS + (block_x(a, g.kx0 + mbx) - g.ux0);
             float2 nc[8][4];
 #pragma unroll
             for (int i = 0; i < 8; ++i)
 #pragma unroll
                 for (int p = 0; p < 4; ++p)
-                    nc[i][p] = make_float2(-reg[moff + i * REG_COLS + 2 * p], -reg[moff + i * REG_COLS + 2 * p + 1]);
+                    nc[i][p] = make_float2(-reg2[moff + i * REG_COLS + 2 * p], -reg2[moff + i * REG_COLS + 2 * p + 1]);
             for (int k = grp; k < c0n + c1n; k += 3) {
                 const int p = k < c0n ? 0 : 1, idx = (p * CAP + (p ? k - c0n : k)) * M + m;
-                const unsigned f = buf[idx];
-                const int r = div_small(f, inv), cc = (int)f - r * g.stride;
-                // penalised positions are never collected; keep the guard for the index arithmetic
-                errs[idx] = (r < g.nur && cc < g.nuc) ? exact_ssd2(nc, reg + r * REG_COLS + cc, REG_COLS) : ZB_FLT_MAX;
+                const int f = lists[idx];
+                const int r = div_small((unsigned)f, inv), cc = f - r * nuc;
+                errs[idx] = exact_ssd2(nc, reg2 + r * REG_COLS + cc, REG_COLS);
             }
         }
     }
@@ -726,7 +678,7 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     if (prof && tid == 0) prof[6] = clock64();
     if (tid >= M) return;
     const int c0n = cntx[tid], c1n = cntx[M + tid];
-    const bool fb = valid && (bad_tile || !okx[tid] || c0n > CAP || c1n > CAP);
+    const bool fb = valid && (skip_tile || c0n > CAP || c1n > CAP || !(tx[tid] < __int_as_float(0x7f800000)));
     if (valid) {
         const int bi = (g.ky0 + byl) * a.nbx + (g.kx0 + bxl);
         if (fb) {
@@ -737,19 +689,13 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 e[i] = ZB_FLT_MAX;
-                q[i] = 0;
+                q[i] = 0x7fffffff;
             }
-            int i0 = 0, i1 = 0;
-            while (i0 < c0n || i1 < c1n) {
-                const unsigned f0 = i0 < c0n ? buf[i0 * M + tid] : 0xffffffffu;
-                const unsigned f1 = i1 < c1n ? buf[(CAP + i1) * M + tid] : 0xffffffffu;
-                const bool take0 = f0 < f1;  // a flat index belongs to one chunk, so to one list
-                const unsigned f = take0 ? f0 : f1;
-                const float err = take0 ? errs[i0 * M + tid] : errs[(CAP + i1) * M + tid];
-                i0 += take0;
-                i1 += !take0;
-                const int r = div_small(f, inv), cc = (int)f - r * g.stride;
-                if (err < e[7]) top8_insert(e, q, err, pack_pos(g.ux0 + cc, g.uy0 + r));
+            for (int k = 0; k < c0n + c1n; ++k) {
+                const int p = k < c0n ? 0 : 1, idx = (p * CAP + (p ? k - c0n : k)) * M + tid;
+                const int f = lists[idx];
+                const int r = div_small((unsigned)f, inv), cc = f - r * nuc;
+                top8_insert_lex(e, q, errs[idx], pack_pos(g.ux0 + cc, g.uy0 + r));
             }
             store_list(a, bi, xb, yb, e, q);
         }
@@ -795,7 +741,7 @@ int tc_debug_cols(const MatchArgs &a) {
     const int x1 = std::min(std::min(a.bs * (nvx - 1), a.w - 8) + R, a.w - 8);
     const int y1 = std::min(std::min(a.bs * (nvy - 1), a.h - 8) + R, a.h - 8);
     const int nuc = x1 + 1, nur = y1 + 1;
-    const int flat = nur * (nuc | 1);
+    const int flat = nur * nuc;
     return (flat + tc::N - 1) / tc::N * tc::N;
 }
 

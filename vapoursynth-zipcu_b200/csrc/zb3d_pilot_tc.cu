@@ -383,6 +383,7 @@ __global__ void __launch_bounds__(Shape<CIN, COUT>::THREADS, Shape<CIN, COUT>::C
     fence_before_sync();
     __syncthreads();
     if (warp == 2) {
+        __syncwarp();  // tcgen05.dealloc is .sync.aligned: reconverge after the per-lane waits
         fence_after_sync();
         tmem_dealloc(tmem, S::TMEM_COLS);
     }

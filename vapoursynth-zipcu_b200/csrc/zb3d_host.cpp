@@ -32,6 +32,8 @@ namespace zb {
 
 cudaError_t launch_match(MatchArgs a, int metric, int rows_per_cta, bool use_tiled, cudaStream_t st);
 bool tc_eligible(const MatchArgs &a);
+cudaError_t launch_match_tc(const MatchArgs &a, cudaStream_t st);
+cudaError_t launch_tc_fallback(MatchArgs a, cudaStream_t st);
 int tc_debug_cols(const MatchArgs &a);
 size_t match_tile_bytes(const MatchArgs &a, int rows_per_cta);
 cudaError_t launch_filter(const FilterArgs &a, bool final_, int t2d, int t1d, cudaStream_t st);
@@ -1261,18 +1263,32 @@ int zb3d_tc_probe(const float *d_plane, int width, int height, int pitch, int bl
     if (ce == cudaSuccess) ce = cudaMemset(st, 0, 4 * sizeof(unsigned long long));
     a.tc_ws = ws;
     a.tc_stats = st;
-    if (ce == cudaSuccess) ce = launch_match(a, M_SSD, 4, false, nullptr);
+    // the tensor-core kernel alone first, then the FP32 scan of the blocks it listed, each
+    // synchronised, so that an error is attributed to the kernel that raised it
+    a.self_incl = 1;
+    const char *stage = "tensor-core kernel";
+    if (ce == cudaSuccess) ce = launch_match_tc(a, nullptr);
     if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
-    int flag = 0;
+    int ws_head[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (ce == cudaSuccess) ce = cudaMemcpy(ws_head, ws, sizeof ws_head, cudaMemcpyDeviceToHost);
+    if (ce == cudaSuccess) {
+        stage = "FP32 scan of the listed blocks";
+        ce = launch_tc_fallback(a, nullptr);
+    }
+    if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
     if (ce == cudaSuccess) ce = cudaMemcpy(stats, st, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
-    if (ce == cudaSuccess) ce = cudaMemcpy(&flag, ws + 1, sizeof(int), cudaMemcpyDeviceToHost);
     cudaFree(ws);
     cudaFree(st);
     if (ce != cudaSuccess) {
-        set_err(err, errlen, "zb3d_tc_probe: %s.", cudaGetErrorString(ce));
+        set_err(err, errlen, "zb3d_tc_probe: %s (%s).", cudaGetErrorString(ce), stage);
         return -1;
     }
-    if (flag) {
+    if (ws_head[2]) {
+        set_err(err, errlen, "zb3d_tc_probe: self-check %d failed (values %d %d %d, tile %d).", ws_head[2],
+                ws_head[3], ws_head[4], ws_head[5], ws_head[6]);
+        return -1;
+    }
+    if (ws_head[1]) {
         set_err(err, errlen, "zb3d_tc_probe: an MMA wait timed out (its tiles went to the FP32 scan).");
         return -1;
     }

@@ -1030,6 +1030,13 @@ size_t match_tile_bytes(const MatchArgs &a, int rows_per_cta) {
 bool tc_eligible(const MatchArgs &a);                          // zb3d_match_tc.cu
 cudaError_t launch_match_tc(const MatchArgs &a, cudaStream_t st);
 
+// The FP32 scan of the blocks the tensor-core kernel listed (SSD, radius 0).
+cudaError_t launch_tc_fallback(MatchArgs a, cudaStream_t st) {
+    a.self_incl = a.radius == 0;
+    a.gen_mode = 2;
+    return launch_global_m<M_SSD>(a, st);
+}
+
 cudaError_t launch_match(MatchArgs a, int metric, int rows_per_cta, bool use_tiled, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
     const bool tiled = use_tiled && (a.bs == 4 || a.bs == 8);

@@ -266,18 +266,40 @@ __device__ __forceinline__ void top8_insert_lex(float (&e)[8], int (&q)[8], floa
     }
 }
 
+// Self-check of an index, address or descriptor range before it is used.  A failed
+// check skips the access, records the first failure of the launch in tc_ws[2]
+// (code) and tc_ws[3..6] (values, tile), and marks the tile (*tile_bad) so that all
+// its blocks go to the exact matcher.
+__device__ __forceinline__ bool guard(const MatchArgs &a, int *tile_bad, bool ok, int code, int v0, int v1, int v2) {
+    if (!ok) {
+        if (atomicCAS(a.tc_ws + 2, 0, code) == 0) {
+            a.tc_ws[3] = v0;
+            a.tc_ws[4] = v1;
+            a.tc_ws[5] = v2;
+            a.tc_ws[6] = (int)(blockIdx.y * 65536 + blockIdx.x);
+        }
+        *tile_bad = 1;
+    }
+    return ok;
+}
+
 __device__ __forceinline__ void list_fallback(const MatchArgs &a, int bi) {
     const int k = atomicAdd(a.tc_ws, 1);
-    a.tc_ws[kTcWsList + k] = bi;
+    if (k < a.nbx * a.nby) a.tc_ws[kTcWsList + k] = bi;
 }
 
 // Asynchronous copy of the tile's FP32 region (union rows + 7, columns + 7) into
-// shared memory at pitch REG_COLS; columns beyond it are zero-filled.
-__device__ __forceinline__ void stage_region(float *reg, const float *plane, int P, const Geom &g, int tid) {
+// shared memory, at pitch REG_COLS; columns beyond it are zero-filled.  `cap` is
+// the floats the destination area holds.
+__device__ __forceinline__ void stage_region(float *reg, int cap, const float *plane, int P, const Geom &g, int tid,
+                                             const MatchArgs &a, int *tile_bad) {
     const int rr = g.nur + 7, rc = g.nuc + 7;
     for (int i = tid; i < rr * REG_COLS; i += THREADS) {
         const int row = i >> 6, col = i & 63;
         const bool ok = col < rc;
+        if (!guard(a, tile_bad, i < cap && g.uy0 >= 0 && g.uy0 + row < a.h && g.ux0 >= 0 && g.ux0 + (ok ? col : 0) < a.w,
+                   10, g.uy0 + row, g.ux0 + col, i))
+            continue;
         const float *src = plane + (long long)(g.uy0 + row) * P + g.ux0 + (ok ? col : 0);
         asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_u32(reg + i)), "l"(src),
                      "r"(ok ? 4 : 0)
@@ -304,6 +326,7 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + OFF_MISC + 32);
     int *oor = reinterpret_cast<int *>(smem + OFF_MISC + 36);
     int *tmax = reinterpret_cast<int *>(smem + OFF_MISC + 40);        // max |S|, bits of a non-negative float
+    int *tile_bad = reinterpret_cast<int *>(smem + OFF_MISC + 44);    // a self-check failed in this tile
     float *red = reinterpret_cast<float *>(smem + OFF_MISC + 48);     // [0..3] mean sums, [4..7] counts
     float *rowmax = reinterpret_cast<float *>(smem + OFF_ROWMAX);
     float *reg = reinterpret_cast<float *>(smem + OFF_BUF);           // setup: FP32 region
@@ -333,12 +356,15 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         *oor = 0;
         *tmax = 0;
+        *tile_bad = 0;
     }
-    stage_region(reg, plane, P, g, tid);
+    __syncthreads();
+    stage_region(reg, SZ_BUF / 4, plane, P, g, tid, a, tile_bad);
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
     const uint32_t tbase = *tslot;
+    if (tid == 0) guard(a, tile_bad, tbase == 0u, 1, (int)tbase, 0, 0);  // all 512 columns: lane 0, column 0
     if (prof && tid == 0) prof[1] = clock64();
 
     // ---- per-block means; c0 = mean of the tile's block means -----------------
@@ -385,8 +411,10 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
                 s += d;
                 q = fmaf(d, d, q);
             }
-            hs[row * MAX_UC + cc] = s;
-            hp[row * MAX_UC + cc] = q;
+            if (guard(a, tile_bad, row * MAX_UC + cc < REG_ROWS * MAX_UC, 20, row, cc, 0)) {
+                hs[row * MAX_UC + cc] = s;
+                hp[row * MAX_UC + cc] = q;
+            }
         }
     }
     if (bad) *oor = 1;
@@ -408,7 +436,8 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
             __half sh, sl, ph, pl;
             split_h(s, sh, sl);
             split_h(q, ph, pl);
-            tt[r * nuc + c] = make_uint4(h2u(sh, sl), h2u(sh, ph), h2u(pl, __float2half_rn(0.0f)), 0u);
+            if (guard(a, tile_bad, r * nuc + c < T_ENTRIES && (r + 7) * MAX_UC + c < REG_ROWS * MAX_UC, 21, r, c, nuc))
+                tt[r * nuc + c] = make_uint4(h2u(sh, sl), h2u(sh, ph), h2u(pl, __float2half_rn(0.0f)), 0u);
             smax = fmaxf(smax, fabsf(s));
             mx = fmaxf(mx, q);
         }
@@ -431,9 +460,11 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
         __half h[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) h[j] = __float2half_rn(rp[j] - c0);
-        ee[i] = make_uint4(h2u(h[0], h[1]), h2u(h[2], h[3]), h2u(h[4], h[5]), h2u(h[6], h[7]));
+        if (guard(a, tile_bad, i < E_ENTRIES && y * REG_COLS + x + 7 < REG_ROWS * REG_COLS, 22, i, y, x))
+            ee[i] = make_uint4(h2u(h[0], h[1]), h2u(h[2], h[3]), h2u(h[4], h[5]), h2u(h[6], h[7]));
     }
-    for (int i = ne + tid; i < ne + N; i += THREADS) ee[i] = make_uint4(0, 0, 0, 0);
+    for (int i = ne + tid; i < ne + N; i += THREADS)
+        if (guard(a, tile_bad, i < E_ENTRIES, 23, i, ne, 0)) ee[i] = make_uint4(0, 0, 0, 0);
     if (prof && tid == 0) prof[3] = clock64();
 
     // ---- operand A (one row per block) and the block's error bound ------------
@@ -487,7 +518,7 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     fence_before_sync();
     __syncthreads();  // the FP32 region in the list area is dead from here on
     fence_after_sync();
-    const bool bad_tile = *oor != 0;
+    const bool bad_tile = *oor != 0 || *tile_bad != 0;
     if (prof && tid == 0) prof[4] = clock64();
 
     // ---- the MMA stream ------------------------------------------------------------
@@ -554,6 +585,12 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
             for (int gg = g_lo; gg < g_hi; ++gg) {
                 float v[32];
                 __syncwarp();  // tcgen05.ld is warp-collective: reconverge after the collection code
+                if (!guard(a, tile_bad, gg >= 0 && gg < 8 && (tl >> 16) == (uint32_t)(32 * q) &&
+                                            (tl & 0xffffu) + 32u * gg + 32u <= 512u,
+                           40, gg, (int)tl, j)) {
+                    timeout = 1;
+                    break;
+                }
                 const long long t0 = prof ? clock64() : 0;
                 tmem_ld32(tl + 32 * gg, v);
                 if (prof) {
@@ -562,7 +599,7 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
                 }
                 const int g0 = base + 32 * gg;
                 if (!pass2) {
-                    if (dbg) {
+                    if (dbg && guard(a, tile_bad, g0 + 31 < nch * N, 41, g0, m, nch)) {
                         float *o = a.tc_dbg + (size_t)m * (nch * N) + g0;
 #pragma unroll
                         for (int r = 0; r < 32; ++r) o[r] = v[r];
@@ -580,7 +617,8 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
 #pragma unroll
                         for (int r = 0; r < 32; ++r) {
                             if (((wm >> r) & 1u) && v[r] <= T) {
-                                if (cnt < CAP) mylist[cnt * M + m] = (uint16_t)(g0 + r);
+                                if (cnt < CAP && guard(a, tile_bad, g0 + r < g.flat, 42, g0 + r, cnt, g.flat))
+                                    mylist[cnt * M + m] = (uint16_t)(g0 + r);
                                 ++cnt;
                             }
                         }
@@ -607,6 +645,19 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
             fence_after_sync();
             const uint32_t d = tbase + (uint32_t)(s * N);
             const uint32_t eb = e_saddr + 16u * (uint32_t)(c * N);
+            // last byte each operand's descriptors reach: E (8 patch rows of 256 candidates),
+            // the norm table (256 rows + the overlapping second chunk), A (10 K chunks)
+            const uint32_t e_end = eb + 7u * row_bytes + 255u * 16u + 15u;
+            const uint32_t t_end = t_saddr + 16u * (uint32_t)(c * N) + 256u * 16u + 15u;
+            const uint32_t a_end = a_saddr + 10u * A_KCHUNK - 1u;
+            if (!guard(a, tile_bad,
+                       e_end < e_saddr + (uint32_t)SZ_E && t_end < t_saddr + (uint32_t)SZ_T &&
+                           a_end < a_saddr + (uint32_t)SZ_A && (d >> 16) == 0u && (d & 0xffffu) + N <= 512u &&
+                           t_saddr + (uint32_t)SZ_T < (1u << 18),
+                       30, (int)(e_end - e_saddr), (int)(t_end - t_saddr), (int)d)) {
+                timeout = 1;
+                break;
+            }
 #pragma unroll
             for (int kk = 0; kk < KSTEPS - 1; ++kk)
                 mma_kind_f16(d, desc(a_saddr + 2 * kk * A_KCHUNK, A_KCHUNK, 128),
@@ -652,7 +703,7 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     const bool skip_tile = stop || bad_tile;
     float *reg2 = reinterpret_cast<float *>(smem + OFF_E);  // the FP32 region again
     float *errs = reinterpret_cast<float *>(smem + OFF_T);  // [2][CAP][128]
-    if (!skip_tile) stage_region(reg2, plane, P, g, tid);
+    if (!skip_tile) stage_region(reg2, SZ_E / 4, plane, P, g, tid, a, tile_bad);
     __syncthreads();
     if (!skip_tile && tid < 3 * M) {
         const int m = tid & 127, grp = tid >> 7;
@@ -670,7 +721,10 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
                 const int p = k < c0n ? 0 : 1, idx = (p * CAP + (p ? k - c0n : k)) * M + m;
                 const int f = lists[idx];
                 const int r = div_small((unsigned)f, inv), cc = f - r * nuc;
-                errs[idx] = exact_ssd2(nc, reg2 + r * REG_COLS + cc, REG_COLS);
+                errs[idx] = guard(a, tile_bad, f < g.flat && (r + 7) * REG_COLS + cc + 7 < REG_ROWS * REG_COLS, 50,
+                                  f, r, cc)
+                                ? exact_ssd2(nc, reg2 + r * REG_COLS + cc, REG_COLS)
+                                : 0.0f;
             }
         }
     }
@@ -678,7 +732,8 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     if (prof && tid == 0) prof[6] = clock64();
     if (tid >= M) return;
     const int c0n = cntx[tid], c1n = cntx[M + tid];
-    const bool fb = valid && (skip_tile || c0n > CAP || c1n > CAP || !(tx[tid] < __int_as_float(0x7f800000)));
+    const bool fb = valid && (skip_tile || *tile_bad || c0n > CAP || c1n > CAP ||
+                              !(tx[tid] < __int_as_float(0x7f800000)));
     if (valid) {
         const int bi = (g.ky0 + byl) * a.nbx + (g.kx0 + bxl);
         if (fb) {
@@ -697,7 +752,13 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
                 const int r = div_small((unsigned)f, inv), cc = f - r * nuc;
                 top8_insert_lex(e, q, errs[idx], pack_pos(g.ux0 + cc, g.uy0 + r));
             }
-            store_list(a, bi, xb, yb, e, q);
+            bool in_plane = true;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) in_plane = in_plane && pos_x(q[i]) <= W - 8 && pos_y(q[i]) <= H - 8;
+            if (guard(a, tile_bad, in_plane, 60, bi, q[7], c0n + c1n))
+                store_list(a, bi, xb, yb, e, q);
+            else
+                list_fallback(a, bi);
         }
     }
     if (prof && tid == 0) prof[7] = clock64();

@@ -30,7 +30,7 @@ def _tile_geom(w, h, bs, R):
     ux0, uy0 = max(bx[0] - R, 0), max(by[0] - R, 0)
     nuc = min(bx[-1] + R, w - 8) - ux0 + 1
     nur = min(by[-1] + R, h - 8) - uy0 + 1
-    return bx, by, ux0, uy0, nuc, nur, nuc
+    return bx, by, ux0, uy0, nuc, nur, 56  # flat candidates f = row * 56 + column
 
 
 def _expected(plane, w, h, bs, R):
@@ -89,7 +89,7 @@ def test_tc_distances_within_bound(w, h, bs, R, sigma):
     exp, (ux0, uy0, nuc, nur, stride) = _expected(plane, w, h, bs, R)
     worst = 0.0
     for m, (d, win, eps) in exp.items():
-        row = dist[m][:nur * stride].reshape(nur, stride)
+        row = dist[m][:nur * stride].reshape(nur, stride)[:, :nuc]
         assert not np.isnan(row[win]).any(), f"block {m}: window candidates not read"
         err = np.abs(row[win] - d[win])
         worst = max(worst, float((err / eps).max()))

@@ -6,20 +6,27 @@
 //
 //  1. A tile is 8 x 16 reference blocks (M = 128 rows of the MMA, TMEM lane m =
 //     block m).  The candidate positions of the union of their search windows,
-//     nur rows x nuc columns, are numbered row-major: flat f = r * nuc + c.  They
-//     stream through tcgen05.mma (kind::f16, FP32 accumulation in tensor memory)
-//     in chunks of N = 256 consecutive f.  Row m of the product is, for block m
-//     and candidate f,
+//     nur rows x nuc columns (nuc <= 56), are numbered row-major at a fixed row
+//     pitch of 56: flat f = r * 56 + c.  They stream through tcgen05.mma
+//     (kind::f16, FP32 accumulation in tensor memory) in chunks of N = 224
+//     consecutive f, i.e. 4 whole rows.  Row m of the product is, for block m and
+//     a candidate f inside block m's columns,
 //         d(m, f) = |b_f - c0|^2 - 2 (mu_m - c0) S_f - 2 (a_m - mu_m) . (b_f - c0)
 //     (c0 a tile constant, mu_m the block mean, S_f the candidate sum), which
 //     equals SSD(a_m, b_f) - |a_m - c0|^2.  The pixel cross term runs on FP16
-//     operands, the norm terms enter as FP16 hi/lo pairs in a fifth K step.
+//     operands; the norm terms enter as FP16 hi/lo pairs in a fifth K step, whose
+//     second half adds 16384 where the candidate's column lies outside block m's
+//     window (a one-hot of the block column in A against a per-column penalty row
+//     in B; the penalty rows repeat every 56 candidates, so one 224-row table
+//     serves every chunk).
 //  2. Operand B needs no per-chunk build: the tile's region is expanded once into
 //     E[y][x] = the 8 FP16 pixels (y, x .. x + 7) - c0, 16 bytes per position, at
-//     a row pitch of nuc positions.  Patch row i of candidate f is then E entry
-//     f + i * nuc, so one shared-memory descriptor (8-row core matrices 128 bytes
-//     apart, K chunks one E row apart) walks 256 consecutive candidates and the
+//     the row pitch of 56 positions.  Patch row i of candidate f is then E entry
+//     f + 56 i, so one shared-memory descriptor (8-row core matrices 128 bytes
+//     apart, K chunks one E row apart) walks 224 consecutive candidates and the
 //     8 patch rows.  The norm terms sit in a per-candidate table read the same way.
+//     A 32-column group of a chunk spans at most two rows, so the window's rows
+//     are two compares per block and group.
 //  3. Pass 1 keeps, per block, the minimum of d over 16 groups of its window
 //     candidates (flat index mod 16).  The eighth smallest group minimum U comes
 //     from eight distinct window candidates, so the reference's eighth-best FP32
@@ -55,42 +62,49 @@ namespace tc {
 using namespace tc05;
 
 constexpr int BX = 8, BY = 16, M = BX * BY;  // reference blocks per tile
-constexpr int N = 256;                       // candidates per MMA chunk = TMEM columns of one slot
-constexpr int KSTEPS = 5;                    // patch rows (0,1) (2,3) (4,5) (6,7), then the norm terms
-constexpr int MAX_UC = 56, MAX_UR = 88;      // candidate union of a tile: columns, rows
+constexpr int WX = 56;                       // flat row pitch: candidate columns per union row (nuc <= WX)
+constexpr int ROWS_PER_CHUNK = 4;
+constexpr int N = ROWS_PER_CHUNK * WX;       // candidates per MMA chunk = TMEM columns of one slot (224)
+constexpr int NGROUP = N / 32;               // 32-column TMEM loads per chunk
+constexpr int KSTEPS = 5;                    // patch rows (0,1) (2,3) (4,5) (6,7), then norms + column penalties
+constexpr int MAX_UC = WX, MAX_UR = 88;      // candidate union of a tile: columns, rows
 constexpr int REG_ROWS = MAX_UR + 7;
 constexpr int REG_COLS = 64;                 // staged FP32 region: columns (union + 7, padded)
-constexpr int E_ENTRIES = REG_ROWS * MAX_UC + N;   // + the tail the last chunk reads
-constexpr int T_ENTRIES = MAX_UR * MAX_UC + N + 16;
-constexpr int CAP = 48;                      // collected candidates per block and job parity
+constexpr int E_ROWS = MAX_UR + ROWS_PER_CHUNK - 1 + 7;  // candidate rows of the last chunk + 7 patch rows
+constexpr int T_ROWS = MAX_UR + ROWS_PER_CHUNK - 1;
+constexpr int CAP = 32;                      // collected candidates per block and job parity
 constexpr int THREADS = 384;                 // warps 0-7: blocks (two per lane quarter: even / odd
                                              // jobs), warp 8: TMEM owner and MMA issuer, 9-11: setup
 constexpr int NWARPS = THREADS / 32;
+constexpr float BIG = 16384.0f;              // column-window penalty (exact in FP16)
 constexpr float RANGE = 4.0f;                // pixel magnitude the FP16 terms are sized for
 constexpr unsigned WAIT_LIMIT = 1u << 22;    // polls of an mbarrier before giving up (~0.5 s)
 
 // shared memory plan (bytes)
 constexpr int OFF_E = 0;                                     // expanded region, FP16 x 8 per position
-constexpr int SZ_E = E_ENTRIES * 16;
+constexpr int SZ_E = E_ROWS * WX * 16;
 constexpr int OFF_T = OFF_E + SZ_E;                          // per candidate: S hi, S lo, S hi, p hi, p lo, 0, 0, 0
-constexpr int SZ_T = T_ENTRIES * 16;
-constexpr int OFF_A = OFF_T + SZ_T;                          // operand A: 10 K chunks x 128 rows x 16 bytes
+constexpr int SZ_T = T_ROWS * WX * 16;
+constexpr int OFF_XP = OFF_T + SZ_T;                         // per chunk column: 8 block-column penalties (FP16)
+constexpr int SZ_XP = N * 16;
+constexpr int OFF_A = OFF_XP + SZ_XP;                        // operand A: 10 K chunks x 128 rows x 16 bytes
 constexpr int A_KCHUNK = M * 16;
 constexpr int SZ_A = 10 * A_KCHUNK;
-constexpr int OFF_BUF = OFF_A + SZ_A;                        // setup: FP32 region; stream: collected candidates
+constexpr int OFF_BUF = OFF_A + SZ_A;                        // setup: FP32 region; stream: lists + group minima
 constexpr int SZ_REG = REG_ROWS * REG_COLS * 4;
 constexpr int SZ_LIST = 2 * CAP * M * 2;                     // [2][CAP][128] flat indices (16 bits)
-constexpr int SZ_BUF = SZ_REG > SZ_LIST ? SZ_REG : SZ_LIST;
-constexpr int OFF_GMX = OFF_BUF + SZ_BUF;                    // [16][128] odd-parity group minima at the pass boundary
-constexpr int OFF_EPS = OFF_GMX + 16 * M * 4;                // [128] 2 eps
+constexpr int OFF_GMX = OFF_BUF + SZ_LIST;                   // [16][128] odd-parity group minima at the pass boundary
+constexpr int SZ_BUF = SZ_REG > SZ_LIST + 16 * M * 4 ? SZ_REG : SZ_LIST + 16 * M * 4;
+constexpr int OFF_EPS = OFF_BUF + SZ_BUF;                    // [128] 2 eps
 constexpr int OFF_TX = OFF_EPS + M * 4;                      // [128] collection bound U + 2 eps
 constexpr int OFF_CNT = OFF_TX + M * 4;                      // [2][128] collection counts
 constexpr int OFF_ROWMAX = OFF_CNT + 2 * M * 4;              // [MAX_UR] max |b - c0|^2 per union row
 constexpr int OFF_MISC = OFF_ROWMAX + MAX_UR * 4;            // mbarriers, TMEM address, flags, reductions
 constexpr int SMEM_BYTES = OFF_MISC + 96;
 static_assert(SMEM_BYTES <= 227 * 1024, "tensor-core matcher exceeds shared memory");
-static_assert(OFF_T % 16 == 0 && OFF_A % 128 == 0 && OFF_BUF % 16 == 0 && OFF_MISC % 16 == 0,
+static_assert(OFF_T % 16 == 0 && OFF_XP % 16 == 0 && OFF_A % 128 == 0 && OFF_BUF % 16 == 0 && OFF_MISC % 16 == 0,
               "shared-memory regions must stay aligned");
+static_assert(N % 16 == 0 && N <= 256 && 2 * N <= 512 && N % 32 == 0, "chunk shape");
 // during setup the E area holds the horizontal sums; during the re-rank the FP32 region
 // (E area) and the exact errors (T area)
 static_assert(2 * REG_ROWS * MAX_UC * 4 <= SZ_E && SZ_REG <= SZ_E && 2 * CAP * M * 4 <= SZ_T, "scratch reuse");
@@ -133,8 +147,8 @@ __device__ __forceinline__ void split_h(float x, __half &hi, __half &lo) {
 // ---------------------------------------------------------------------------
 // Tile geometry.  Tile (blockIdx.x, blockIdx.y) holds reference blocks
 // kx0 + [0, 8) x ky0 + [0, 16); block m = 8 * row + column is TMEM lane m.
-// The candidate union is [ux0, ux0 + nuc) x [uy0, uy0 + nur), flat f = r * nuc + c;
-// chunk c is the flat range [256 c, 256 c + 256).
+// The candidate union is [ux0, ux0 + nuc) x [uy0, uy0 + nur), flat f = r * 56 + c;
+// chunk k is the flat range [224 k, 224 k + 224), union rows 4 k .. 4 k + 3.
 // ---------------------------------------------------------------------------
 struct Geom {
     int kx0, ky0, nvx, nvy;
@@ -155,8 +169,8 @@ __device__ __forceinline__ Geom tile_geom(const MatchArgs &a) {
     g.uy0 = max(block_y(a, g.ky0) - R, 0);
     g.nuc = min(block_x(a, g.kx0 + g.nvx - 1) + R, a.w - 8) - g.ux0 + 1;
     g.nur = min(block_y(a, g.ky0 + g.nvy - 1) + R, a.h - 8) - g.uy0 + 1;
-    g.flat = g.nur * g.nuc;
-    g.nch = (g.flat + N - 1) / N;
+    g.flat = g.nur * WX;
+    g.nch = (g.nur + ROWS_PER_CHUNK - 1) / ROWS_PER_CHUNK;
     return g;
 }
 
@@ -227,26 +241,8 @@ __device__ __forceinline__ float eighth_smallest(const float (&g)[16]) {
     return v[7];
 }
 
-// floor(f / s) for f < 2^16, s < 2^10: multiply by 2^32 / s rounded up (error < 2^-16)
-__device__ __forceinline__ int div_small(unsigned f, unsigned long long inv) { return (int)((f * inv) >> 32); }
-
-// Bits j (0..31) of the flat candidates g0 + j that lie in a block's window,
-// union rows [r0, r1] x columns [c0, c1].
-__device__ __forceinline__ uint32_t window_mask(int g0, int nuc, unsigned long long inv, int r0, int r1, int c0,
-                                                int c1) {
-    int r = div_small((unsigned)g0, inv);
-    int off = r * nuc - g0;  // bit index of column 0 of row r (<= 0 for the first row)
-    uint32_t mask = 0;
-    while (off < 32) {
-        if (r >= r0 && r <= r1) {
-            const int jl = max(off + c0, 0), jh = min(off + c1, 31);
-            if (jl <= jh) mask |= (0xffffffffu >> (31 - jh)) & (0xffffffffu << jl);
-        }
-        ++r;
-        off += nuc;
-    }
-    return mask;
-}
+// Bits [0, b) set (b in 0..32).
+__device__ __forceinline__ uint32_t low_bits(int b) { return b >= 32 ? 0xffffffffu : ((1u << b) - 1u); }
 
 // (error, scan position) order: the reference's strict-less insertion over a
 // row-major scan keeps, among equal errors, the one scanned first
@@ -310,7 +306,7 @@ __device__ __forceinline__ void stage_region(float *reg, int cap, const float *p
 
 // One CTA per tile of 8 x 16 reference blocks.  Warps 0-7 own the blocks: warp w
 // reads TMEM lanes 32 (w mod 4) .. + 31 (block m = lane index) for the jobs of
-// parity w / 4, which use TMEM slot w / 4 (columns [256 s, 256 s + 256)).  Lane 0 of
+// parity w / 4, which use TMEM slot w / 4 (columns [224 s, 224 s + 224)).  Lane 0 of
 // warp 8 issues the MMAs.  The roles meet at mbarriers: done[s] (MMAs of the job
 // complete, tcgen05.commit) and free[s] (the slot read by the 4 warps of its
 // parity); job j waits for phase (j / 2) mod 2 of both.
@@ -339,9 +335,12 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     int *cntx = reinterpret_cast<int *>(smem + OFF_CNT);
     const uint32_t mb = smem_u32(mbar);
     const uint32_t done0 = mb, free0 = mb + 16;  // slot s at +8 s
-    const unsigned long long inv = (0x100000000ull + nuc - 1) / nuc;
 
     unsigned long long *prof = a.tc_prof ? a.tc_prof + 16 * (blockIdx.y * gridDim.x + blockIdx.x) : nullptr;
+    // tile (1, 1) also traces every job after the per-tile blocks: [j][0] issued (MMA thread,
+    // after its commit), [j][1] completion seen and [j][2] slot freed (warp 0 or 4, lane 0)
+    unsigned long long *trace = (a.tc_prof && blockIdx.x == 1 && blockIdx.y == 1)
+                                    ? a.tc_prof + 16 * (gridDim.x * gridDim.y) : nullptr;
     unsigned polls = 0;
     if (prof && tid == 0) prof[0] = clock64();
     if (warp == 8) {
@@ -422,49 +421,71 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     if (prof && tid == 0) prof[2] = clock64();
 
     // ---- norm table: per candidate S and p as FP16 hi/lo, row maxima of p ------
+    // rows up to the last chunk's; columns nuc .. 55 and rows nur .. zero (never in a window)
     uint4 *tt = reinterpret_cast<uint4 *>(smem + OFF_T);
+    const int trows = g.nch * ROWS_PER_CHUNK;
     float smax = 0.0f;
-    for (int r = warp; r < g.nur; r += NWARPS) {
+    for (int r = warp; r < trows; r += NWARPS) {
         float mx = 0.0f;
-        for (int c = lane; c < nuc; c += 32) {
-            float s = 0.0f, q = 0.0f;
+        for (int c = lane; c < WX; c += 32) {
+            uint4 e = make_uint4(0, 0, 0, 0);
+            if (r < g.nur && c < nuc) {
+                float s = 0.0f, q = 0.0f;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                s += hs[(r + k) * MAX_UC + c];
-                q += hp[(r + k) * MAX_UC + c];
+                for (int k = 0; k < 8; ++k) {
+                    s += hs[(r + k) * MAX_UC + c];
+                    q += hp[(r + k) * MAX_UC + c];
+                }
+                __half sh, sl, ph, pl;
+                split_h(s, sh, sl);
+                split_h(q, ph, pl);
+                e = make_uint4(h2u(sh, sl), h2u(sh, ph), h2u(pl, __float2half_rn(0.0f)), 0u);
+                smax = fmaxf(smax, fabsf(s));
+                mx = fmaxf(mx, q);
             }
-            __half sh, sl, ph, pl;
-            split_h(s, sh, sl);
-            split_h(q, ph, pl);
-            if (guard(a, tile_bad, r * nuc + c < T_ENTRIES && (r + 7) * MAX_UC + c < REG_ROWS * MAX_UC, 21, r, c, nuc))
-                tt[r * nuc + c] = make_uint4(h2u(sh, sl), h2u(sh, ph), h2u(pl, __float2half_rn(0.0f)), 0u);
-            smax = fmaxf(smax, fabsf(s));
-            mx = fmaxf(mx, q);
+            if (guard(a, tile_bad, r < T_ROWS, 21, r, c, 0)) tt[r * WX + c] = e;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        if (lane == 0) rowmax[r] = mx;
+        if (lane == 0 && r < g.nur) rowmax[r] = mx;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) smax = fmaxf(smax, __shfl_xor_sync(0xffffffffu, smax, o));
     if (lane == 0) atomicMax(tmax, __float_as_int(smax));
-    for (int i = g.flat + tid; i < T_ENTRIES; i += THREADS) tt[i] = make_uint4(0, 0, 0, 0);
+    // column penalties: chunk column n is union column n mod 56; block column j's window
+    // is [x_j - R, x_j + R]; columns at or beyond nuc are not candidates
+    {
+        const __half hbig = __float2half_rn(BIG), hzero = __float2half_rn(0.0f);
+        uint4 *xp = reinterpret_cast<uint4 *>(smem + OFF_XP);
+        for (int n = tid; n < N; n += THREADS) {
+            const int c = n % WX;
+            __half pnl[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const bool out = c >= nuc || (j < g.nvx && abs(g.ux0 + c - block_x(a, g.kx0 + j)) > R);
+                pnl[j] = out ? hbig : hzero;
+            }
+            xp[n] = make_uint4(h2u(pnl[0], pnl[1]), h2u(pnl[2], pnl[3]), h2u(pnl[4], pnl[5]), h2u(pnl[6], pnl[7]));
+        }
+    }
     __syncthreads();  // the horizontal sums are dead from here on
 
     // ---- expanded region: E[y][x] = FP16 (x + j, j < 8) - c0 of region row y -----
+    // rows beyond the region (read only by the last chunk's padding rows) are zero
     uint4 *ee = reinterpret_cast<uint4 *>(smem + OFF_E);
-    const int ne = rr * nuc;
-    for (int i = tid; i < ne; i += THREADS) {
-        const int y = div_small((unsigned)i, inv), x = i - y * nuc;
-        const float *rp = reg + y * REG_COLS + x;
-        __half h[8];
+    const int erows = trows + 7;
+    for (int i = tid; i < erows * WX; i += THREADS) {
+        const int y = i / WX, x = i - y * WX;
+        uint4 e = make_uint4(0, 0, 0, 0);
+        if (y < rr) {
+            const float *rp = reg + y * REG_COLS + x;
+            __half h[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) h[j] = __float2half_rn(rp[j] - c0);
-        if (guard(a, tile_bad, i < E_ENTRIES && y * REG_COLS + x + 7 < REG_ROWS * REG_COLS, 22, i, y, x))
-            ee[i] = make_uint4(h2u(h[0], h[1]), h2u(h[2], h[3]), h2u(h[4], h[5]), h2u(h[6], h[7]));
+            for (int j = 0; j < 8; ++j) h[j] = __float2half_rn(rp[j] - c0);
+            e = make_uint4(h2u(h[0], h[1]), h2u(h[2], h[3]), h2u(h[4], h[5]), h2u(h[6], h[7]));
+        }
+        if (guard(a, tile_bad, y < E_ROWS && x + 7 < REG_COLS, 22, i, y, x)) ee[i] = e;
     }
-    for (int i = ne + tid; i < ne + N; i += THREADS)
-        if (guard(a, tile_bad, i < E_ENTRIES, 23, i, ne, 0)) ee[i] = make_uint4(0, 0, 0, 0);
     if (prof && tid == 0) prof[3] = clock64();
 
     // ---- operand A (one row per block) and the block's error bound ------------
@@ -492,12 +513,16 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
             const __half m2h = __float2half_rn(-2.0f * __half2float(nh));
             const __half m2l = __float2half_rn(-2.0f * __half2float(nl));
             const __half one = __float2half_rn(1.0f), zero = __float2half_rn(0.0f);
-            // [S hi, S lo, S hi, p hi, p lo] . [-2 nh, -2 nh, -2 nl, 1, 1]
+            // [S hi, S lo, S hi, p hi, p lo] . [-2 nh, -2 nh, -2 nl, 1, 1], then the block
+            // column's one-hot against the column penalties
             pa[8] = make_uint4(h2u(m2h, m2h), h2u(m2l, one), h2u(one, zero), 0u);
-            pa[9] = make_uint4(0, 0, 0, 0);
+            __half oh[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) oh[j] = j == bxl ? one : zero;
+            pa[9] = make_uint4(h2u(oh[0], oh[1]), h2u(oh[2], oh[3]), h2u(oh[4], oh[5]), h2u(oh[6], oh[7]));
             // eps bounds |d - (SSD_ref - |a - c0|^2)| over the block's window:
             // FP16 rounding of both cross-term operands (2^-11 each, x2 for the factor 2),
-            // FP32 accumulation and the hi/lo splits (2^-15 of the term sizes).
+            // FP32 accumulation and the hi/lo splits (2^-15 of the term sizes)
             const int r0 = max(yb - R, 0) - g.uy0, r1 = min(yb + R, H - 8) - g.uy0;
             float pm = 0.0f;
             for (int r = r0; r <= r1; ++r) pm = fmaxf(pm, rowmax[r]);
@@ -534,17 +559,17 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
         const int mbx = m & 7, mby = m >> 3;
         const bool mvalid = mbx < g.nvx && mby < g.nvy;
         uint16_t *mylist = lists + par * CAP * M;
-        // the quarter's blocks need the flat range [flo, fhi)
-        int flo = 0, fhi = 0;
+        // the quarter's blocks need union rows [qr0, qr1]
+        int qr0 = 1, qr1 = 0;
         const int by0 = 4 * q, nr = min(4, g.nvy - by0);
         if (nr > 0) {
-            flo = (max(block_y(a, g.ky0 + by0) - R, 0) - g.uy0) * nuc;
-            fhi = (min(block_y(a, g.ky0 + by0 + nr - 1) + R, H - 8) - g.uy0 + 1) * nuc;
+            qr0 = max(block_y(a, g.ky0 + by0) - R, 0) - g.uy0;
+            qr1 = min(block_y(a, g.ky0 + by0 + nr - 1) + R, H - 8) - g.uy0;
         }
-        // the block's window in union coordinates (empty for idle lanes)
-        const int mx = block_x(a, g.kx0 + mbx), my = block_y(a, g.ky0 + mby);
+        // the block's window rows (empty for idle lanes); its columns are handled by the
+        // penalties inside the product
+        const int my = block_y(a, g.ky0 + mby);
         const int wr0 = mvalid ? max(my - R, 0) - g.uy0 : 1, wr1 = mvalid ? min(my + R, H - 8) - g.uy0 : 0;
-        const int wc0 = max(mx - R, 0) - g.ux0, wc1 = min(mx + R, W - 8) - g.ux0;
         float gm[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) gm[i] = __int_as_float(0x7f800000);
@@ -557,14 +582,16 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
 #pragma unroll
                 for (int i = 0; i < 16; ++i) gmx[i * M + m] = gm[i];
             }
-            asm volatile("bar.sync %0, 64;\n" ::"r"(1 + q) : "memory");
+            __syncwarp();
+            asm volatile("barrier.sync %0, 64;\n" ::"r"(1 + q) : "memory");
             if (par == 0) {
 #pragma unroll
                 for (int i = 0; i < 16; ++i) gm[i] = fminf(gm[i], gmx[i * M + m]);
                 if (mvalid) T = eighth_smallest(gm) + eps2x[m];
                 tx[m] = T;
             }
-            asm volatile("bar.sync %0, 64;\n" ::"r"(1 + q) : "memory");
+            __syncwarp();
+            asm volatile("barrier.sync %0, 64;\n" ::"r"(1 + q) : "memory");
             if (par == 1) T = tx[m];
             have_t = true;
         };
@@ -578,15 +605,18 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
                 break;
             }
             fence_after_sync();
-            const int base = (pass2 ? j - nch : j) * N;
-            const int g_lo = max(flo - base, 0) >> 5;
-            const int g_hi = (min(fhi - base, N) + 31) >> 5;
+            if (trace && q == 0 && lane == 0) trace[3 * j + 1] = clock64();
+            const int ck = pass2 ? j - nch : j;
+            const int row0 = ROWS_PER_CHUNK * ck;
             const uint32_t tl = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(s * N);
-            for (int gg = g_lo; gg < g_hi; ++gg) {
+            for (int gg = 0; gg < NGROUP; ++gg) {
+                // group gg: chunk columns 32 gg .. + 31, union rows ra (bits below bnd) and rb
+                const int ra = row0 + (32 * gg) / WX, rb = row0 + (32 * gg + 31) / WX;
+                if (rb < qr0 || ra > qr1) continue;  // no block of this quarter looks at these rows
+                const int bnd = rb > ra ? (rb - row0) * WX - 32 * gg : 32;
                 float v[32];
                 __syncwarp();  // tcgen05.ld is warp-collective: reconverge after the collection code
-                if (!guard(a, tile_bad, gg >= 0 && gg < 8 && (tl >> 16) == (uint32_t)(32 * q) &&
-                                            (tl & 0xffffu) + 32u * gg + 32u <= 512u,
+                if (!guard(a, tile_bad, (tl >> 16) == (uint32_t)(32 * q) && (tl & 0xffffu) + 32u * gg + 32u <= 512u,
                            40, gg, (int)tl, j)) {
                     timeout = 1;
                     break;
@@ -597,45 +627,54 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
                     t_ld += clock64() - t0;
                     ++n_ld;
                 }
-                const int g0 = base + 32 * gg;
+                const int g0 = ck * N + 32 * gg;
+                const bool ina = ra >= wr0 && ra <= wr1, inb = rb >= wr0 && rb <= wr1;
+                const uint32_t ymask = (ina ? low_bits(bnd) : 0u) | (inb ? ~low_bits(bnd) : 0u);
                 if (!pass2) {
                     if (dbg && guard(a, tile_bad, g0 + 31 < nch * N, 41, g0, m, nch)) {
                         float *o = a.tc_dbg + (size_t)m * (nch * N) + g0;
 #pragma unroll
                         for (int r = 0; r < 32; ++r) o[r] = v[r];
                     }
-                    // group minima over the block's own window candidates
-                    const uint32_t wm = window_mask(g0, nuc, inv, wr0, wr1, wc0, wc1);
+                    // group minima (flat index mod 16) over the block's window rows; out-of-window
+                    // columns carry the penalty
+                    if (ymask == 0xffffffffu) {
 #pragma unroll
-                    for (int r = 0; r < 32; ++r)
-                        if (!((wm >> r) & 1u)) v[r] = __int_as_float(0x7f800000);
+                        for (int r = 0; r < 16; ++r) gm[r] = min3(gm[r], v[r], v[r + 16]);
+                    } else if (ymask) {
 #pragma unroll
-                    for (int r = 0; r < 16; ++r) gm[r] = min3(gm[r], v[r], v[r + 16]);
-                } else if (min32(v) <= T) {
-                    const uint32_t wm = window_mask(g0, nuc, inv, wr0, wr1, wc0, wc1);
-                    if (wm) {
+                        for (int r = 0; r < 32; ++r)
+                            if (!((ymask >> r) & 1u)) v[r] = __int_as_float(0x7f800000);
 #pragma unroll
-                        for (int r = 0; r < 32; ++r) {
-                            if (((wm >> r) & 1u) && v[r] <= T) {
-                                if (cnt < CAP && guard(a, tile_bad, g0 + r < g.flat, 42, g0 + r, cnt, g.flat))
-                                    mylist[cnt * M + m] = (uint16_t)(g0 + r);
-                                ++cnt;
-                            }
-                        }
+                        for (int r = 0; r < 16; ++r) gm[r] = min3(gm[r], v[r], v[r + 16]);
+                    }
+                } else if (ymask && min32(v) <= T) {
+                    uint32_t hit = 0;
+#pragma unroll
+                    for (int r = 0; r < 32; ++r) hit |= (v[r] <= T ? 1u : 0u) << r;
+                    hit &= ymask;
+                    while (hit) {
+                        const int r = __ffs(hit) - 1;
+                        hit &= hit - 1;
+                        if (cnt < CAP && guard(a, tile_bad, g0 + r < g.flat, 42, g0 + r, cnt, g.flat))
+                            mylist[cnt * M + m] = (uint16_t)(g0 + r);
+                        ++cnt;
                     }
                 }
             }
             fence_before_sync();
             __syncwarp();
             if (lane == 0) mbar_arrive(free0 + 8 * s);
+            if (trace && q == 0 && lane == 0) trace[3 * j + 2] = clock64();
+            if (timeout) break;
         }
         if (!have_t) exchange();  // both warps of a pair pass the boundary exactly once
         cntx[par * M + m] = cnt;
         if (par == 0) tx[m] = T;
     } else if (warp == 8 && lane == 0) {
         const uint32_t a_saddr = smem_u32(smem + OFF_A), e_saddr = smem_u32(smem + OFF_E),
-                       t_saddr = smem_u32(smem + OFF_T);
-        const uint32_t row_bytes = 16u * (uint32_t)nuc;
+                       t_saddr = smem_u32(smem + OFF_T), xp_saddr = smem_u32(smem + OFF_XP);
+        const uint32_t row_bytes = 16u * (uint32_t)WX;
         for (int j = 0; j < J; ++j) {
             const int s = j & 1, c = j < nch ? j : j - nch;
             if (j >= 2 && !mbar_wait(free0 + 8 * s, ((j - 2) >> 1) & 1, polls)) {
@@ -645,15 +684,14 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
             fence_after_sync();
             const uint32_t d = tbase + (uint32_t)(s * N);
             const uint32_t eb = e_saddr + 16u * (uint32_t)(c * N);
-            // last byte each operand's descriptors reach: E (8 patch rows of 256 candidates),
-            // the norm table (256 rows + the overlapping second chunk), A (10 K chunks)
-            const uint32_t e_end = eb + 7u * row_bytes + 255u * 16u + 15u;
-            const uint32_t t_end = t_saddr + 16u * (uint32_t)(c * N) + 256u * 16u + 15u;
-            const uint32_t a_end = a_saddr + 10u * A_KCHUNK - 1u;
+            const uint32_t tb = t_saddr + 16u * (uint32_t)(c * N);
+            // last byte each operand's descriptors reach: E (8 patch rows of N candidates),
+            // the norm table (N rows), the penalties (N rows), A (10 K chunks)
+            const uint32_t e_end = eb + 7u * row_bytes + (uint32_t)(N * 16 - 1);
+            const uint32_t t_end = tb + (uint32_t)(N * 16 - 1);
             if (!guard(a, tile_bad,
-                       e_end < e_saddr + (uint32_t)SZ_E && t_end < t_saddr + (uint32_t)SZ_T &&
-                           a_end < a_saddr + (uint32_t)SZ_A && (d >> 16) == 0u && (d & 0xffffu) + N <= 512u &&
-                           t_saddr + (uint32_t)SZ_T < (1u << 18),
+                       e_end < e_saddr + (uint32_t)SZ_E && t_end < t_saddr + (uint32_t)SZ_T && xp_saddr > tb &&
+                           xp_saddr - tb < (1u << 18) && (d >> 16) == 0u && (d & 0xffffu) + N <= 512u,
                        30, (int)(e_end - e_saddr), (int)(t_end - t_saddr), (int)d)) {
                 timeout = 1;
                 break;
@@ -662,11 +700,11 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
             for (int kk = 0; kk < KSTEPS - 1; ++kk)
                 mma_kind_f16(d, desc(a_saddr + 2 * kk * A_KCHUNK, A_KCHUNK, 128),
                              desc(eb + 2 * kk * row_bytes, row_bytes, 128), IDESC, kk);
-            // norm terms: one 16-byte table row per candidate; the K step's second 8-element
-            // chunk (A entries zero) reads the next candidate's row
-            mma_kind_f16(d, desc(a_saddr + 8 * A_KCHUNK, A_KCHUNK, 128),
-                         desc(t_saddr + 16u * (uint32_t)(c * N), 16, 128), IDESC, 1);
+            // norm terms (the chunk's table rows) and, as the K step's second 8-element
+            // chunk, the column penalties (the same 224-row table for every chunk)
+            mma_kind_f16(d, desc(a_saddr + 8 * A_KCHUNK, A_KCHUNK, 128), desc(tb, xp_saddr - tb, 128), IDESC, 1);
             mma_commit(done0 + 8 * s);
+            if (trace) trace[3 * j] = clock64();
             last = j;
         }
     }
@@ -720,9 +758,8 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
             for (int k = grp; k < c0n + c1n; k += 3) {
                 const int p = k < c0n ? 0 : 1, idx = (p * CAP + (p ? k - c0n : k)) * M + m;
                 const int f = lists[idx];
-                const int r = div_small((unsigned)f, inv), cc = f - r * nuc;
-                errs[idx] = guard(a, tile_bad, f < g.flat && (r + 7) * REG_COLS + cc + 7 < REG_ROWS * REG_COLS, 50,
-                                  f, r, cc)
+                const int r = f / WX, cc = f - r * WX;
+                errs[idx] = guard(a, tile_bad, r < g.nur && cc < nuc, 50, f, r, cc)
                                 ? exact_ssd2(nc, reg2 + r * REG_COLS + cc, REG_COLS)
                                 : 0.0f;
             }
@@ -749,7 +786,7 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
             for (int k = 0; k < c0n + c1n; ++k) {
                 const int p = k < c0n ? 0 : 1, idx = (p * CAP + (p ? k - c0n : k)) * M + tid;
                 const int f = lists[idx];
-                const int r = div_small((unsigned)f, inv), cc = f - r * nuc;
+                const int r = f / WX, cc = f - r * WX;
                 top8_insert_lex(e, q, errs[idx], pack_pos(g.ux0 + cc, g.uy0 + r));
             }
             bool in_plane = true;
@@ -795,15 +832,15 @@ cudaError_t launch_match_tc(const MatchArgs &a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-// Flat candidates per tile row of the debug dump (tile (0, 0)): nch * 256.
+// Flat candidates per block row of the debug dump (tile (0, 0)): chunks * 224.
 int tc_debug_cols(const MatchArgs &a) {
     const int R = a.range;
     const int nvx = a.nbx < tc::BX ? a.nbx : tc::BX, nvy = a.nby < tc::BY ? a.nby : tc::BY;
-    const int x1 = std::min(std::min(a.bs * (nvx - 1), a.w - 8) + R, a.w - 8);
+    (void)nvx;
     const int y1 = std::min(std::min(a.bs * (nvy - 1), a.h - 8) + R, a.h - 8);
-    const int nuc = x1 + 1, nur = y1 + 1;
-    const int flat = nur * nuc;
-    return (flat + tc::N - 1) / tc::N * tc::N;
+    const int nur = y1 + 1;
+    const int nch = (nur + tc::ROWS_PER_CHUNK - 1) / tc::ROWS_PER_CHUNK;
+    return nch * tc::N;
 }
 
 }  // namespace zb

@@ -28,10 +28,11 @@
 //     A 32-column group of a chunk spans at most two rows, so the window's rows
 //     are two compares per block and group.
 //  3. Pass 1 keeps, per block, the minimum of d over 16 groups of its window
-//     candidates (flat index mod 16).  The eighth smallest group minimum U comes
-//     from eight distinct window candidates, so the reference's eighth-best FP32
-//     error is at most U + |a - c0|^2 + eps, where eps bounds
-//     |d - (SSD_ref - |a - c0|^2)|.  Pass 2 recomputes the chunks and collects
+//     candidates by flat index mod 16, and over 16 groups by union row mod 16 (good
+//     matches along a vertical edge share few column residues but many rows).  The
+//     smaller of the two eighth smallest group minima, U, comes from eight distinct
+//     window candidates, so the reference's eighth-best FP32 error is at most
+//     U + |a - c0|^2 + eps, where eps bounds |d - (SSD_ref - |a - c0|^2)|.  Pass 2 recomputes the chunks and collects
 //     every window candidate with d <= U + 2 eps: a superset of the exact top 8,
 //     ties included.
 //  4. The collected candidates get the exact FP32 SSD in the reference's order
@@ -95,7 +96,8 @@ constexpr int SZ_REG = REG_ROWS * REG_COLS * 4;
 constexpr int SZ_LIST = 2 * CAP * M * 2;                     // [2][CAP][128] flat indices (16 bits)
 constexpr int OFF_GMX = OFF_BUF + SZ_LIST;                   // [16][128] odd-parity group minima at the pass boundary
 constexpr int SZ_BUF = SZ_REG > SZ_LIST + 16 * M * 4 ? SZ_REG : SZ_LIST + 16 * M * 4;
-constexpr int OFF_EPS = OFF_BUF + SZ_BUF;                    // [128] 2 eps
+constexpr int OFF_GMR = OFF_BUF + SZ_BUF;                    // [16][128] minima per union row mod 16 (pass 1)
+constexpr int OFF_EPS = OFF_GMR + 16 * M * 4;                // [128] 2 eps
 constexpr int OFF_TX = OFF_EPS + M * 4;                      // [128] collection bound U + 2 eps
 constexpr int OFF_CNT = OFF_TX + M * 4;                      // [2][128] collection counts
 constexpr int OFF_ROWMAX = OFF_CNT + 2 * M * 4;              // [MAX_UR] max |b - c0|^2 per union row
@@ -330,6 +332,7 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     float *hp = hs + REG_ROWS * MAX_UC;
     uint16_t *lists = reinterpret_cast<uint16_t *>(smem + OFF_BUF);   // [2][CAP][128]
     float *gmx = reinterpret_cast<float *>(smem + OFF_GMX);           // [16][128]
+    float *gmr = reinterpret_cast<float *>(smem + OFF_GMR);           // [16][128]
     float *eps2x = reinterpret_cast<float *>(smem + OFF_EPS);
     float *tx = reinterpret_cast<float *>(smem + OFF_TX);
     int *cntx = reinterpret_cast<int *>(smem + OFF_CNT);
@@ -538,6 +541,8 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
         for (int kc = 0; kc < 10; ++kc)
             *reinterpret_cast<uint4 *>(smem + OFF_A + kc * A_KCHUNK + (tid >> 3) * 128 + (tid & 7) * 16) = pa[kc];
         eps2x[tid] = 2.0f * eps;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) gmr[i * M + tid] = __int_as_float(0x7f800000);
     }
     fence_async_smem();
     fence_before_sync();
@@ -587,7 +592,10 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
             if (par == 0) {
 #pragma unroll
                 for (int i = 0; i < 16; ++i) gm[i] = fminf(gm[i], gmx[i * M + m]);
-                if (mvalid) T = eighth_smallest(gm) + eps2x[m];
+                float rw[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) rw[i] = gmr[i * M + m];
+                if (mvalid) T = fminf(eighth_smallest(gm), eighth_smallest(rw)) + eps2x[m];
                 tx[m] = T;
             }
             __syncwarp();
@@ -636,17 +644,35 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
 #pragma unroll
                         for (int r = 0; r < 32; ++r) o[r] = v[r];
                     }
-                    // group minima (flat index mod 16) over the block's window rows; out-of-window
-                    // columns carry the penalty
-                    if (ymask == 0xffffffffu) {
+                    // group minima over the block's window rows (out-of-window columns carry
+                    // the penalty): by flat index mod 16, and by union row mod 16 (this
+                    // parity's chunks own row residues 4 (k mod 4) .. + 3, so the two warps of
+                    // a pair never write the same slot)
+                    if (ymask) {
+                        if (ymask != 0xffffffffu) {
+#pragma unroll
+                            for (int r = 0; r < 32; ++r)
+                                if (!((ymask >> r) & 1u)) v[r] = __int_as_float(0x7f800000);
+                        }
 #pragma unroll
                         for (int r = 0; r < 16; ++r) gm[r] = min3(gm[r], v[r], v[r + 16]);
-                    } else if (ymask) {
+                        float b8[4];
 #pragma unroll
-                        for (int r = 0; r < 32; ++r)
-                            if (!((ymask >> r) & 1u)) v[r] = __int_as_float(0x7f800000);
-#pragma unroll
-                        for (int r = 0; r < 16; ++r) gm[r] = min3(gm[r], v[r], v[r + 16]);
+                        for (int k = 0; k < 4; ++k)
+                            b8[k] = min3(min3(v[8 * k], v[8 * k + 1], v[8 * k + 2]),
+                                         min3(v[8 * k + 3], v[8 * k + 4], v[8 * k + 5]), fminf(v[8 * k + 6], v[8 * k + 7]));
+                        // bnd is 8, 16, 24 or 32: the row ra owns the 8-element blocks below it
+                        const float sa = bnd <= 8 ? b8[0] : bnd <= 16 ? fminf(b8[0], b8[1])
+                                                    : bnd <= 24 ? min3(b8[0], b8[1], b8[2])
+                                                                : fminf(fminf(b8[0], b8[1]), fminf(b8[2], b8[3]));
+                        const float sb = bnd <= 8 ? min3(b8[1], b8[2], b8[3]) : bnd <= 16 ? fminf(b8[2], b8[3])
+                                                    : bnd <= 24 ? b8[3] : __int_as_float(0x7f800000);
+                        float *ga = gmr + (ra & 15) * M + m;
+                        *ga = fminf(*ga, sa);
+                        if (rb > ra) {
+                            float *gb = gmr + (rb & 15) * M + m;
+                            *gb = fminf(*gb, sb);
+                        }
                     }
                 } else if (ymask && min32(v) <= T) {
                     uint32_t hit = 0;

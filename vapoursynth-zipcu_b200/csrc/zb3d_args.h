@@ -31,7 +31,7 @@ struct MatchArgs {
     float *tc_dbg;         // optional: pass-1 distances of tile (0, 0), [128][tiles flat candidates]
     unsigned long long *tc_prof;  // optional: per tile [16]: clock64 phase marks [0..7], mbarrier
                                   // polls of the block and issuer warps [8], [10], TMEM load cycles
-                                  // and count [11], [13]; then for tile (1, 1) a per-job trace
+                                  // and count [11], [13], pass-1 / pass-2 / done-wait cycles [12], [14], [15]; then for tile (1, 1) a per-job trace
                                   // [job][3] (issued, completion seen, slot freed), at most 64 jobs
 };
 

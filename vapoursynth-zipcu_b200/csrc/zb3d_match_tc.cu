@@ -66,20 +66,22 @@ constexpr int BX = 8, BY = 16, M = BX * BY;  // reference blocks per tile
 constexpr int WX = 56;                       // flat row pitch: candidate columns per union row (nuc <= WX)
 constexpr int ROWS_PER_CHUNK = 4;
 constexpr int N = ROWS_PER_CHUNK * WX;       // candidates per MMA chunk = TMEM columns of one slot (224)
-constexpr int NGROUP = N / 32;               // 32-column TMEM loads per chunk
 constexpr int KSTEPS = 5;                    // patch rows (0,1) (2,3) (4,5) (6,7), then norms + column penalties
 constexpr int MAX_UC = WX, MAX_UR = 88;      // candidate union of a tile: columns, rows
 constexpr int REG_ROWS = MAX_UR + 7;
 constexpr int REG_COLS = 64;                 // staged FP32 region: columns (union + 7, padded)
 constexpr int E_ROWS = MAX_UR + ROWS_PER_CHUNK - 1 + 7;  // candidate rows of the last chunk + 7 patch rows
 constexpr int T_ROWS = MAX_UR + ROWS_PER_CHUNK - 1;
-constexpr int CAP = 32;                      // collected candidates per block and job parity
-constexpr int THREADS = 384;                 // warps 0-7: blocks (two per lane quarter: even / odd
-                                             // jobs), warp 8: TMEM owner and MMA issuer, 9-11: setup
+constexpr int NLIST = 4;                     // block warps per lane quarter: job parity (x chunk row half
+                                             // when 4); each keeps its own collection list
+constexpr int CAP = NLIST == 4 ? 16 : 32;    // collected candidates per block and list
+constexpr int MMA_WARP = 4 * NLIST;          // TMEM owner and MMA issuer (lane 0); the warps above it help
+                                             // in setup and the re-rank
+constexpr int THREADS = NLIST == 4 ? 544 : 384;
 constexpr int NWARPS = THREADS / 32;
 constexpr float BIG = 16384.0f;              // column-window penalty (exact in FP16)
 constexpr float RANGE = 4.0f;                // pixel magnitude the FP16 terms are sized for
-constexpr unsigned WAIT_LIMIT = 1u << 22;    // polls of an mbarrier before giving up (~0.5 s)
+constexpr unsigned WAIT_LIMIT = 1u << 16;    // suspended waits on an mbarrier before giving up
 
 // shared memory plan (bytes)
 constexpr int OFF_E = 0;                                     // expanded region, FP16 x 8 per position
@@ -93,14 +95,14 @@ constexpr int A_KCHUNK = M * 16;
 constexpr int SZ_A = 10 * A_KCHUNK;
 constexpr int OFF_BUF = OFF_A + SZ_A;                        // setup: FP32 region; stream: lists + group minima
 constexpr int SZ_REG = REG_ROWS * REG_COLS * 4;
-constexpr int SZ_LIST = 2 * CAP * M * 2;                     // [2][CAP][128] flat indices (16 bits)
-constexpr int OFF_GMX = OFF_BUF + SZ_LIST;                   // [16][128] odd-parity group minima at the pass boundary
+constexpr int SZ_LIST = NLIST * CAP * M * 2;                 // [4][CAP][128] flat indices (16 bits)
+constexpr int OFF_GMX = OFF_BUF + SZ_LIST;                   // [16][128] group minima (order-preserving keys)
 constexpr int SZ_BUF = SZ_REG > SZ_LIST + 16 * M * 4 ? SZ_REG : SZ_LIST + 16 * M * 4;
 constexpr int OFF_GMR = OFF_BUF + SZ_BUF;                    // [16][128] minima per union row mod 16 (pass 1)
 constexpr int OFF_EPS = OFF_GMR + 16 * M * 4;                // [128] 2 eps
 constexpr int OFF_TX = OFF_EPS + M * 4;                      // [128] collection bound U + 2 eps
-constexpr int OFF_CNT = OFF_TX + M * 4;                      // [2][128] collection counts
-constexpr int OFF_ROWMAX = OFF_CNT + 2 * M * 4;              // [MAX_UR] max |b - c0|^2 per union row
+constexpr int OFF_CNT = OFF_TX + M * 4;                      // [4][128] collection counts
+constexpr int OFF_ROWMAX = OFF_CNT + NLIST * M * 4;          // [MAX_UR] max |b - c0|^2 per union row
 constexpr int OFF_MISC = OFF_ROWMAX + MAX_UR * 4;            // mbarriers, TMEM address, flags, reductions
 constexpr int SMEM_BYTES = OFF_MISC + 96;
 static_assert(SMEM_BYTES <= 227 * 1024, "tensor-core matcher exceeds shared memory");
@@ -109,7 +111,8 @@ static_assert(OFF_T % 16 == 0 && OFF_XP % 16 == 0 && OFF_A % 128 == 0 && OFF_BUF
 static_assert(N % 16 == 0 && N <= 256 && 2 * N <= 512 && N % 32 == 0, "chunk shape");
 // during setup the E area holds the horizontal sums; during the re-rank the FP32 region
 // (E area) and the exact errors (T area)
-static_assert(2 * REG_ROWS * MAX_UC * 4 <= SZ_E && SZ_REG <= SZ_E && 2 * CAP * M * 4 <= SZ_T, "scratch reuse");
+static_assert(2 * REG_ROWS * MAX_UC * 4 <= SZ_E && SZ_REG <= SZ_E && NLIST * CAP * M * 4 <= SZ_T, "scratch reuse");
+static_assert(N == 4 * 56, "the row-half load table below assumes 4 rows of 56 candidates per chunk");
 
 // Shared-memory matrix descriptor, K-major without swizzle (layout type 0): start
 // address, LBO (distance of K-adjacent core matrices) and SBO (distance of 8-row
@@ -123,15 +126,16 @@ __device__ __forceinline__ uint64_t desc(uint32_t saddr, uint32_t lbo, uint32_t 
 // accumulator, both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
 constexpr uint32_t IDESC = (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 
-// Waits for phase `parity` of an mbarrier, at most WAIT_LIMIT polls; false on
-// timeout.  `polls` counts the unsuccessful polls.
+// Waits for phase `parity` of an mbarrier: try_wait suspends the thread until the
+// phase completes or a hardware time limit passes, so waiting warps take no issue
+// slots from the working ones.  At most WAIT_LIMIT such waits; false on timeout.
+// `polls` counts the waits that ran out.
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, unsigned &polls) {
     for (unsigned i = 0; i < WAIT_LIMIT; ++i) {
-        if (mbar_test(mbar, parity)) {
+        if (mbar_try(mbar, parity)) {
             polls += i;
             return true;
         }
-        if (i > 64) __nanosleep(64);
     }
     return false;
 }
@@ -204,12 +208,34 @@ __device__ __forceinline__ float exact_ssd2(const float2 (&nc)[8][4], const floa
     return ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
 }
 
-// three-operand minimum (sm_100)
-__device__ __forceinline__ float min3(float a, float b, float c) {
-    float r;
-    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
+// The same exact SSD with the reference patch c read from shared memory as well:
+// n + (-c) is computed as -(c - n) exactly, so the value is the one above.
+__device__ __forceinline__ float exact_ssd2_s(const float *c, const float *n, int pitch) {
+    float s[8];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        float2 d[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            d[i] = __fadd2_rn(make_float2(n[i * pitch + 2 * p], n[i * pitch + 2 * p + 1]),
+                              make_float2(-c[i * pitch + 2 * p], -c[i * pitch + 2 * p + 1]));
+        float2 e0 = __fmul2_rn(d[0], d[0]);
+        float2 e1 = __fmul2_rn(d[1], d[1]);
+        e0 = __ffma2_rn(d[2], d[2], e0);
+        e1 = __ffma2_rn(d[3], d[3], e1);
+        e0 = __ffma2_rn(d[4], d[4], e0);
+        e1 = __ffma2_rn(d[5], d[5], e1);
+        e0 = __ffma2_rn(d[6], d[6], e0);
+        e1 = __ffma2_rn(d[7], d[7], e1);
+        const float2 t = __fadd2_rn(e0, e1);
+        s[2 * p] = t.x;
+        s[2 * p + 1] = t.y;
+    }
+    return ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
 }
+
+// minimum of three (two two-operand minima: the three-operand PTX form costs more)
+__device__ __forceinline__ float min3(float a, float b, float c) { return fminf(fminf(a, b), c); }
 
 // minimum of 32 values, depth 4
 __device__ __forceinline__ float min32(const float (&v)[32]) {
@@ -245,6 +271,19 @@ __device__ __forceinline__ float eighth_smallest(const float (&g)[16]) {
 
 // Bits [0, b) set (b in 0..32).
 __device__ __forceinline__ uint32_t low_bits(int b) { return b >= 32 ? 0xffffffffu : ((1u << b) - 1u); }
+
+// Order-preserving integer key of a float (no NaN): a < b  <=>  key(a) < key(b), so that
+// shared-memory atomicMin can merge minima of any sign.
+__device__ __forceinline__ int fkey(float f) {
+    const int k = __float_as_int(f);
+    return k >= 0 ? k : k ^ 0x7fffffff;
+}
+__device__ __forceinline__ float fkey_inv(int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7fffffff); }
+
+// The TMEM loads of one chunk row half (chunk columns, width 32 or 16): rows 0-1 are
+// columns 0-111, rows 2-3 columns 112-223.  Half 0 loads columns 0, 32, 64 and 96 (16
+// wide), half 1 columns 112 (16 wide), 128, 160 and 192; a load's bits below bnd lie in
+// its first row, the rest in the next one (bnd = 24 at column 32, 8 at column 160).
 
 // (error, scan position) order: the reference's strict-less insertion over a
 // row-major scan keeps, among equal errors, the one scanned first
@@ -306,12 +345,13 @@ __device__ __forceinline__ void stage_region(float *reg, int cap, const float *p
     asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
-// One CTA per tile of 8 x 16 reference blocks.  Warps 0-7 own the blocks: warp w
-// reads TMEM lanes 32 (w mod 4) .. + 31 (block m = lane index) for the jobs of
-// parity w / 4, which use TMEM slot w / 4 (columns [224 s, 224 s + 224)).  Lane 0 of
-// warp 8 issues the MMAs.  The roles meet at mbarriers: done[s] (MMAs of the job
-// complete, tcgen05.commit) and free[s] (the slot read by the 4 warps of its
-// parity); job j waits for phase (j / 2) mod 2 of both.
+// One CTA per tile of 8 x 16 reference blocks.  The block warps (4 NLIST) own the
+// blocks: warp w reads TMEM lanes 32 (w mod 4) .. + 31 (block m = lane index), for the
+// jobs of parity (w / 4) mod 2, which use TMEM slot (w / 4) mod 2 (columns
+// [224 s, 224 s + 224)); with NLIST = 4 each takes one half of the chunk's rows.  Lane 0
+// of warp MMA_WARP issues the MMAs.  The roles meet at mbarriers: done[s] (MMAs of the
+// job complete, tcgen05.commit) and free[s] (the slot read by the block warps of its
+// parity); job j waits for phase (j / 2) mod 2.
 __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -346,14 +386,14 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
                                     ? a.tc_prof + 16 * (gridDim.x * gridDim.y) : nullptr;
     unsigned polls = 0;
     if (prof && tid == 0) prof[0] = clock64();
-    if (warp == 8) {
+    if (warp == MMA_WARP) {
         __syncwarp();  // tcgen05.alloc is .sync.aligned
         tmem_alloc(smem_u32(tslot), 512);
     }
     if (tid == 0) {
         for (int k = 0; k < 2; ++k) {
             mbar_init(done0 + 8 * k, 1);
-            mbar_init(free0 + 8 * k, 4);
+            mbar_init(free0 + 8 * k, 2 * NLIST);  // the block warps of the slot's job parity
         }
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         *oor = 0;
@@ -542,7 +582,10 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
             *reinterpret_cast<uint4 *>(smem + OFF_A + kc * A_KCHUNK + (tid >> 3) * 128 + (tid & 7) * 16) = pa[kc];
         eps2x[tid] = 2.0f * eps;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) gmr[i * M + tid] = __int_as_float(0x7f800000);
+        for (int i = 0; i < 16; ++i) {
+            gmr[i * M + tid] = __int_as_float(0x7f800000);
+            reinterpret_cast<int *>(gmx)[i * M + tid] = fkey(__int_as_float(0x7f800000));
+        }
     }
     fence_async_smem();
     fence_before_sync();
@@ -555,15 +598,18 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     // jobs j = 0 .. 2 nch - 1 are (pass j / nch, chunk j mod nch) on TMEM slot j mod 2
     const int nch = g.nch, J = 2 * nch;
     int timeout = 0, last = -1;
-    long long t_ld = 0;  // profiling: cycles in TMEM loads
+    long long t_ld = 0, t_p1 = 0, t_p2 = 0, t_wait = 0;  // profiling: cycles in TMEM loads, passes, waits
     int n_ld = 0;
     if (bad_tile) {
         // pixels beyond the FP16 sizing: every block of the tile goes to the FP32 scan
-    } else if (warp < 8) {
-        const int q = warp & 3, par = warp >> 2, m = 32 * q + lane;
+    } else if (warp < MMA_WARP) {
+        const int q = warp & 3, par = (warp >> 2) & 1, m = 32 * q + lane;
+        const int half0 = NLIST == 4 ? warp >> 3 : 0, nhalf = NLIST == 4 ? 1 : 2;  // chunk row halves
+        const int lid = NLIST == 4 ? 2 * par + half0 : par;  // this warp's collection list
         const int mbx = m & 7, mby = m >> 3;
         const bool mvalid = mbx < g.nvx && mby < g.nvy;
-        uint16_t *mylist = lists + par * CAP * M;
+        uint16_t *mylist = lists + lid * CAP * M;
+        int *gmk = reinterpret_cast<int *>(gmx);
         // the quarter's blocks need union rows [qr0, qr1]
         int qr0 = 1, qr1 = 0;
         const int by0 = 4 * q, nr = min(4, g.nvy - by0);
@@ -581,26 +627,25 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
         float T = -__int_as_float(0x7f800000);  // collection bound (stays -inf for idle lanes)
         int cnt = 0;
         bool have_t = false;
-        // pass boundary: the pair (warps q, q + 4) merges its minima and agrees on T
+        // pass boundary: the quarter's four warps merge their minima and agree on T
         auto exchange = [&]() {
-            if (par == 1) {
 #pragma unroll
-                for (int i = 0; i < 16; ++i) gmx[i * M + m] = gm[i];
-            }
+            for (int i = 0; i < 16; ++i) atomicMin(gmk + i * M + m, fkey(gm[i]));
             __syncwarp();
-            asm volatile("barrier.sync %0, 64;\n" ::"r"(1 + q) : "memory");
-            if (par == 0) {
+            asm volatile("barrier.sync %0, %1;\n" ::"r"(1 + q), "r"(32 * NLIST) : "memory");
+            if (lid == 0) {
+                float ge[16], rw[16];
 #pragma unroll
-                for (int i = 0; i < 16; ++i) gm[i] = fminf(gm[i], gmx[i * M + m]);
-                float rw[16];
-#pragma unroll
-                for (int i = 0; i < 16; ++i) rw[i] = gmr[i * M + m];
-                if (mvalid) T = fminf(eighth_smallest(gm), eighth_smallest(rw)) + eps2x[m];
+                for (int i = 0; i < 16; ++i) {
+                    ge[i] = fkey_inv(gmk[i * M + m]);
+                    rw[i] = gmr[i * M + m];
+                }
+                if (mvalid) T = fminf(eighth_smallest(ge), eighth_smallest(rw)) + eps2x[m];
                 tx[m] = T;
             }
             __syncwarp();
-            asm volatile("barrier.sync %0, 64;\n" ::"r"(1 + q) : "memory");
-            if (par == 1) T = tx[m];
+            asm volatile("barrier.sync %0, %1;\n" ::"r"(1 + q), "r"(32 * NLIST) : "memory");
+            if (lid != 0) T = tx[m];
             have_t = true;
         };
         const bool dbg = a.tc_dbg != nullptr && blockIdx.x == 0 && blockIdx.y == 0;
@@ -608,96 +653,125 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
         for (int j = par; j < J; j += 2) {
             const bool pass2 = j >= nch;
             if (pass2 && !have_t) exchange();
+            const long long tw0 = prof ? clock64() : 0;
             if (!mbar_wait(done0 + 8 * s, (j >> 1) & 1, polls)) {
                 timeout = 1;
                 break;
             }
+            if (prof) t_wait += clock64() - tw0;
             fence_after_sync();
-            if (trace && q == 0 && lane == 0) trace[3 * j + 1] = clock64();
+            if (trace && q == 0 && lid == 0 && lane == 0) trace[3 * j + 1] = clock64();
             const int ck = pass2 ? j - nch : j;
             const int row0 = ROWS_PER_CHUNK * ck;
             const uint32_t tl = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(s * N);
-            for (int gg = 0; gg < NGROUP; ++gg) {
-                // group gg: chunk columns 32 gg .. + 31, union rows ra (bits below bnd) and rb
-                const int ra = row0 + (32 * gg) / WX, rb = row0 + (32 * gg + 31) / WX;
+            for (int li = 0; li < 4 * nhalf; ++li) {
+                // load li of this warp's row halves: chunk columns col .. col + 31 (or + 15),
+                // union rows ra (bits below bnd) and rb
+                const int half = half0 + (li >> 2), l = li & 3;
+                // half 0: columns 0, 32, 64, 96 (16 wide); half 1: 112 (16 wide), 128, 160, 192
+                const int col = half == 0 ? 32 * l : (l == 0 ? 112 : 96 + 32 * l);
+                const bool narrow = col == 96 || col == 112;
+                const int ra = row0 + col / WX;
+                const int bnd = col + 32 > (ra - row0 + 1) * WX && !narrow ? (ra - row0 + 1) * WX - col : 32;
+                const int rb = bnd < 32 ? ra + 1 : ra;
                 if (rb < qr0 || ra > qr1) continue;  // no block of this quarter looks at these rows
-                const int bnd = rb > ra ? (rb - row0) * WX - 32 * gg : 32;
                 float v[32];
                 __syncwarp();  // tcgen05.ld is warp-collective: reconverge after the collection code
-                if (!guard(a, tile_bad, (tl >> 16) == (uint32_t)(32 * q) && (tl & 0xffffu) + 32u * gg + 32u <= 512u,
-                           40, gg, (int)tl, j)) {
+                if (!guard(a, tile_bad,
+                           (tl >> 16) == (uint32_t)(32 * q) && (tl & 0xffffu) + (uint32_t)col + (narrow ? 16u : 32u) <= 512u,
+                           40, col, (int)tl, j)) {
                     timeout = 1;
                     break;
                 }
                 const long long t0 = prof ? clock64() : 0;
-                tmem_ld32(tl + 32 * gg, v);
+                if (narrow) {
+                    tmem_ld16(tl + col, v);
+#pragma unroll
+                    for (int r = 16; r < 32; ++r) v[r] = __int_as_float(0x7f800000);
+                } else {
+                    tmem_ld32(tl + col, v);
+                }
                 if (prof) {
                     t_ld += clock64() - t0;
                     ++n_ld;
                 }
-                const int g0 = ck * N + 32 * gg;
+                const long long tp0 = prof ? clock64() : 0;
+                const int g0 = ck * N + col;
                 const bool ina = ra >= wr0 && ra <= wr1, inb = rb >= wr0 && rb <= wr1;
-                const uint32_t ymask = (ina ? low_bits(bnd) : 0u) | (inb ? ~low_bits(bnd) : 0u);
-                if (!pass2) {
-                    if (dbg && guard(a, tile_bad, g0 + 31 < nch * N, 41, g0, m, nch)) {
-                        float *o = a.tc_dbg + (size_t)m * (nch * N) + g0;
+                // the row boundary is a multiple of 8, so the window's rows select whole
+                // 8-element blocks: bit k of bsel = block k is in the window's rows
+                const int nba = bnd >> 3;  // blocks in row ra
+                const uint32_t bsel = ((ina ? (1u << nba) - 1u : 0u) | (inb ? (0xfu & ~((1u << nba) - 1u)) : 0u)) &
+                                      (narrow ? 0x3u : 0xfu);
+                if (!bsel) {
+                    // no window row of this block
+                } else {
+                    float b8[4];
 #pragma unroll
-                        for (int r = 0; r < 32; ++r) o[r] = v[r];
-                    }
-                    // group minima over the block's window rows (out-of-window columns carry
-                    // the penalty): by flat index mod 16, and by union row mod 16 (this
-                    // parity's chunks own row residues 4 (k mod 4) .. + 3, so the two warps of
-                    // a pair never write the same slot)
-                    if (ymask) {
-                        if (ymask != 0xffffffffu) {
+                    for (int k = 0; k < 4; ++k)
+                        b8[k] = min3(min3(v[8 * k], v[8 * k + 1], v[8 * k + 2]),
+                                     min3(v[8 * k + 3], v[8 * k + 4], v[8 * k + 5]), fminf(v[8 * k + 6], v[8 * k + 7]));
+                    const float inf = __int_as_float(0x7f800000);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (!((bsel >> k) & 1u)) b8[k] = inf;
+                    if (!pass2) {
+                        if (dbg && guard(a, tile_bad, g0 + (narrow ? 15 : 31) < nch * N, 41, g0, m, nch)) {
+                            float *o = a.tc_dbg + (size_t)m * (nch * N) + g0;
 #pragma unroll
                             for (int r = 0; r < 32; ++r)
-                                if (!((ymask >> r) & 1u)) v[r] = __int_as_float(0x7f800000);
+                                if (r < 16 || !narrow) o[r] = v[r];
+                        }
+                        // group minima over the block's window rows (out-of-window columns carry
+                        // the penalty): by flat index mod 16 (col is a multiple of 16), and by
+                        // union row mod 16 (this warp's chunks own row residues 4 (k mod 4) + its
+                        // row halves, so no two warps of a quarter write the same slot)
+                        if (bsel != (narrow ? 0x3u : 0xfu)) {
+#pragma unroll
+                            for (int r = 0; r < 32; ++r)
+                                if (!((bsel >> (r >> 3)) & 1u)) v[r] = inf;
                         }
 #pragma unroll
                         for (int r = 0; r < 16; ++r) gm[r] = min3(gm[r], v[r], v[r + 16]);
-                        float b8[4];
-#pragma unroll
-                        for (int k = 0; k < 4; ++k)
-                            b8[k] = min3(min3(v[8 * k], v[8 * k + 1], v[8 * k + 2]),
-                                         min3(v[8 * k + 3], v[8 * k + 4], v[8 * k + 5]), fminf(v[8 * k + 6], v[8 * k + 7]));
-                        // bnd is 8, 16, 24 or 32: the row ra owns the 8-element blocks below it
-                        const float sa = bnd <= 8 ? b8[0] : bnd <= 16 ? fminf(b8[0], b8[1])
-                                                    : bnd <= 24 ? min3(b8[0], b8[1], b8[2])
-                                                                : fminf(fminf(b8[0], b8[1]), fminf(b8[2], b8[3]));
-                        const float sb = bnd <= 8 ? min3(b8[1], b8[2], b8[3]) : bnd <= 16 ? fminf(b8[2], b8[3])
-                                                    : bnd <= 24 ? b8[3] : __int_as_float(0x7f800000);
+                        const float sa = nba == 1 ? b8[0] : nba == 3 ? min3(b8[0], b8[1], b8[2])
+                                                                      : fminf(fminf(b8[0], b8[1]), fminf(b8[2], b8[3]));
                         float *ga = gmr + (ra & 15) * M + m;
                         *ga = fminf(*ga, sa);
                         if (rb > ra) {
+                            const float sb = nba == 1 ? min3(b8[1], b8[2], b8[3]) : b8[3];
                             float *gb = gmr + (rb & 15) * M + m;
                             *gb = fminf(*gb, sb);
                         }
-                    }
-                } else if (ymask && min32(v) <= T) {
-                    uint32_t hit = 0;
+                    } else if (fminf(fminf(b8[0], b8[1]), fminf(b8[2], b8[3])) <= T) {
+                        // collect the window candidates at or below T, block by block
 #pragma unroll
-                    for (int r = 0; r < 32; ++r) hit |= (v[r] <= T ? 1u : 0u) << r;
-                    hit &= ymask;
-                    while (hit) {
-                        const int r = __ffs(hit) - 1;
-                        hit &= hit - 1;
-                        if (cnt < CAP && guard(a, tile_bad, g0 + r < g.flat, 42, g0 + r, cnt, g.flat))
-                            mylist[cnt * M + m] = (uint16_t)(g0 + r);
-                        ++cnt;
+                        for (int k = 0; k < 4; ++k) {
+                            if (!(b8[k] <= T)) continue;
+                            uint32_t hit = 0;
+#pragma unroll
+                            for (int r = 0; r < 8; ++r) hit |= (v[8 * k + r] <= T ? 1u : 0u) << r;
+                            while (hit) {
+                                const int r = 8 * k + __ffs(hit) - 1;
+                                hit &= hit - 1;
+                                if (cnt < CAP && guard(a, tile_bad, g0 + r < g.flat, 42, g0 + r, cnt, g.flat))
+                                    mylist[cnt * M + m] = (uint16_t)(g0 + r);
+                                ++cnt;
+                            }
+                        }
                     }
                 }
+                if (prof) (pass2 ? t_p2 : t_p1) += clock64() - tp0;
             }
             fence_before_sync();
             __syncwarp();
             if (lane == 0) mbar_arrive(free0 + 8 * s);
-            if (trace && q == 0 && lane == 0) trace[3 * j + 2] = clock64();
+            if (trace && q == 0 && lid == 0 && lane == 0) trace[3 * j + 2] = clock64();
             if (timeout) break;
         }
-        if (!have_t) exchange();  // both warps of a pair pass the boundary exactly once
-        cntx[par * M + m] = cnt;
-        if (par == 0) tx[m] = T;
-    } else if (warp == 8 && lane == 0) {
+        if (!have_t) exchange();  // every warp of a quarter passes the boundary exactly once
+        cntx[lid * M + m] = cnt;
+        if (lid == 0) tx[m] = T;
+    } else if (warp == MMA_WARP && lane == 0) {
         const uint32_t a_saddr = smem_u32(smem + OFF_A), e_saddr = smem_u32(smem + OFF_E),
                        t_saddr = smem_u32(smem + OFF_T), xp_saddr = smem_u32(smem + OFF_XP);
         const uint32_t row_bytes = 16u * (uint32_t)WX;
@@ -738,20 +812,23 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     if (prof) {
         const unsigned wp = __reduce_add_sync(0xffffffffu, polls);
         if (lane == 0) {
-            atomicAdd(prof + (warp < 8 ? 8 : 10), (unsigned long long)wp);
-            if (warp < 8) {
+            atomicAdd(prof + (warp < MMA_WARP ? 8 : 10), (unsigned long long)wp);
+            if (warp < MMA_WARP) {
                 atomicAdd(prof + 11, (unsigned long long)t_ld);
+                atomicAdd(prof + 12, (unsigned long long)t_p1);
                 atomicAdd(prof + 13, (unsigned long long)n_ld);
+                atomicAdd(prof + 14, (unsigned long long)t_p2);
+                atomicAdd(prof + 15, (unsigned long long)t_wait);
             }
         }
     }
     // ---- drain and release tensor memory -------------------------------------------
-    if (stop && warp == 8 && lane == 0 && last >= 0)
+    if (stop && warp == MMA_WARP && lane == 0 && last >= 0)
         mbar_wait(done0 + 8 * (last & 1), (last >> 1) & 1, polls);
     if (stop && tid == 0) a.tc_ws[1] = 1;
     fence_before_sync();
     __syncthreads();
-    if (warp == 8) {
+    if (warp == MMA_WARP) {
         // lane 0 of this warp ran the MMA loop alone: tcgen05.dealloc is .sync.aligned, so
         // the warp must be converged before it
         __syncwarp();
@@ -761,42 +838,45 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     if (prof && tid == 0) prof[5] = clock64();
 
     // ---- exact re-rank of the collected candidates from the FP32 region ------------
-    // Three threads per block compute the exact errors of its collected candidates
-    // (entries k = grp, grp + 3, ... of [even-job list, odd-job list]); then the
-    // block's thread keeps the eight smallest by (error, scan position).
+    // RR threads per block compute the exact errors of its collected candidates
+    // (entries grp, grp + RR, ... of each of its lists); then the block's thread keeps
+    // the eight smallest by (error, scan position).
     const bool skip_tile = stop || bad_tile;
     float *reg2 = reinterpret_cast<float *>(smem + OFF_E);  // the FP32 region again
     float *errs = reinterpret_cast<float *>(smem + OFF_T);  // [2][CAP][128]
     if (!skip_tile) stage_region(reg2, SZ_E / 4, plane, P, g, tid, a, tile_bad);
     __syncthreads();
-    if (!skip_tile && tid < 3 * M) {
+    constexpr int RR = THREADS / M;  // threads per block in the exact re-rank
+    if (!skip_tile && tid < RR * M) {
         const int m = tid & 127, grp = tid >> 7;
         const int mbx = m & 7, mby = m >> 3;
-        const int c0n = cntx[m], c1n = cntx[M + m];
-        if (mbx < g.nvx && mby < g.nvy && c0n <= CAP && c1n <= CAP && tx[m] < __int_as_float(0x7f800000)) {
-            const int moff = (block_y(a, g.ky0 + mby) - g.uy0) * REG_COLS + (block_x(a, g.kx0 + mbx) - g.ux0);
-            float2 nc[8][4];
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-#pragma unroll
-                for (int p = 0; p < 4; ++p)
-                    nc[i][p] = make_float2(-reg2[moff + i * REG_COLS + 2 * p], -reg2[moff + i * REG_COLS + 2 * p + 1]);
-            for (int k = grp; k < c0n + c1n; k += 3) {
-                const int p = k < c0n ? 0 : 1, idx = (p * CAP + (p ? k - c0n : k)) * M + m;
-                const int f = lists[idx];
-                const int r = f / WX, cc = f - r * WX;
-                errs[idx] = guard(a, tile_bad, r < g.nur && cc < nuc, 50, f, r, cc)
-                                ? exact_ssd2(nc, reg2 + r * REG_COLS + cc, REG_COLS)
-                                : 0.0f;
+        const int cn0 = cntx[m], cn1 = cntx[M + m];
+        const int cn2 = NLIST == 4 ? cntx[2 * M + m] : 0, cn3 = NLIST == 4 ? cntx[3 * M + m] : 0;
+        const bool over = cn0 > CAP || cn1 > CAP || cn2 > CAP || cn3 > CAP;
+        if (mbx < g.nvx && mby < g.nvy && !over && tx[m] < __int_as_float(0x7f800000)) {
+            const float *ref = reg2 + (block_y(a, g.ky0 + mby) - g.uy0) * REG_COLS + (block_x(a, g.kx0 + mbx) - g.ux0);
+            // thread grp of the block takes the entries grp, grp + RR, ... of each list
+            for (int li = 0; li < NLIST; ++li) {
+                const int n = li == 0 ? cn0 : li == 1 ? cn1 : li == 2 ? cn2 : cn3;
+                for (int k = grp; k < n; k += RR) {
+                    const int idx = (li * CAP + k) * M + m;
+                    const int f = lists[idx];
+                    const int r = f / WX, cc = f - r * WX;
+                    errs[idx] = guard(a, tile_bad, r < g.nur && cc < nuc, 50, f, r, cc)
+                                    ? exact_ssd2_s(ref, reg2 + r * REG_COLS + cc, REG_COLS)
+                                    : 0.0f;
+                }
             }
         }
     }
     __syncthreads();
     if (prof && tid == 0) prof[6] = clock64();
     if (tid >= M) return;
-    const int c0n = cntx[tid], c1n = cntx[M + tid];
-    const bool fb = valid && (skip_tile || *tile_bad || c0n > CAP || c1n > CAP ||
-                              !(tx[tid] < __int_as_float(0x7f800000)));
+    const int cn0 = cntx[tid], cn1 = cntx[M + tid];
+    const int cn2 = NLIST == 4 ? cntx[2 * M + tid] : 0, cn3 = NLIST == 4 ? cntx[3 * M + tid] : 0;
+    const bool over = cn0 > CAP || cn1 > CAP || cn2 > CAP || cn3 > CAP;
+    const int total = cn0 + cn1 + cn2 + cn3;
+    const bool fb = valid && (skip_tile || *tile_bad || over || !(tx[tid] < __int_as_float(0x7f800000)));
     if (valid) {
         const int bi = (g.ky0 + byl) * a.nbx + (g.kx0 + bxl);
         if (fb) {
@@ -809,16 +889,19 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
                 e[i] = ZB_FLT_MAX;
                 q[i] = 0x7fffffff;
             }
-            for (int k = 0; k < c0n + c1n; ++k) {
-                const int p = k < c0n ? 0 : 1, idx = (p * CAP + (p ? k - c0n : k)) * M + tid;
-                const int f = lists[idx];
-                const int r = f / WX, cc = f - r * WX;
-                top8_insert_lex(e, q, errs[idx], pack_pos(g.ux0 + cc, g.uy0 + r));
+            for (int li = 0; li < NLIST; ++li) {
+                const int n = li == 0 ? cn0 : li == 1 ? cn1 : li == 2 ? cn2 : cn3;
+                for (int kk = 0; kk < n; ++kk) {
+                    const int idx = (li * CAP + kk) * M + tid;
+                    const int f = lists[idx];
+                    const int r = f / WX, cc = f - r * WX;
+                    top8_insert_lex(e, q, errs[idx], pack_pos(g.ux0 + cc, g.uy0 + r));
+                }
             }
             bool in_plane = true;
 #pragma unroll
             for (int i = 0; i < 8; ++i) in_plane = in_plane && pos_x(q[i]) <= W - 8 && pos_y(q[i]) <= H - 8;
-            if (guard(a, tile_bad, in_plane, 60, bi, q[7], c0n + c1n))
+            if (guard(a, tile_bad, in_plane, 60, bi, q[7], total))
                 store_list(a, bi, xb, yb, e, q);
             else
                 list_fallback(a, bi);
@@ -828,7 +911,7 @@ __global__ void __launch_bounds__(THREADS, 1) zb_match_tc(MatchArgs a) {
     if (a.tc_stats) {
         const unsigned nval = __popc(__ballot_sync(0xffffffffu, valid));
         const unsigned nfb = __popc(__ballot_sync(0xffffffffu, fb));
-        const unsigned ns = __reduce_add_sync(0xffffffffu, valid && !fb ? (unsigned)(c0n + c1n) : 0u);
+        const unsigned ns = __reduce_add_sync(0xffffffffu, valid && !fb ? (unsigned)total : 0u);
         if (lane == 0) {
             atomicAdd(a.tc_stats + 1, (unsigned long long)nval);
             atomicAdd(a.tc_stats + 2, (unsigned long long)ns);

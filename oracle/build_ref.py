@@ -10,8 +10,9 @@ options (vszipcu src/bm3d.zig:20-31, cudaz/src/nvrtc.zig:137-211):
 
 For the match-index pins a second variant stores the final match list of each
 reference block: a copy of ``bm3d.cu`` written into ``oracle/_ref/gen/`` (never
-into the reference tree) gets a ``__device__`` dump pointer and one store block
-inserted right after the self-inclusion step (src/bm3d.cu:788).
+into the reference tree) gets ``__device__`` dump pointers (indices, and optionally
+the list's distances) and one store block inserted right after the self-inclusion
+step (src/bm3d.cu:788).
 
 Outputs go only to ``oracle/_ref/`` (git-ignored; it travels with the tree to the
 GPU machine, where the reference sources do not exist).
@@ -32,15 +33,17 @@ REF_ROOT = os.environ.get("ZB3D_REFERENCE_ROOT", "")
 OUT = os.path.join(HERE, "_ref")
 GEN = os.path.join(OUT, "gen")
 
-_DUMP_DECL = "\n#ifdef ZB_REF_DUMP\n__device__ int *zb_ref_dump;\n#endif\n"
+_DUMP_DECL = "\n#ifdef ZB_REF_DUMP\n__device__ int *zb_ref_dump;\n__device__ float *zb_ref_dump_err;\n#endif\n"
 _DUMP_STORE = """
 #ifdef ZB_REF_DUMP
     {
         const int zb_bx = 4 * gid + lane_id / 8;
-        int *zb_p = zb_ref_dump + (((long long)blockIdx.y * ZB_REF_NBX + zb_bx) * 8 + sub_lane_id) * 3;
+        const long long zb_slot = ((long long)blockIdx.y * ZB_REF_NBX + zb_bx) * 8 + sub_lane_id;
+        int *zb_p = zb_ref_dump + zb_slot * 3;
         zb_p[0] = index8_x;
         zb_p[1] = index8_y;
         zb_p[2] = index8_z;
+        if (zb_ref_dump_err) zb_ref_dump_err[zb_slot] = errors8;
     }
 #endif
 """

@@ -164,6 +164,9 @@ def parity_specs():
                             sigma=(8.0, 6.0, 6.0)))
     specs.append(_small(w=48, h=40, stride=48, chroma=1, proc_mask=5, sigma=(8.0, 0.0, 6.0)))
     specs.append(_small(w=48, h=40, stride=48, chroma=1, proc_mask=7, radius=1, sigma=(8.0, 6.0, 6.0)))
+    # ssd/norm on more blocks: approximate square root and reciprocal in both kernels
+    specs.append(_small(w=256, h=192, stride=256, block_step=4, bm_range=12, bm_error="ssd_norm", sigma=(10.0,) * 3))
+    specs.append(_small(w=200, h=150, stride=224, block_step=8, bm_range=9, bm_error="ssd_norm", final=1))
     return specs
 
 

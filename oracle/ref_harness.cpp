@@ -96,6 +96,18 @@ int refh_set_dump(void *h, unsigned long long dptr, char *err, int errlen) {
     return 0;
 }
 
+// Sets the distance dump pointer of a dump-variant module (float[nby][nbx][8]; 0 = off).
+int refh_set_dump_err(void *h, unsigned long long dptr, char *err, int errlen) {
+    RefModule *m = (RefModule *)h;
+    CUdeviceptr sym;
+    size_t bytes;
+    CUresult r = cuModuleGetGlobal(&sym, &bytes, m->mod, "zb_ref_dump_err");
+    if (r != CUDA_SUCCESS) return fail(err, errlen, "zb_ref_dump_err symbol", r);
+    r = cuMemcpyHtoD(sym, &dptr, sizeof dptr);
+    if (r != CUDA_SUCCESS) return fail(err, errlen, "set distance dump pointer", r);
+    return 0;
+}
+
 // memset(res) + bm3d (+ aggregate when dst != 0) on `stream`.
 int refh_bm3d(void *h, unsigned long long res, unsigned long long src, unsigned long long dst, size_t res_bytes,
               int w, int hgt, int block_step, int warps, int agg_planes, unsigned long long stream, char *err,

@@ -32,6 +32,7 @@ def lib():
         _lib.refh_load.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
         _lib.refh_unload.argtypes = [ctypes.c_void_p]
         _lib.refh_set_dump.argtypes = [ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_char_p, ctypes.c_int]
+        _lib.refh_set_dump_err.argtypes = [ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_char_p, ctypes.c_int]
         _lib.refh_bm3d.argtypes = [ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_ulonglong,
                                    ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_int, ctypes.c_ulonglong, ctypes.c_char_p, ctypes.c_int]
@@ -75,6 +76,12 @@ class RefKernel:
     def set_dump(self, dptr: int):
         err = ctypes.create_string_buffer(512)
         if lib().refh_set_dump(self.h, dptr, err, 512):
+            raise RuntimeError(err.value.decode())
+
+    def set_dump_err(self, dptr: int):
+        """Also store each list slot's distance (float[nby][nbx][8]); 0 turns it off."""
+        err = ctypes.create_string_buffer(512)
+        if lib().refh_set_dump_err(self.h, dptr, err, 512):
             raise RuntimeError(err.value.decode())
 
     def run(self, res_ptr: int, src_ptr: int, dst_ptr: int, res_bytes: int, stream: int = 0):

@@ -152,8 +152,13 @@ __device__ __forceinline__ float half_distance(const float (&c)[8][4], const flo
         float hx = (x[0] + x[1]) + (x[2] + x[3]);
         float nn = sqrtf(hq + __shfl_xor_sync(pm, hq, 1));
         float dot = hx + __shfl_xor_sync(pm, hx, 1);
-        // full distance; the caller's half join is skipped for this metric
-        return 2.0f - 2.0f * dot / __fmaf_rn(st, nn, ZB_FLT_EPS);
+        // full distance; the caller's half join is skipped for this metric.  The
+        // reference's 2 - 2 dot / (|a| |b| + eps) under fast math is the approximate
+        // reciprocal of the denominator with the subtraction fused into it; written out
+        // so that no kernel's instruction selection can round it differently
+        float r;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(__fmaf_rn(st, nn, ZB_FLT_EPS)));
+        return __fmaf_rn(-2.0f * dot, r, 2.0f);
     }
     return (s[0] + s[1]) + (s[2] + s[3]);
 }

@@ -345,15 +345,20 @@ def run_pilot_form(torch, frames, clip: int, steps: int, warmup: int, psnr_frame
                     "frames" % (net.layers, net.width, nstreams, min(psnr_frames, nf))}
 
 
-def run_e2e(frames, steps: int, warmup: int, num_streams: int = 4):
-    """Same job through the public API on host frames (zb3d.BM3Dv2)."""
+def run_e2e(frames, steps: int, warmup: int, num_streams: int = 4, pinned: bool = True, pilot=None):
+    """Same job through the public API on host frames (zb3d.BM3Dv2): page-locked frames (the
+    library DMAs them) or pageable ones (copied through its pinned staging).  With `pilot`
+    (a zb3d.Pilot) the two steps are one filter, BM3Dv2(clip, pilot=...)."""
     import zb3d
     from zb3d import _native as N
     nfr = BATCH * (steps + warmup)
     host = [frames[i % len(frames)] for i in range(nfr)]
-    clip = zb3d.Clip.from_frames(host, family=N.YUV, subsampling=(1, 1), pinned=True)
-    basic = zb3d.BM3Dv2(clip, num_streams=num_streams, **KW)
-    final = zb3d.BM3Dv2(clip, ref=basic, num_streams=num_streams, **KW)
+    clip = zb3d.Clip.from_frames(host, family=N.YUV, subsampling=(1, 1), pinned=pinned)
+    if pilot is not None:
+        final = zb3d.BM3Dv2(clip, pilot=pilot, num_streams=num_streams, **KW)
+    else:
+        basic = zb3d.BM3Dv2(clip, num_streams=num_streams, **KW)
+        final = zb3d.BM3Dv2(clip, ref=basic, num_streams=num_streams, **KW)
     # two request threads per stream keep every stream fed while the other thread of the
     # pair waits for its frame; frames are requested continuously (no drain between steps)
     # and each output is dropped once read, so the page-locked output pool stays small
@@ -369,9 +374,10 @@ def run_e2e(frames, steps: int, warmup: int, num_streams: int = 4):
     dt = time.perf_counter() - t0
     pool.shutdown()
     # bytes per step: pass 1 uploads the clip, pass 2 the ref and the clip; both download their output
-    px = sum(((w + 31) // 32 * 32) * h for w, h in plane_dims())
-    h2d = 3 * px * 4 * BATCH
-    d2h = 2 * px * 4 * BATCH
+    # (the pilot form uploads the clip once and downloads its output once)
+    px = sum(w * h for w, h in plane_dims())
+    h2d = (1 if pilot is not None else 3) * px * 4 * BATCH
+    d2h = (1 if pilot is not None else 2) * px * 4 * BATCH
     return dt, h2d, d2h
 
 
@@ -1022,6 +1028,12 @@ def main():
                       "how": "zb3d.BM3Dv2 twice (basic, then ref=basic) on host frames in page-locked memory "
                              "(the library DMAs them; outputs land in pooled page-locked frames), 4 streams, "
                              "8 request threads, frames requested continuously, wall clock"}
+        dt, h2d, d2h = run_e2e(frames, args.steps, args.warmup, pinned=False)
+        out["e2e"]["pageable"] = {
+            "value": W * H * args.steps * BATCH * world / dt / 1e6, "unit": "Mpix/s",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "how": "the same two filters on pageable host frames (as VapourSynth frames are): the library "
+                   "copies them through its page-locked staging buffers"}
     if rank == 0 and not args.no_pilot:
         if pipe is not None:
             pipe.close()
@@ -1029,6 +1041,19 @@ def main():
         # timed over the same K steps as the plain form (8 frames each)
         out["pilot_form"] = run_pilot_form(torch, frames, rank, args.steps, 1, nstreams=args.streams,
                                            weights=args.pilot_weights, conv_ctas_per_sm=args.pilot_conv_ctas)
+        if not args.no_e2e and args.pilot_weights is None:
+            # the pilot form through the C ABI (zb3d_args.pilot, shipped file and gate) on host frames
+            import zb3d
+            torch.cuda.empty_cache()
+            pl = zb3d.Pilot()
+            dt, h2d, d2h = run_e2e(frames, args.steps, args.warmup, pilot=pl)
+            out["pilot_form"]["e2e"] = {
+                "value": W * H * args.steps * BATCH / dt / 1e6, "unit": "Mpix/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "pilot_used_per_plane": [pl.accepts(SIGMA, w, h) for w, h in plane_dims()],
+                "how": "zb3d.BM3Dv2(clip, pilot=zb3d.Pilot()) on host frames in page-locked memory: one filter "
+                       "runs the pilot (its gate accepting sigma) and step 2 per frame, 4 streams, 8 request "
+                       "threads, wall clock"}
         if args.pilot_weights is None:
             # the 48-channel, 10-layer net of the learned-pilot configuration, on the same frames
             from zb3d import pilot as P
@@ -1058,6 +1083,8 @@ def main():
             vs = {"ref_cuda_mpix_s": rv, "ref_cuda_streams": max(by_ns), "plain_x": value / world / rv}
             if "pilot_form" in out and out["pilot_form"].get("value"):
                 vs["pilot_x"] = out["pilot_form"]["value"] / rv
+                if out["pilot_form"].get("e2e"):
+                    vs["pilot_e2e_pinned_x"] = out["pilot_form"]["e2e"]["value"] / rv
             if "e2e" in out:
                 vs["e2e_pinned_x"] = out["e2e"]["value"] / world / rv
                 if out["e2e"].get("pageable"):

@@ -67,6 +67,15 @@ typedef struct zb3d_args {
      * with bm_range <= 13, for example); not given = the autotuner picks per plane
      * (zb3d_entry_tuning).  Every form gives the same lists. */
     int match_form;
+    /* Not in the reference.  A learned pilot network (zb3d_pilot_load) that makes
+     * BM3Dv2's step-1 estimate: the filter then runs both steps in one call, the pilot
+     * (or, for a plane entry whose sigma the pilot's gate refuses, the plain step 1: hard
+     * threshold with the step-1 sigma factor) into the reference slot, then step 2
+     * (Wiener) matching on it, and returns step 2.  This is the two-pass
+     * BM3Dv2(clip, ref=BM3Dv2(clip)) of the reference (src/bm3d.zig:995-1011) with
+     * step 1 replaced.  BM3Dv2 only, no "ref" clip, radius 0, the pilot on device_id;
+     * the filter does not own the pilot, which must outlive it.  NULL = off. */
+    const struct zb3d_pilot *pilot;
 } zb3d_args;
 
 /* Fills `a` with "nothing given" (all defaults). */
@@ -332,6 +341,41 @@ int zb3d_pilot_adam(float *w, float *m, float *v, const float *g, long long coun
 /* wt[ci][8 - tap][co] = w[co][tap][ci]: weights of the backward pass to a layer's input. */
 int zb3d_pilot_flip_weights(const void *w, int cin, int cout, void *wt, void *stream);
 int zb3d_pilot_to_bf16(const float *a, long long count, void *b, void *stream);
+
+/* ---- the pilot network as one object (not in the reference) ----------------------
+ *
+ * Weights file "ZB3DPLT1": header (architecture, noise-level input scale, the gate
+ * table), FP32 weights and biases of each layer, CRC-32 of the whole; written by
+ * zb3d.pilot.save_weights.  The gate table lists, per calibrated noise level (8-bit
+ * scale) and plane size, the mean two-pass PSNR difference (pilot minus plain step 1)
+ * measured on held-out synthetic planes of that size; the pilot is accepted for a plane
+ * when the level of the nearest calibrated size (by area) nearest to its sigma has a
+ * difference >= -tol (tol = 0.05 dB in the shipped files). */
+typedef struct zb3d_pilot zb3d_pilot;
+/* Loads a weights file (or the same bytes from memory) onto device_id.  Returns NULL
+ * and writes a reason into err when the file is missing, damaged (checksum), of another
+ * version or architecture, or the device has no room. */
+zb3d_pilot *zb3d_pilot_load(const char *path, int device_id, char *err, size_t errlen);
+zb3d_pilot *zb3d_pilot_from_memory(const void *data, size_t bytes, int device_id, char *err, size_t errlen);
+void zb3d_pilot_free(zb3d_pilot *p);
+/* Hidden channels, layer count and gate levels of the network. */
+void zb3d_pilot_describe(const zb3d_pilot *p, int *width, int *layers, int *gate_levels);
+/* Gate level i: its noise level, plane size and measured two-pass difference in dB.
+ * 0, or -1 out of range. */
+int zb3d_pilot_gate_level(const zb3d_pilot *p, int i, float *sigma, int *width, int *height, float *delta_db);
+/* 1 if the gate accepts the pilot for a width x height plane at this noise level (8-bit
+ * scale), else 0. */
+int zb3d_pilot_accepts(const zb3d_pilot *p, float sigma, int width, int height);
+/* Device workspace zb3d_pilot_run needs for a width x height plane (bytes). */
+size_t zb3d_pilot_workspace_bytes(const zb3d_pilot *p, int width, int height);
+/* The pilot estimate of one FP32 plane: d_out = d_noisy + net(d_noisy, sigma), rows
+ * pitch / out_pitch floats apart (0: width).  d_workspace: zb3d_pilot_workspace_bytes,
+ * 256-byte aligned, not shared with a concurrent call.  d_status (device int, may be
+ * NULL) becomes non-zero if a convolution pipeline wait timed out.  Asynchronous on
+ * stream (a cudaStream_t or NULL); call with the pilot's device current.  Returns 0, or -1
+ * for bad arguments or a launch error. */
+int zb3d_pilot_run(const zb3d_pilot *p, const float *d_noisy, int width, int height, int pitch, float sigma,
+                   float *d_out, int out_pitch, void *d_workspace, int *d_status, void *stream);
 
 /* Library version string. */
 const char *zb3d_version(void);

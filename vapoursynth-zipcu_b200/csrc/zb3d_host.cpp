@@ -35,6 +35,7 @@ bool tc_eligible(const MatchArgs &a);
 cudaError_t launch_match_tc(const MatchArgs &a, cudaStream_t st);
 cudaError_t launch_tc_fallback(MatchArgs a, cudaStream_t st);
 int tc_debug_cols(const MatchArgs &a);
+int pilot_device(const zb3d_pilot *p);
 size_t match_tile_bytes(const MatchArgs &a, int rows_per_cta);
 cudaError_t launch_filter(const FilterArgs &a, bool final_, int t2d, int t1d, cudaStream_t st);
 cudaError_t launch_finish(const unsigned long long *num, const unsigned long long *den, long long acc_plane_stride,
@@ -225,7 +226,10 @@ struct Entry {
     int w, h, pitch;
     int nplanes;
     int planes[3];
-    float sigma[3];  // scaled
+    float sigma[3];        // scaled (the filter's step)
+    float sigma_basic[3];  // scaled with the step-1 factor (the plain step 1 of the pilot form)
+    float sigma_raw[3];    // as given (8-bit scale)
+    bool pilot_step1 = false;  // pilot form: the pilot makes this entry's step 1 (else the plain step 1)
     int bs, range, ps_num, ps_range;
     unsigned proc_mask;
     int metric, t2d, t1d;
@@ -252,6 +256,9 @@ struct Slot {
     unsigned long long *tc_stats = nullptr;  // tensor-core form: counters
     float *h_stage = nullptr;
     size_t stage_up = 0, stage_down = 0;
+    void *pilot_ws = nullptr;         // pilot form: the network's activations
+    int *pilot_status = nullptr;      // pilot form: convolution pipeline status (device)
+    int *h_pilot_status = nullptr;    // its page-locked read-back
 
     void destroy() {
         if (st) cudaStreamDestroy(st);
@@ -265,7 +272,10 @@ struct Slot {
         cudaFree(errs);
         cudaFree(tc_ws);
         cudaFree(tc_stats);
+        cudaFree(pilot_ws);
+        cudaFree(pilot_status);
         if (h_stage) cudaFreeHost(h_stage);
+        if (h_pilot_status) cudaFreeHost(h_pilot_status);
         *this = Slot();
     }
 };
@@ -277,6 +287,8 @@ struct Filter {
     bool v2 = false, passthrough = false;
     bool final_ = false, chroma = false, fused = false, zero_init = true;
     int match_form = -1;           // -1: chosen per entry by the autotuner; 0 / 1: forced
+    const zb3d_pilot *pilot = nullptr;  // pilot form (BM3Dv2 two-pass in one call), not owned
+    size_t pilot_ws_bytes = 0;
     int radius = 0, tw = 1;
     int nclips = 1;
     float extractor = 0.0f;
@@ -349,6 +361,13 @@ bool alloc_slot(Filter *f, Slot &s) {
         if (!ok(cudaMalloc(&s.tc_ws, (kTcWsList + f->max_blocks) * sizeof(int)))) return false;
         if (!ok(cudaMalloc(&s.tc_stats, 4 * sizeof(unsigned long long)))) return false;
         if (!ok(cudaMemset(s.tc_stats, 0, 4 * sizeof(unsigned long long)))) return false;
+    }
+    if (f->pilot) {
+        if (f->pilot_ws_bytes && !ok(cudaMalloc(&s.pilot_ws, f->pilot_ws_bytes))) return false;
+        if (!ok(cudaMalloc(&s.pilot_status, sizeof(int)))) return false;
+        if (!ok(cudaMemset(s.pilot_status, 0, sizeof(int)))) return false;
+        if (!ok(cudaHostAlloc((void **)&s.h_pilot_status, sizeof(int), cudaHostAllocDefault))) return false;
+        *s.h_pilot_status = 0;
     }
     s.stage_up = f->v2 && f->radius > 0 ? f->frame_elems : src;
     s.stage_down = dst;
@@ -556,7 +575,8 @@ cudaEvent_t prof_event(Filter *f, std::vector<cudaEvent_t> &v, cudaStream_t st) 
 }
 
 // Runs every entry of one window (d_src, entry layout) into d_dst on the slot's stream.
-cudaError_t run_entry(Filter *f, Slot &s, const Entry &en, const float *src, float *dst);
+cudaError_t run_entry(Filter *f, Slot &s, const Entry &en, const float *src, float *dst, bool basic = false);
+cudaError_t run_entry_steps(Filter *f, Slot &s, const Entry &en, const float *src, float *dst);
 
 // Runs `fn(s)` (launches on s.st) as a CUDA graph: captured once per key on the slot's
 // own stream, then replayed on `launch`.  A window's whole launch sequence (memsets,
@@ -611,14 +631,40 @@ cudaError_t run_graphed(Filter *f, Slot &s, std::tuple<const void *, const void 
 
 cudaError_t run_window(Filter *f, Slot &s, const float *d_src, float *d_dst) {
     for (const Entry &en : f->entries) {
-        cudaError_t e = run_entry(f, s, en, d_src + en.src_off, d_dst + en.dst_off);
+        cudaError_t e = run_entry_steps(f, s, en, d_src + en.src_off, d_dst + en.dst_off);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
 
+// One entry with, in the pilot form, its step 1 first: the pilot (or the plain step 1
+// where the gate refused the entry's sigma) writes the reference planes (clip 0 of the
+// entry's block) from the noisy planes (clip 1); then step 2 runs as with a ref clip.
+cudaError_t run_entry_steps(Filter *f, Slot &s, const Entry &en, const float *src, float *dst) {
+    if (f->pilot) {
+        float *ref = const_cast<float *>(src);  // clip 0: [planes][h][pitch] (radius 0)
+        const float *noisy = src + (size_t)en.nplanes * en.plane_elems;
+        cudaError_t e = cudaSuccess;
+        if (en.pilot_step1) {
+            for (int i = 0; i < en.nplanes && e == cudaSuccess; ++i) {
+                if (!((en.proc_mask >> i) & 1)) continue;
+                if (zb3d_pilot_run(f->pilot, noisy + (size_t)i * en.plane_elems, en.w, en.h, en.pitch,
+                                   en.sigma_raw[i], ref + (size_t)i * en.plane_elems, en.pitch, s.pilot_ws,
+                                   s.pilot_status, s.st) != 0)
+                    e = cudaErrorLaunchFailure;
+            }
+        } else {
+            e = run_entry(f, s, en, noisy, ref, true);
+        }
+        if (e != cudaSuccess) return e;
+    }
+    return run_entry(f, s, en, src, dst);
+}
+
 // One entry: src = its [clips][planes][tw][h][pitch] block, dst = its output block.
-cudaError_t run_entry(Filter *f, Slot &s, const Entry &en, const float *src, float *dst) {
+// basic: the plain step 1 of the pilot form (hard threshold, step-1 sigma) on the noisy
+// planes at src (one clip), written to dst as [planes][h][pitch].
+cudaError_t run_entry(Filter *f, Slot &s, const Entry &en, const float *src, float *dst, bool basic) {
     cudaError_t e = cudaSuccess;
     {
         const size_t acc = (size_t)en.nplanes * f->tw * en.plane_elems;
@@ -639,14 +685,14 @@ cudaError_t run_entry(Filter *f, Slot &s, const Entry &en, const float *src, flo
         fa.chroma = f->chroma;
         fa.list = s.list;
         fa.nblocks = (int)en.nblocks;
-        for (int i = 0; i < 3; ++i) fa.sigma[i] = en.sigma[i];
+        for (int i = 0; i < 3; ++i) fa.sigma[i] = basic ? en.sigma_basic[i] : en.sigma[i];
         fa.extractor = f->extractor;
         fa.num = s.num;
         fa.den = s.den;
         fa.acc_frame_stride = (long long)en.plane_elems;
         fa.acc_plane_stride = (long long)f->tw * en.plane_elems;
         if (f->profile) prof_event(f, f->prof_filter, s.st);
-        if ((e = launch_filter(fa, f->final_, en.t2d, en.t1d, s.st)) != cudaSuccess) return e;
+        if ((e = launch_filter(fa, f->final_ && !basic, en.t2d, en.t1d, s.st)) != cudaSuccess) return e;
         if (f->profile) prof_event(f, f->prof_filter, s.st);
         if (f->radius == 0) {
             e = launch_finish(s.num, s.den, fa.acc_plane_stride, fa.acc_frame_stride, en.w, en.h, en.pitch,
@@ -799,6 +845,26 @@ static Filter *create_impl(const zb3d_video_info *clip, const zb3d_args *a, int 
         }
         f->final_ = true;
     }
+    if (a->pilot) {
+        if (!f->v2) {
+            set_err(err, errlen, "BM3D: \"pilot\" needs BM3Dv2.");
+            return nullptr;
+        }
+        if (a->ref) {
+            set_err(err, errlen, "BM3D: \"pilot\" makes the reference itself; \"ref\" must not be given.");
+            return nullptr;
+        }
+        if (pick(a->radius, 0) != 0) {
+            set_err(err, errlen, "BM3D: \"pilot\" needs radius 0.");
+            return nullptr;
+        }
+        if (zb::pilot_device(a->pilot) != pick(a->device_id, 0)) {
+            set_err(err, errlen, "BM3D: \"pilot\" was loaded on another device.");
+            return nullptr;
+        }
+        f->pilot = a->pilot;
+        f->final_ = true;  // the filter's own step is step 2
+    }
     float sigma[3];
     per_plane<float>(a->sigma, a->n_sigma, 3.0f, sigma);
     for (float s : sigma)
@@ -809,6 +875,11 @@ static Filter *create_impl(const zb3d_video_info *clip, const zb3d_args *a, int 
     for (int i = 0; i < 3; ++i) f->process[i] = !(sigma[i] < kFltEpsilon);
     // f32(2.7*0.75*64/255) / f32(0.75*64/255) as the reference stores them (src/bm3d.zig:1019-1024)
     const float factor = f->final_ ? f32_from_bits(0x3e40c0c1u) : f32_from_bits(0x3f021bb6u);
+    float sigma_raw[3], sigma_basic[3];
+    for (int i = 0; i < 3; ++i) {
+        sigma_raw[i] = sigma[i];
+        sigma_basic[i] = sigma[i] * f32_from_bits(0x3f021bb6u);
+    }
     for (float &s : sigma) s *= factor;
 
     int block_step[3], bm_range[3], ps_num[3], ps_range[3];
@@ -926,6 +997,8 @@ static Filter *create_impl(const zb3d_video_info *clip, const zb3d_args *a, int 
         for (int i = 0; i < 3; ++i) {
             e.planes[i] = i;
             e.sigma[i] = sigma[i];
+            e.sigma_basic[i] = sigma_basic[i];
+            e.sigma_raw[i] = sigma_raw[i];
         }
         e.bs = block_step[0];
         e.range = bm_range[0];
@@ -955,6 +1028,8 @@ static Filter *create_impl(const zb3d_video_info *clip, const zb3d_args *a, int 
             e.nplanes = 1;
             e.planes[0] = p;
             e.sigma[0] = e.sigma[1] = e.sigma[2] = sigma[p];
+            e.sigma_basic[0] = e.sigma_basic[1] = e.sigma_basic[2] = sigma_basic[p];
+            e.sigma_raw[0] = e.sigma_raw[1] = e.sigma_raw[2] = sigma_raw[p];
             e.bs = block_step[p];
             e.range = bm_range[p];
             e.ps_num = ps_num[p];
@@ -993,6 +1068,17 @@ static Filter *create_impl(const zb3d_video_info *clip, const zb3d_args *a, int 
         if (e.plane_elems * f->tw * 2 * 4 >= (1ull << 32)) {
             set_err(err, errlen, "BM3D: stacked output plane too large (exceeds 4 GiB).");
             return nullptr;
+        }
+    }
+    if (f->pilot) {
+        // the pilot makes step 1 of an entry when its gate accepts every processed plane's sigma
+        for (Entry &e : f->entries) {
+            e.pilot_step1 = true;
+            for (int i = 0; i < e.nplanes; ++i)
+                if (((e.proc_mask >> i) & 1) && !zb3d_pilot_accepts(f->pilot, e.sigma_raw[i], e.w, e.h))
+                    e.pilot_step1 = false;
+            if (e.pilot_step1)
+                f->pilot_ws_bytes = std::max(f->pilot_ws_bytes, zb3d_pilot_workspace_bytes(f->pilot, e.w, e.h));
         }
     }
     f->sum_src = src_off;
@@ -1139,7 +1225,7 @@ int zb3d_process_entry_device(zb3d_filter *fp, int e, const float *d_src, float 
     const cudaStream_t st = stream ? (cudaStream_t)stream : s.st;
     const zb::Entry &en = f->entries[e];
     cudaError_t ce = zb::run_graphed(f, s, std::make_tuple((const void *)d_src, (const void *)d_dst, e), st,
-                                     [&](zb::Slot &x) { return zb::run_entry(f, x, en, d_src, d_dst); });
+                                     [&](zb::Slot &x) { return zb::run_entry_steps(f, x, en, d_src, d_dst); });
     if (ce != cudaSuccess) {
         zb::set_err(err, errlen, "BM3D: process frame failed (%s).", cudaGetErrorString(ce));
         return -1;
@@ -1320,7 +1406,7 @@ static int get_frame_window(Filter *f, int n, const zb3d_frame *clip_frames, con
     bool direct_in = true;
     auto each_src = [&](auto fn) {
         for (const Entry &e : f->entries)
-            for (int c = 0; c < f->nclips; ++c) {
+            for (int c = f->pilot ? 1 : 0; c < f->nclips; ++c) {  // pilot form: step 1 makes clip 0
                 const zb3d_frame *frames = (f->final_ && c == 0) ? ref_frames : clip_frames;
                 for (int i = 0; i < e.nplanes; ++i)
                     for (int t = 0; t < f->tw; ++t) {
@@ -1351,6 +1437,8 @@ static int get_frame_window(Filter *f, int n, const zb3d_frame *clip_frames, con
     if (ce == cudaSuccess)
         ce = run_graphed(f, s, std::make_tuple((const void *)s.d_src, (const void *)s.d_dst, -1), s.st,
                          [&](Slot &x) { return run_window(f, x, x.d_src, x.d_dst); });
+    if (ce == cudaSuccess && f->pilot && s.pilot_status)
+        ce = cudaMemcpyAsync(s.h_pilot_status, s.pilot_status, sizeof(int), cudaMemcpyDeviceToHost, s.st);
     // page-locked output planes receive the result directly (denoised planes only;
     // the stacked accumulator layout goes through staging)
     bool direct_out = !f->stacked_out();
@@ -1376,6 +1464,15 @@ static int get_frame_window(Filter *f, int n, const zb3d_frame *clip_frames, con
         cudaStreamSynchronize(s.st);
         release_slot(f, slot);
         set_err(err, errlen, "BM3D: process frame failed. (%s)", cudaGetErrorString(ce));
+        return -1;
+    }
+    if (f->pilot && s.h_pilot_status && *s.h_pilot_status != 0) {
+        // a convolution pipeline wait ran out: the frame's reference is incomplete
+        *s.h_pilot_status = 0;
+        cudaMemsetAsync(s.pilot_status, 0, sizeof(int), s.st);
+        cudaStreamSynchronize(s.st);
+        release_slot(f, slot);
+        set_err(err, errlen, "BM3D: process frame failed. (pilot convolution pipeline timed out)");
         return -1;
     }
     for (const Entry &e : f->entries) {
@@ -1460,7 +1557,7 @@ static int get_frame_temporal(Filter *f, int n, const zb3d_frame *clip_frames, c
         const int idx = sframes[q];
         float *stage = s.h_stage;  // one frame at a time through the up-stage
         for (const Entry &e : f->entries)
-            for (int c = 0; c < f->nclips; ++c) {
+            for (int c = f->pilot ? 1 : 0; c < f->nclips; ++c) {  // pilot form: step 1 makes clip 0
                 const zb3d_frame *frames = (f->final_ && c == 0) ? ref_frames : clip_frames;
                 const zb3d_frame &fr = frames[idx - first];
                 for (int i = 0; i < e.nplanes; ++i) {
@@ -1567,7 +1664,7 @@ int zb3d_get_frame(zb3d_filter *fp, int n, const zb3d_frame *clip_frames, const 
         }
         return 0;
     }
-    if (f->final_ && !ref_frames) {
+    if (f->final_ && !f->pilot && !ref_frames) {
         zb::set_err(err, errlen, "BM3D: ref frames are required.");
         return -1;
     }

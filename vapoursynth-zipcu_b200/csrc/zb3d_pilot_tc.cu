@@ -69,9 +69,10 @@ struct Args {
     const __nv_bfloat16 *wgt;  // [cout][9][cin]
     const float *bias;         // [cout]
     __nv_bfloat16 *y;          // [n][cout / 8][h][w][8] or null
-    float *y0;                 // [n][h][w] (images y0_stride apart) or null: channel 0 (+ resid) in FP32
-    const float *resid;        // [n][h][w] (images resid_stride apart) or null
+    float *y0;                 // [n][h][y0_pitch] (images y0_stride apart) or null: channel 0 (+ resid) in FP32
+    const float *resid;        // [n][h][resid_pitch] (images resid_stride apart) or null
     long long y0_stride, resid_stride;
+    int y0_pitch, resid_pitch; // floats between rows (>= w)
     int n, h, w, relu;
     int strips;                // ceil(w / 128)
     int grouped;               // boxes of 8-pixel groups (w % 8 == 0), else of single pixels
@@ -375,8 +376,9 @@ __global__ void __launch_bounds__(Shape<CIN, COUT>::THREADS, Shape<CIN, COUT>::C
                                                     pack_bf16(v[8 * i + 4], v[8 * i + 5]), pack_bf16(v[8 * i + 6], v[8 * i + 7]));
                 }
                 if (p.y0)
-                    p.y0[(size_t)k.img * p.y0_stride + pix] =
-                        v[0] + (p.resid ? p.resid[(size_t)k.img * p.resid_stride + pix] : 0.0f);
+                    p.y0[(size_t)k.img * p.y0_stride + (size_t)y * p.y0_pitch + x] =
+                        v[0] + (p.resid ? p.resid[(size_t)k.img * p.resid_stride + (size_t)y * p.resid_pitch + x]
+                                        : 0.0f);
             }
         }
     }
@@ -390,15 +392,18 @@ __global__ void __launch_bounds__(Shape<CIN, COUT>::THREADS, Shape<CIN, COUT>::C
 }
 
 // x0 [n][2][h][w][8]: block 0 = (noisy, sigma / 255 * level_scale, 0 x 6), block 1 = 0;
-// the noisy images are noisy_stride floats apart
-__global__ void pack_input_blocked(const float *noisy, long long noisy_stride, const float *sigma, int n, int h, int w,
-                                   float level_scale, __nv_bfloat16 *x0) {
+// the noisy images are noisy_stride floats apart, their rows `pitch` floats apart; the
+// noise level of image i is sigma[i], or sigma_all when sigma is null
+__global__ void pack_input_blocked(const float *noisy, long long noisy_stride, int pitch, const float *sigma,
+                                   float sigma_all, int n, int h, int w, float level_scale, __nv_bfloat16 *x0) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long plane = (long long)h * w;
     if (i >= n * plane) return;
     const long long img = i / plane, pix = i - img * plane;
+    const long long y = pix / w, x = pix - y * w;
+    const float s = sigma ? sigma[img] : sigma_all;
     uint4 *o = reinterpret_cast<uint4 *>(x0) + img * 2 * plane + pix;
-    o[0] = make_uint4(pack_bf16(noisy[img * noisy_stride + pix], sigma[img] * (1.0f / 255.0f) * level_scale), 0u, 0u,
+    o[0] = make_uint4(pack_bf16(noisy[img * noisy_stride + y * pitch + x], s * (1.0f / 255.0f) * level_scale), 0u, 0u,
                       0u);
     o[plane] = make_uint4(0u, 0u, 0u, 0u);
 }
@@ -465,39 +470,75 @@ static cudaError_t conv_tc_t(const void *x, pilot_tc::Args a, cudaStream_t st) {
 
 }  // namespace zb
 
-// ---- C ABI (include/zb3d.h) ---------------------------------------------------------
+// ---- entry points -------------------------------------------------------------------
 
-extern "C" int zb3d_pilot_conv3x3_tc(const void *x, int n, int h, int w, int cin, const void *wgt, const float *bias,
-                                     int cout, int relu, void *y, float *y0, const float *resid, long long y0_stride,
-                                     long long resid_stride, int *status, void *stream) {
-    if (n <= 0 || h <= 0 || w <= 0) return n == 0 ? 0 : -1;
+namespace zb {
+
+// One 3x3 convolution layer on the tensor cores (zb3d_pilot_conv3x3_tc), with row pitches
+// for the FP32 output and residual planes.
+cudaError_t pilot_conv_tc(const void *x, int n, int h, int w, int cin, const void *wgt, const float *bias, int cout,
+                          int relu, void *y, float *y0, long long y0_stride, int y0_pitch, const float *resid,
+                          long long resid_stride, int resid_pitch, int *status, cudaStream_t st) {
+    if (n <= 0 || h <= 0 || w <= 0) return n == 0 ? cudaSuccess : cudaErrorInvalidValue;
     if ((reinterpret_cast<uintptr_t>(x) & 15) || (reinterpret_cast<uintptr_t>(wgt) & 15) ||
         (reinterpret_cast<uintptr_t>(y) & 15))
-        return -1;
-    zb::pilot_tc::Args a{};
+        return cudaErrorInvalidValue;
+    pilot_tc::Args a{};
     a.wgt = static_cast<const __nv_bfloat16 *>(wgt);
     a.bias = bias;
     a.y = static_cast<__nv_bfloat16 *>(y);
     a.y0 = y0;
     a.resid = resid;
-    a.y0_stride = y0_stride > 0 ? y0_stride : (long long)h * w;
-    a.resid_stride = resid_stride > 0 ? resid_stride : (long long)h * w;
-    if (a.y0_stride < (long long)h * w || a.resid_stride < (long long)h * w) return -1;
+    a.y0_pitch = y0_pitch > 0 ? y0_pitch : w;
+    a.resid_pitch = resid_pitch > 0 ? resid_pitch : w;
+    if (a.y0_pitch < w || a.resid_pitch < w) return cudaErrorInvalidValue;
+    a.y0_stride = y0_stride > 0 ? y0_stride : (long long)h * a.y0_pitch;
+    a.resid_stride = resid_stride > 0 ? resid_stride : (long long)h * a.resid_pitch;
+    if (a.y0_stride < (long long)h * a.y0_pitch || a.resid_stride < (long long)h * a.resid_pitch)
+        return cudaErrorInvalidValue;
     a.n = n;
     a.h = h;
     a.w = w;
     a.relu = relu;
     a.status = status;
-    cudaError_t e = cudaErrorInvalidValue;
-    const cudaStream_t st = (cudaStream_t)stream;
-    if (cin == 16 && cout == 48) e = zb::conv_tc_t<16, 48>(x, a, st);
-    else if (cin == 48 && cout == 48) e = zb::conv_tc_t<48, 48>(x, a, st);
-    else if (cin == 48 && cout == 16) e = zb::conv_tc_t<48, 16>(x, a, st);
-    else if (cin == 16 && cout == 32) e = zb::conv_tc_t<16, 32>(x, a, st);
-    else if (cin == 32 && cout == 32) e = zb::conv_tc_t<32, 32>(x, a, st);
-    else if (cin == 32 && cout == 16) e = zb::conv_tc_t<32, 16>(x, a, st);
-    else if (cin == 16 && cout == 16) e = zb::conv_tc_t<16, 16>(x, a, st);
-    return e == cudaSuccess ? 0 : -1;
+    if (cin == 16 && cout == 48) return conv_tc_t<16, 48>(x, a, st);
+    if (cin == 48 && cout == 48) return conv_tc_t<48, 48>(x, a, st);
+    if (cin == 48 && cout == 16) return conv_tc_t<48, 16>(x, a, st);
+    if (cin == 16 && cout == 32) return conv_tc_t<16, 32>(x, a, st);
+    if (cin == 32 && cout == 32) return conv_tc_t<32, 32>(x, a, st);
+    if (cin == 32 && cout == 16) return conv_tc_t<32, 16>(x, a, st);
+    if (cin == 16 && cout == 16) return conv_tc_t<16, 16>(x, a, st);
+    return cudaErrorInvalidValue;
+}
+
+// The network input of n images (zb3d_pilot_pack_input_blocked), rows `pitch` floats apart;
+// sigma: n device values, or null for sigma_all on every image.
+cudaError_t pilot_pack_input(const float *noisy, long long noisy_stride, int pitch, const float *sigma,
+                             float sigma_all, int n, int h, int w, float level_scale, void *x0, cudaStream_t st) {
+    const long long np = (long long)n * h * w;
+    if (np <= 0) return np == 0 ? cudaSuccess : cudaErrorInvalidValue;
+    if (pitch <= 0) pitch = w;
+    if (noisy_stride <= 0) noisy_stride = (long long)h * pitch;
+    if (pitch < w || noisy_stride < (long long)h * pitch) return cudaErrorInvalidValue;
+    pilot_tc::pack_input_blocked<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(
+        noisy, noisy_stride, pitch, sigma, sigma_all, n, h, w, level_scale, static_cast<__nv_bfloat16 *>(x0));
+    return cudaGetLastError();
+}
+
+}  // namespace zb
+
+// ---- C ABI (include/zb3d.h) ---------------------------------------------------------
+
+extern "C" int zb3d_pilot_conv3x3_tc(const void *x, int n, int h, int w, int cin, const void *wgt, const float *bias,
+                                     int cout, int relu, void *y, float *y0, const float *resid, long long y0_stride,
+                                     long long resid_stride, int *status, void *stream) {
+    if (n == 0) return 0;
+    if (y0_stride > 0 && y0_stride < (long long)h * w) return -1;
+    if (resid_stride > 0 && resid_stride < (long long)h * w) return -1;
+    return zb::pilot_conv_tc(x, n, h, w, cin, wgt, bias, cout, relu, y, y0, y0_stride, w, resid, resid_stride, w,
+                             status, (cudaStream_t)stream) == cudaSuccess
+               ? 0
+               : -1;
 }
 
 extern "C" int zb3d_pilot_tc_ctas_per_sm(int ctas) {
@@ -508,11 +549,9 @@ extern "C" int zb3d_pilot_tc_ctas_per_sm(int ctas) {
 
 extern "C" int zb3d_pilot_pack_input_blocked(const float *noisy, long long noisy_stride, const float *sigma, int n,
                                              int h, int w, float level_scale, void *x0, void *stream) {
-    const long long np = (long long)n * h * w;
-    if (np <= 0) return np == 0 ? 0 : -1;
-    if (noisy_stride <= 0) noisy_stride = (long long)h * w;
-    if (noisy_stride < (long long)h * w) return -1;
-    zb::pilot_tc::pack_input_blocked<<<(unsigned)((np + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
-        noisy, noisy_stride, sigma, n, h, w, level_scale, static_cast<__nv_bfloat16 *>(x0));
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    if ((long long)n * h * w < 0 || !sigma) return -1;
+    return zb::pilot_pack_input(noisy, noisy_stride, w, sigma, 0.0f, n, h, w, level_scale, x0,
+                                (cudaStream_t)stream) == cudaSuccess
+               ? 0
+               : -1;
 }

@@ -23,7 +23,8 @@ import numpy as np
 
 from . import _native as N
 
-__all__ = ["Clip", "Error", "BM3D", "BM3Dv2", "VAggregate", "GRAY", "YUV", "RGB", "version", "pinned_empty"]
+__all__ = ["Clip", "Error", "BM3D", "BM3Dv2", "VAggregate", "Pilot", "GRAY", "YUV", "RGB", "version",
+           "pinned_empty"]
 
 GRAY, RGB, YUV = N.GRAY, N.RGB, N.YUV
 FLT_EPSILON = np.float32(1.19209290e-7)
@@ -140,6 +141,45 @@ def _frame_struct(planes, keep: list) -> N.Frame:
     return fr
 
 
+class Pilot:
+    """A learned pilot network loaded through the C ABI (zb3d_pilot_load) from a ZB3DPLT1
+    weights file (default: the shipped 32 ch x 7 layer net with its gate).  Pass it as
+    ``BM3Dv2(clip, sigma=..., pilot=p)`` to run both steps in one filter with the pilot as
+    step 1 wherever its gate accepts the plane's sigma (the plain step 1 elsewhere).  The
+    filters keep a reference to it."""
+
+    def __init__(self, path: Optional[str] = None, device_id: int = 0):
+        if path is None:
+            import os
+            path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "pilot_bs4_r12.zb3dp")
+        err = N.err_buf()
+        self.h = N.lib().zb3d_pilot_load(path.encode(), int(device_id), err, len(err))
+        if not self.h:
+            raise Error(err.value.decode())
+        self.path, self.device_id = path, int(device_id)
+        w, l, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        N.lib().zb3d_pilot_describe(self.h, ctypes.byref(w), ctypes.byref(l), ctypes.byref(g))
+        self.width, self.layers = w.value, l.value
+        self.gate = []  # (sigma, plane width, plane height, two-pass delta dB)
+        for i in range(g.value):
+            s, d, pw, ph = ctypes.c_float(), ctypes.c_float(), ctypes.c_int(), ctypes.c_int()
+            N.lib().zb3d_pilot_gate_level(self.h, i, ctypes.byref(s), ctypes.byref(pw), ctypes.byref(ph),
+                                          ctypes.byref(d))
+            self.gate.append((s.value, pw.value, ph.value, d.value))
+
+    def accepts(self, sigma: float, width: int, height: int) -> bool:
+        """Whether the gate accepts the pilot for a width x height plane at this sigma."""
+        return bool(N.lib().zb3d_pilot_accepts(self.h, float(sigma), int(width), int(height)))
+
+    def __del__(self):
+        try:
+            if self.h:
+                N.lib().zb3d_pilot_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
 def _per_plane(v, ctype):
     if v is None:
         return None, 0
@@ -172,7 +212,7 @@ class _NativeFilter:
 
 def _make_args(ref, sigma, block_step, bm_range, radius, ps_num, ps_range, chroma, device_id, num_streams,
                extractor_exp, bm_error_s, transform_2d_s, transform_1d_s, zero_init, fast_fused, keep,
-               match_form=None):
+               match_form=None, pilot=None):
     a = N.Args()
     N.lib().zb3d_args_init(ctypes.byref(a))
     if ref is not None:
@@ -199,6 +239,9 @@ def _make_args(ref, sigma, block_step, bm_range, radius, ps_num, ps_range, chrom
                       ("zero_init", zero_init), ("fast_fused", fast_fused), ("match_form", match_form)):
         if val is not None:
             setattr(a, name, int(val))
+    if pilot is not None:
+        keep.append(pilot)
+        a.pilot = pilot.h
     return a
 
 
@@ -210,7 +253,9 @@ def _create(v2, clip, ref, **kw):
     h = N.lib().zb3d_create(ctypes.byref(ci), ctypes.byref(a), v2, err, len(err))
     if not h:
         raise Error(err.value.decode())
-    return _NativeFilter(h, N.lib().zb3d_free)
+    nf = _NativeFilter(h, N.lib().zb3d_free)
+    nf.pilot = kw.get("pilot")  # the filter must not outlive its pilot
+    return nf
 
 
 def _filter_clip(nf: _NativeFilter, clip: Clip, ref: Optional[Clip]) -> Clip:
@@ -285,13 +330,23 @@ def _processed_planes(sigma, num_planes):
 def BM3Dv2(clip: Clip, ref: Optional[Clip] = None, sigma=None, block_step=None, bm_range=None, radius=None,
            ps_num=None, ps_range=None, chroma=None, device_id=None, num_streams=None, extractor_exp=None,
            bm_error_s=None, transform_2d_s=None, transform_1d_s=None, zero_init=None, fast_fused=None,
-           match_form=None) -> Clip:
+           match_form=None, pilot: Optional[Pilot] = None) -> Clip:
     """vszipcu BM3Dv2 (src/bm3d.zig:1432-1501): pass-through when no plane is
     processed; radius 0 = BM3D; radius > 0 = BM3D + VAggregate, or the fused
-    device path with fast_fused (same output bytes).  match_form as in BM3D."""
+    device path with fast_fused (same output bytes).  match_form as in BM3D.
+    pilot (not in the reference; a Pilot, radius 0, no ref): the two-pass result
+    BM3Dv2(clip, ref=<step 1>) in one filter, with the pilot as step 1 where its gate
+    accepts the plane's sigma and the plain step 1 elsewhere."""
     proc = _processed_planes(sigma, clip.num_planes)
     if not any(proc):
         return clip
+    if pilot is not None:
+        nf = _create(1, clip, ref, sigma=sigma, block_step=block_step, bm_range=bm_range, radius=radius,
+                     ps_num=ps_num, ps_range=ps_range, chroma=chroma, device_id=device_id, num_streams=num_streams,
+                     extractor_exp=extractor_exp, bm_error_s=bm_error_s, transform_2d_s=transform_2d_s,
+                     transform_1d_s=transform_1d_s, zero_init=zero_init, fast_fused=None, match_form=match_form,
+                     pilot=pilot)
+        return _filter_clip(nf, clip, None)
     kw = dict(sigma=sigma, block_step=block_step, bm_range=bm_range, radius=radius, ps_num=ps_num,
               ps_range=ps_range, chroma=chroma, device_id=device_id, num_streams=num_streams,
               extractor_exp=extractor_exp, bm_error_s=bm_error_s, transform_2d_s=transform_2d_s,

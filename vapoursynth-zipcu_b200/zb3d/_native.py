@@ -38,6 +38,7 @@ class Args(ctypes.Structure):
         ("transform_2d_s", ctypes.POINTER(c_char_p)), ("n_transform_2d_s", c_int),
         ("transform_1d_s", ctypes.POINTER(c_char_p)), ("n_transform_1d_s", c_int),
         ("zero_init", c_int), ("fast_fused", c_int), ("match_form", c_int),
+        ("pilot", c_void_p),
     ]
 
 
@@ -109,6 +110,16 @@ EXPORTS = {
                                 c_float, c_int, c_float, c_void_p, c_void_p, c_void_p]),
     "zb3d_pilot_flip_weights": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "zb3d_pilot_to_bf16": (c_int, [c_void_p, ctypes.c_longlong, c_void_p, c_void_p]),
+    "zb3d_pilot_load": (c_void_p, [c_char_p, c_int, c_char_p, c_size_t]),
+    "zb3d_pilot_from_memory": (c_void_p, [c_void_p, c_size_t, c_int, c_char_p, c_size_t]),
+    "zb3d_pilot_free": (None, [c_void_p]),
+    "zb3d_pilot_describe": (None, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
+    "zb3d_pilot_gate_level": (c_int, [c_void_p, c_int, ctypes.POINTER(c_float), ctypes.POINTER(c_int),
+                                      ctypes.POINTER(c_int), ctypes.POINTER(c_float)]),
+    "zb3d_pilot_accepts": (c_int, [c_void_p, c_float, c_int, c_int]),
+    "zb3d_pilot_workspace_bytes": (c_size_t, [c_void_p, c_int, c_int]),
+    "zb3d_pilot_run": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_void_p, c_int, c_void_p,
+                               c_void_p, c_void_p]),
     "zb3d_host_alloc": (c_void_p, [c_size_t]),
     "zb3d_host_free": (None, [c_void_p]),
 }

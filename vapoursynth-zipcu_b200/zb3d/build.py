@@ -30,6 +30,7 @@ UNITS = [
     ("zb3d_pilot_tc.cu", ARCH),
     ("zb3d_dct_tc.cu", ARCH),
     ("zb3d_host.cpp", ARCH),
+    ("zb3d_pilot_net.cpp", ARCH),
     ("zb3d_noalloc.cu", ARCH),
 ]
 HEADERS = ["zb3d_args.h", "zb3d_match.cuh", "zb3d_transforms.cuh", "zb3d_tcgen05.cuh"]

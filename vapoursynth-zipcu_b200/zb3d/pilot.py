@@ -9,9 +9,11 @@ by the project's own kernels (csrc/zb3d_pilot.cu: BF16 operands, FP32
 accumulation); inference runs on the tensor cores (csrc/zb3d_pilot_tc.cu: tcgen05.mma
 with the accumulator in tensor memory, TMA-staged input rows).  Its forward and backward passes are checked against the numpy
 oracle (oracle/pilot_oracle.py).  Step 2 keeps exact block matching; the plain
-two-pass form remains the fallback: `PilotGate` accepts the pilot for a noise level
-only where its two-pass PSNR is within 0.05 dB of the plain two-pass PSNR on
-held-out synthetic frames.
+two-pass form remains the fallback: the gate accepts the pilot for a noise level and
+plane size only where its two-pass PSNR is, on average over held-out synthetic planes,
+within 0.05 dB of the plain two-pass PSNR (`PilotGate` here; for the C ABI the table
+measured by `calibrate_file` travels inside the ZB3DPLT1 weights file that
+zb3d_pilot_load reads, and BM3Dv2(pilot=...) decides per plane).
 
 torch provides device memory and streams here; every operation on the data is a
 zb3d kernel.
@@ -35,7 +37,7 @@ def arch(width: int = 32, layers: int = 6) -> list:
     return [(16, width)] + [(width, width)] * (layers - 2) + [(width, 16)]
 
 
-SHAPES = arch(32, 6)                                 # the default (and shipped) architecture
+SHAPES = arch(32, 7)                                 # the default (and shipped) architecture
 REAL_IN, REAL_OUT = 2, 1
 LEVEL_SCALE = 4.0                                    # noise-level plane = sigma / 255 * LEVEL_SCALE
 LOSS_SCALE = 1024.0                                  # keeps BF16 gradients clear of underflow
@@ -54,7 +56,7 @@ def _ok(rc: int, what: str):
 class PilotNet:
     """The network, its FP32 master weights and Adam state, on one CUDA device."""
 
-    def __init__(self, seed: int = 0, device: str = "cuda", width: int = 32, layers: int = 6):
+    def __init__(self, seed: int = 0, device: str = "cuda", width: int = 32, layers: int = 7):
         import torch
         self.torch, self.dev = torch, device
         self.width, self.layers = width, layers
@@ -270,16 +272,34 @@ def make_pairs(count: int, size, sigmas: Sequence[float], seed: int = 1, clip0: 
     return noisy, target, clean, sig
 
 
+def detail_weights(target, strength: float) -> np.ndarray:
+    """Sampling weights of the training frames: 1 + strength x (the frame's mean squared
+    Laplacian of its step-1 target, over the mean of all frames).  Frames with fine texture,
+    which step 1 keeps and a small net tends to smooth, are drawn more often."""
+    hf = []
+    for t in target:
+        t = np.asarray(t, np.float64)
+        lap = 4.0 * t[1:-1, 1:-1] - t[:-2, 1:-1] - t[2:, 1:-1] - t[1:-1, :-2] - t[1:-1, 2:]
+        hf.append(float(np.mean(lap * lap)))
+    hf = np.asarray(hf)
+    w = 1.0 + strength * hf / max(float(hf.mean()), 1e-30)
+    return w / w.sum()
+
+
 def train(net: PilotNet, noisy, target, sigma, steps: int, batch: int = 32, crop: int = 64, lr: float = 1e-3,
-          seed: int = 0, log_every: int = 0) -> list:
-    """Adam on random crop x crop patches of the pairs; returns the loss history."""
+          seed: int = 0, log_every: int = 0, frame_weights=None) -> list:
+    """Adam on random crop x crop patches of the pairs; returns the loss history.
+    frame_weights: sampling probability of each pair's frame (None = uniform)."""
     torch = net.torch
     rng = np.random.default_rng(seed)
     dn = [torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(net.dev) for a in noisy]
     dt = [torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(net.dev) for a in target]
     hist = []
     for it in range(steps):
-        idx = rng.integers(0, len(dn), size=batch)
+        if frame_weights is None:
+            idx = rng.integers(0, len(dn), size=batch)
+        else:
+            idx = rng.choice(len(dn), size=batch, p=frame_weights)
         xs, ts = [], []
         for i in idx:
             h, w = dn[i].shape
@@ -348,11 +368,116 @@ class PilotGate:
 
 
 # ---------------------------------------------------------------------------------------
-# the shipped pilot
+# the weights file of the C ABI (zb3d_pilot_load): "ZB3DPLT1"
 # ---------------------------------------------------------------------------------------
 import os as _os
+import struct as _struct
+import zlib as _zlib
 
-# 32 ch x 6 layers, trained by `python -m zb3d.pilot train` with its defaults
+MAGIC = b"ZB3DPLT1"
+
+
+def save_weights(path: str, state, gate: Sequence = (), gate_frames: int = 0, tol: float = 0.05,
+                 level_scale: float = LEVEL_SCALE) -> None:
+    """Write the weights of `state` (PilotNet.state() or a loaded .npz: arch, w{l}, b{l})
+    with the gate table [(sigma, plane width, plane height, two-pass delta dB), ...] as the
+    ZB3DPLT1 file that zb3d_pilot_load reads (layout in csrc/zb3d_pilot_net.cpp), CRC-32 last."""
+    width, layers = (int(v) for v in np.asarray(state["arch"]).ravel()[:2])
+    shapes = arch(width, layers)
+    out = bytearray(MAGIC)
+    out += _struct.pack("<IIIf", 1, width, layers, float(level_scale))
+    out += _struct.pack("<IfI", int(gate_frames), float(tol), len(gate))
+    for s, gw, gh, d in gate:
+        out += _struct.pack("<fIIf", float(s), int(gw), int(gh), float(d))
+    for l, (cin, cout) in enumerate(shapes):
+        w = np.asarray(state[f"w{l}"], np.float32)
+        b = np.asarray(state[f"b{l}"], np.float32)
+        if w.shape != (cout, 3, 3, cin) or b.shape != (cout,):
+            raise ValueError(f"zb3d pilot: layer {l} has shape {w.shape}/{b.shape}, expected {(cout, 3, 3, cin)}")
+        out += np.ascontiguousarray(w).astype("<f4").tobytes() + np.ascontiguousarray(b).astype("<f4").tobytes()
+    out += _struct.pack("<I", _zlib.crc32(bytes(out)) & 0xFFFFFFFF)
+    tmp = path + ".tmp"
+    with open(tmp, "wb") as f:
+        f.write(bytes(out))
+    _os.replace(tmp, path)
+
+
+def read_weights(path: str) -> dict:
+    """Parse a ZB3DPLT1 file: {arch, version, level_scale, gate_frames, tol, gate, w{l}, b{l}}."""
+    with open(path, "rb") as f:
+        data = f.read()
+    if data[:8] != MAGIC:
+        raise ValueError("zb3d pilot: not a ZB3DPLT1 weights file")
+    if _zlib.crc32(data[:-4]) & 0xFFFFFFFF != _struct.unpack("<I", data[-4:])[0]:
+        raise ValueError("zb3d pilot: weights checksum mismatch")
+    at = 8
+    version, width, layers, level = _struct.unpack_from("<IIIf", data, at)
+    at += 16
+    gf, tol, ng = _struct.unpack_from("<IfI", data, at)
+    at += 12
+    gate = [_struct.unpack_from("<fIIf", data, at + 16 * i) for i in range(ng)]
+    at += 16 * ng
+    st = {"arch": np.array([width, layers], np.int32), "version": version, "level_scale": level,
+          "gate_frames": gf, "tol": tol, "gate": gate}
+    for l, (cin, cout) in enumerate(arch(width, layers)):
+        n = cout * 9 * cin
+        st[f"w{l}"] = np.frombuffer(data, "<f4", n, at).reshape(cout, 3, 3, cin).copy()
+        at += 4 * n
+        st[f"b{l}"] = np.frombuffer(data, "<f4", cout, at).copy()
+        at += 4 * cout
+    if at != len(data) - 4:
+        raise ValueError("zb3d pilot: weights size does not match the architecture")
+    return st
+
+
+GATE_SIGMAS = (5.0, 7.5, 10.0, 12.5, 15.0, 20.0, 25.0)
+GATE_SIZES = ((1920, 1080), (960, 540))   # the planes of 1080p YUV420
+
+
+def gate_deltas(pilot, sigmas=GATE_SIGMAS, sizes=GATE_SIZES, frames: int = 16, seed: int = 0, **kw) -> list:
+    """Per plane size and noise level, the two-pass PSNR difference of each of `frames`
+    held-out synthetic planes: BM3Dv2 with the pilot as step 1 (a zb3d.Pilot whose gate
+    accepts everything) minus the plain BM3Dv2 two-pass.  kw: BM3Dv2 arguments.
+    Returns [(sigma, w, h, [delta per plane])]."""
+    import zb3d
+    rows = []
+    for zi, (w, h) in enumerate(sizes):
+        for si, s in enumerate(sigmas):
+            d = []
+            for fr in range(frames):
+                c = 20000 + 1000 * seed + 200 * zi + 20 * si + fr  # frames < 20 per level stay distinct
+                cl = synth.clean_plane(w, h, c, 0)
+                clip = zb3d.Clip.from_frames([[synth.noisy_plane(w, h, s, clip=c, frame=0)]])
+                basic = zb3d.BM3Dv2(clip, sigma=s, **kw)
+                plain = np.array(zb3d.BM3Dv2(clip, ref=basic, sigma=s, **kw).get_frame(0)[0])
+                piloted = np.array(zb3d.BM3Dv2(clip, sigma=s, pilot=pilot, **kw).get_frame(0)[0])
+                d.append(synth.psnr(piloted, cl) - synth.psnr(plain, cl))
+            rows.append((float(s), w, h, d))
+    return rows
+
+
+def calibrate_file(weights_npz: str, out: str, sigmas=GATE_SIGMAS, sizes=GATE_SIZES, frames: int = 16,
+                   seed: int = 0, tol: float = 0.05, **kw) -> list:
+    """Measure the gate of a trained net through the C ABI and write its ZB3DPLT1 file:
+    per plane size and noise level, the mean two-pass difference over `frames` held-out
+    planes (gate_deltas).  Returns [(sigma, w, h, mean delta dB, per-plane deltas)]."""
+    import zb3d
+    with np.load(weights_npz) as f:
+        st = {k: f[k] for k in f.files}
+    # provisional file that accepts every level, to measure the pilot itself
+    save_weights(out, st, gate=[(s, w, h, 0.0) for w, h in sizes for s in sigmas], gate_frames=frames, tol=tol)
+    pilot = zb3d.Pilot(out)
+    rows = gate_deltas(pilot, sigmas, sizes, frames, seed, **kw)
+    del pilot
+    save_weights(out, st, gate=[(s, w, h, float(np.mean(d))) for s, w, h, d in rows], gate_frames=frames, tol=tol)
+    return [(s, w, h, float(np.mean(d)), d) for s, w, h, d in rows]
+
+
+# ---------------------------------------------------------------------------------------
+# the shipped pilot
+# ---------------------------------------------------------------------------------------
+
+# 32 ch x 7 layers, trained by `python -m zb3d.pilot train` with its defaults
 WEIGHTS = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_bs4_r12.npz")
 # the 48-channel, 10-layer net, trained by
 # `python -m zb3d.pilot train --width 48 --layers 10 --frames 6 --dims 1920x1080,960x540 --steps 12500`
@@ -360,14 +485,17 @@ WEIGHTS_W48_L10 = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "p
 # 48 ch x 10 layers trained on 3840x2160 planes:
 # `python -m zb3d.pilot train --width 48 --layers 10 --dims 3840x2160 --frames 4 --steps 12500`
 WEIGHTS_4K = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_w48_l10_4k_bs4_r12.npz")
+# the default net with its gate, for the C ABI: `python -m zb3d.pilot export` (gate measured
+# on 16 held-out 1920x1080 and 960x540 planes per level)
+WEIGHTS_BIN = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_bs4_r12.zb3dp")
 TRAIN_KW = dict(block_step=4, bm_range=12)   # step-1 configuration the shipped pilot imitates
 TRAIN_SIGMAS = (5.0, 10.0, 15.0, 20.0, 25.0)
 
 
-def shipped(device: str = "cuda", width: int = 32, layers: int = 6) -> PilotNet:
+def shipped(device: str = "cuda", width: int = 32, layers: int = 7) -> PilotNet:
     """A pilot trained by `python -m zb3d.pilot train` (weights next to this file): the
-    default 32 ch x 6 layers, or 48 ch x 10 layers."""
-    paths = {(32, 6): WEIGHTS, (48, 10): WEIGHTS_W48_L10}
+    default 32 ch x 7 layers, or 48 ch x 10 layers."""
+    paths = {(32, 7): WEIGHTS, (48, 10): WEIGHTS_W48_L10}
     if (width, layers) not in paths:
         raise ValueError(f"no shipped pilot of {width} channels x {layers} layers")
     return PilotNet.load(paths[(width, layers)], device=device)
@@ -446,18 +574,34 @@ def time_kernels(width_layers=((32, 6), (48, 10)), w: int = 1920, h: int = 1080,
 def main(argv=None):
     import argparse
     ap = argparse.ArgumentParser(prog="python -m zb3d.pilot")
-    ap.add_argument("cmd", choices=["train", "eval", "time"])
-    ap.add_argument("--frames", type=int, default=16, help="training frames per noise level and frame size")
+    ap.add_argument("cmd", choices=["train", "eval", "time", "export"])
+    ap.add_argument("--frames", type=int, default=32, help="training frames per noise level and frame size")
     ap.add_argument("--dims", default="1920x1080,1920x1080,1920x1080,960x540",
                     help="training frame sizes of the 1080p YUV420 planes; a size listed k times contributes k "
                          "sets of frames (luma-sized planes weigh 3:1 by default)")
-    ap.add_argument("--steps", type=int, default=25000, help="Adam steps of 32 crops (25000 = 800k crops)")
+    ap.add_argument("--steps", type=int, default=50000, help="Adam steps of 32 crops (50000 = 1.6M crops)")
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--width", type=int, default=32, help="channels of the hidden layers (16, 32 or 48)")
-    ap.add_argument("--layers", type=int, default=6, help="number of 3x3 convolutions")
+    ap.add_argument("--layers", type=int, default=7, help="number of 3x3 convolutions")
+    ap.add_argument("--detail", type=float, default=4.0,
+                    help="draw frames with more fine detail (step-1 Laplacian energy) more often: weight "
+                         "1 + detail x energy / mean energy")
     ap.add_argument("--out", default=WEIGHTS)
+    ap.add_argument("--weights", default=WEIGHTS, help="export: the trained .npz")
+    ap.add_argument("--bin", default=WEIGHTS_BIN, help="export: the ZB3DPLT1 file to write")
+    ap.add_argument("--gate-frames", type=int, default=16, help="export: held-out planes per plane size and level")
     a = ap.parse_args(argv)
     import time
+    if a.cmd == "export":
+        t0 = time.time()
+        rows = calibrate_file(a.weights, a.bin, frames=a.gate_frames, **TRAIN_KW)
+        print(f"gate of {a.weights} on {a.gate_frames} held-out planes per size and level "
+              f"({time.time() - t0:.1f} s):")
+        for s, w, h, m, d in rows:
+            print(f"  {w}x{h} sigma {s:5.1f}: two-pass delta mean {m:+.3f} dB (min {min(d):+.3f}, "
+                  f"max {max(d):+.3f}) -> {'pilot' if m >= -0.05 else 'plain step 1'}")
+        print(f"saved {a.bin}")
+        return
     if a.cmd == "time":
         for line in time_kernels():
             print(line)
@@ -472,7 +616,8 @@ def main(argv=None):
         print(f"{len(noisy)} training pairs ({a.dims}, step 1 with {TRAIN_KW}) in {time.time() - t0:.1f} s")
         net = PilotNet(seed=0, width=a.width, layers=a.layers)
         t0 = time.time()
-        hist = train(net, noisy, target, sig, steps=a.steps, batch=32, crop=64, lr=a.lr, seed=5)
+        fw = detail_weights(target, a.detail) if a.detail > 0 else None
+        hist = train(net, noisy, target, sig, steps=a.steps, batch=32, crop=64, lr=a.lr, seed=5, frame_weights=fw)
         net.torch.cuda.synchronize()
         print(f"{a.steps} steps x 32 crops of 64x64 in {time.time() - t0:.1f} s; "
               f"loss {np.mean(hist[:50]):.3e} -> {np.mean(hist[-50:]):.3e}")

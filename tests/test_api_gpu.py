@@ -182,6 +182,29 @@ def test_pinned_and_pageable_frames_take_the_same_path_to_the_same_bytes():
         assert np.array_equal(planes[p], ref[p])
 
 
+def test_large_pageable_planes_split_over_copy_threads():
+    """1920x1080 planes are staged by several copy threads (row chunks of at least 1 MiB):
+    pageable input and output planes, mixed with page-locked ones, give the pinned bytes."""
+    import ctypes
+    w, h, sigma = 1920, 1080, 10.0
+    plane = synth.noisy_plane(w, h, sigma, clip=9, frame=0)
+    kw = dict(sigma=sigma, block_step=4, bm_range=12)
+    pinned = zb3d.BM3Dv2(zb3d.Clip.from_frames([[plane]], pinned=True), **kw).get_frame(0)[0]
+    clip = zb3d.Clip.from_frames([[plane]])
+    nf = zb3d._create(1, clip, None, sigma=sigma, block_step=4, bm_range=12, radius=None, ps_num=None,
+                      ps_range=None, chroma=None, device_id=None, num_streams=None, extractor_exp=None,
+                      bm_error_s=None, transform_2d_s=None, transform_1d_s=None, zero_init=None, fast_fused=None)
+    keep = []
+    cf = (N.Frame * 1)(zb3d._frame_struct(clip.get_frame(0), keep))
+    out = np.zeros((h, w + 3), np.float32)  # pageable, row stride not the plane width
+    fo = N.FrameOut()
+    fo.ptr[0] = out.ctypes.data
+    fo.stride[0] = out.strides[0]
+    err = N.err_buf()
+    assert N.lib().zb3d_get_frame(nf.h, 0, cf, None, ctypes.byref(fo), err, len(err)) == 0, err.value
+    assert np.array_equal(out[:, :w], np.asarray(pinned))
+
+
 def test_graph_replay_equals_direct_launches():
     """Device entry points capture a window's launches into a CUDA graph on first use and
     replay it; profiling forces direct launches.  All three give the same bytes."""

@@ -17,8 +17,11 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <functional>
 #include <sys/stat.h>
 #include <map>
+#include <thread>
 #include <tuple>
 #include <memory>
 #include <mutex>
@@ -707,14 +710,105 @@ cudaError_t run_entry(Filter *f, Slot &s, const Entry &en, const float *src, flo
     return cudaSuccess;
 }
 
+// Host threads for the staging copies of pageable frames.  A plane's rows are split over
+// them (the caller takes a share too), so one frame's copy draws on several cores' memory
+// bandwidth.  ZB3D_COPY_THREADS sets the count (default: half the hardware threads, at
+// most 8; 0 = copies on the calling thread only).  The pool lives for the process.
+class CopyPool {
+public:
+    static CopyPool &get() {
+        static CopyPool *p = new CopyPool();  // never destroyed: workers may be waiting at exit
+        return *p;
+    }
+    int workers() const { return (int)n_; }
+    // fn(k) for k in [0, n): tasks 1.. go to the workers, the caller runs task 0 and then
+    // helps with any queued task until all n are done
+    void run(int n, const std::function<void(int)> &fn) {
+        if (n <= 1 || n_ == 0) {
+            for (int k = 0; k < n; ++k) fn(k);
+            return;
+        }
+        struct Batch {
+            std::mutex mu;
+            std::condition_variable cv;
+            int left;
+        };
+        auto b = std::make_shared<Batch>();
+        b->left = n;
+        auto done = [b] {
+            std::lock_guard<std::mutex> lk(b->mu);
+            if (--b->left == 0) b->cv.notify_all();
+        };
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            for (int k = 1; k < n; ++k)
+                q_.emplace_back([fn, k, done] {
+                    fn(k);
+                    done();
+                });
+        }
+        cv_.notify_all();
+        fn(0);
+        done();
+        for (;;) {  // help: the queue may hold this batch's tasks while every worker is busy
+            std::function<void()> t;
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                if (q_.empty()) break;
+                t = std::move(q_.front());
+                q_.pop_front();
+            }
+            t();
+        }
+        std::unique_lock<std::mutex> lk(b->mu);
+        b->cv.wait(lk, [&] { return b->left == 0; });
+    }
+
+private:
+    CopyPool() {
+        const char *v = getenv("ZB3D_COPY_THREADS");
+        unsigned hw = std::thread::hardware_concurrency();
+        n_ = v ? (unsigned)std::max(0, atoi(v)) : std::min(8u, std::max(1u, hw / 2));
+        for (unsigned i = 0; i < n_; ++i)
+            std::thread([this] {
+                for (;;) {
+                    std::function<void()> t;
+                    {
+                        std::unique_lock<std::mutex> lk(mu_);
+                        cv_.wait(lk, [&] { return !q_.empty(); });
+                        t = std::move(q_.front());
+                        q_.pop_front();
+                    }
+                    t();
+                }
+            }).detach();
+    }
+    unsigned n_ = 0;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<std::function<void()>> q_;
+};
+
+// Row copies of a plane, split into chunks of at least 1 MiB over the copy pool.
+void copy_rows(char *dst, ptrdiff_t dst_stride, const char *src, ptrdiff_t src_stride, size_t row_bytes, int h) {
+    CopyPool &pool = CopyPool::get();
+    const size_t bytes = row_bytes * (size_t)h;
+    const int chunks = (int)std::min<size_t>((size_t)pool.workers() + 1, std::max<size_t>(1, bytes >> 20));
+    const int per = (h + chunks - 1) / chunks;
+    pool.run(chunks, [&](int k) {
+        const int y0 = k * per, y1 = std::min(h, y0 + per);
+        for (int y = y0; y < y1; ++y) memcpy(dst + (ptrdiff_t)y * dst_stride, src + (ptrdiff_t)y * src_stride, row_bytes);
+    });
+}
+
 void copy_plane_in(float *dst, int pitch, const float *src, ptrdiff_t stride_bytes, int w, int h) {
-    for (int y = 0; y < h; ++y)
-        memcpy(dst + (size_t)y * pitch, (const char *)src + (ptrdiff_t)y * stride_bytes, (size_t)w * sizeof(float));
+    copy_rows((char *)dst, (ptrdiff_t)pitch * sizeof(float), (const char *)src, stride_bytes, (size_t)w * sizeof(float),
+              h);
 }
 
 void copy_plane_out(float *dst, ptrdiff_t stride_bytes, const float *src, int pitch, int w, int h) {
-    for (int y = 0; y < h; ++y)
-        memcpy((char *)dst + (ptrdiff_t)y * stride_bytes, src + (size_t)y * pitch, (size_t)w * sizeof(float));
+    copy_rows((char *)dst, stride_bytes, (const char *)src, (ptrdiff_t)pitch * sizeof(float), (size_t)w * sizeof(float),
+              h);
 }
 
 int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
@@ -1400,10 +1494,10 @@ static int get_frame_window(Filter *f, int n, const zb3d_frame *clip_frames, con
     const int slot = acquire_slot(f);
     Slot &s = f->slots[slot];
     cudaSetDevice(f->device);
-    // the window [clips][planes][t][h][pitch] per entry: page-locked caller frames
-    // are copied to the device directly, anything else goes through the slot's
-    // pinned staging buffer (src/bm3d.zig:295-373)
-    bool direct_in = true;
+    // the window [clips][planes][t][h][pitch] per entry, plane by plane: page-locked
+    // caller planes are copied to the device directly; any other plane goes through the
+    // slot's pinned staging buffer (copy threads), and its upload is issued at once, so it
+    // overlaps the staging copy of the next plane (src/bm3d.zig:295-373)
     auto each_src = [&](auto fn) {
         for (const Entry &e : f->entries)
             for (int c = f->pilot ? 1 : 0; c < f->nclips; ++c) {  // pilot form: step 1 makes clip 0
@@ -1418,20 +1512,18 @@ static int get_frame_window(Filter *f, int n, const zb3d_frame *clip_frames, con
                     }
             }
     };
-    each_src([&](const Entry &, size_t, const float *ptr, ptrdiff_t) { direct_in = direct_in && is_pinned(ptr); });
     cudaError_t ce = cudaSuccess;
-    if (direct_in) {
-        each_src([&](const Entry &e, size_t off, const float *ptr, ptrdiff_t stride) {
-            if (ce == cudaSuccess)
-                ce = cudaMemcpy2DAsync(s.d_src + off, (size_t)e.pitch * sizeof(float), ptr, (size_t)stride,
-                                       (size_t)e.w * sizeof(float), e.h, cudaMemcpyHostToDevice, s.cst);
-        });
-    } else {
-        each_src([&](const Entry &e, size_t off, const float *ptr, ptrdiff_t stride) {
+    each_src([&](const Entry &e, size_t off, const float *ptr, ptrdiff_t stride) {
+        if (ce != cudaSuccess) return;
+        if (is_pinned(ptr)) {
+            ce = cudaMemcpy2DAsync(s.d_src + off, (size_t)e.pitch * sizeof(float), ptr, (size_t)stride,
+                                   (size_t)e.w * sizeof(float), e.h, cudaMemcpyHostToDevice, s.cst);
+        } else {
             copy_plane_in(s.h_stage + off, e.pitch, ptr, stride, e.w, e.h);
-        });
-        ce = cudaMemcpyAsync(s.d_src, s.h_stage, f->sum_src * sizeof(float), cudaMemcpyHostToDevice, s.cst);
-    }
+            ce = cudaMemcpyAsync(s.d_src + off, s.h_stage + off, e.plane_elems * sizeof(float),
+                                 cudaMemcpyHostToDevice, s.cst);
+        }
+    });
     if (ce == cudaSuccess) ce = cudaEventRecord(s.ev_up, s.cst);
     if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s.st, s.ev_up, 0);
     if (ce == cudaSuccess)
@@ -1439,21 +1531,25 @@ static int get_frame_window(Filter *f, int n, const zb3d_frame *clip_frames, con
                          [&](Slot &x) { return run_window(f, x, x.d_src, x.d_dst); });
     if (ce == cudaSuccess && f->pilot && s.pilot_status)
         ce = cudaMemcpyAsync(s.h_pilot_status, s.pilot_status, sizeof(int), cudaMemcpyDeviceToHost, s.st);
-    // page-locked output planes receive the result directly (denoised planes only;
-    // the stacked accumulator layout goes through staging)
-    bool direct_out = !f->stacked_out();
-    for (const Entry &e : f->entries)
-        for (int i = 0; i < e.nplanes; ++i)
-            if ((e.proc_mask >> i) & 1) direct_out = direct_out && is_pinned(dst->ptr[e.planes[i]]);
+    // page-locked output planes receive the result directly, the others through staging
+    // (denoised planes; the stacked accumulator layout always goes through staging)
     float *down = s.h_stage + s.stage_up;
-    if (direct_out) {
+    std::vector<std::pair<const Entry *, int>> staged_out;  // (entry, plane of the entry)
+    if (!f->stacked_out()) {
         for (const Entry &e : f->entries)
             for (int i = 0; i < e.nplanes; ++i) {
                 if (!((e.proc_mask >> i) & 1) || ce != cudaSuccess) continue;
                 const int p = e.planes[i];
-                ce = cudaMemcpy2DAsync(dst->ptr[p], (size_t)dst->stride[p], s.d_dst + e.dst_off + (size_t)i * e.plane_elems,
-                                       (size_t)e.pitch * sizeof(float), (size_t)e.w * sizeof(float), e.h,
-                                       cudaMemcpyDeviceToHost, s.st);
+                const size_t off = e.dst_off + (size_t)i * e.plane_elems;
+                if (is_pinned(dst->ptr[p])) {
+                    ce = cudaMemcpy2DAsync(dst->ptr[p], (size_t)dst->stride[p], s.d_dst + off,
+                                           (size_t)e.pitch * sizeof(float), (size_t)e.w * sizeof(float), e.h,
+                                           cudaMemcpyDeviceToHost, s.st);
+                } else {
+                    ce = cudaMemcpyAsync(down + off, s.d_dst + off, e.plane_elems * sizeof(float),
+                                         cudaMemcpyDeviceToHost, s.st);
+                    staged_out.emplace_back(&e, i);
+                }
             }
     } else if (ce == cudaSuccess) {
         ce = cudaMemcpyAsync(down, s.d_dst, f->sum_dst * sizeof(float), cudaMemcpyDeviceToHost, s.st);
@@ -1475,18 +1571,18 @@ static int get_frame_window(Filter *f, int n, const zb3d_frame *clip_frames, con
         set_err(err, errlen, "BM3D: process frame failed. (pilot convolution pipeline timed out)");
         return -1;
     }
+    for (const auto &pe : staged_out) {
+        const Entry &e = *pe.first;
+        copy_plane_out(dst->ptr[e.planes[pe.second]], dst->stride[e.planes[pe.second]],
+                       down + e.dst_off + (size_t)pe.second * e.plane_elems, e.pitch, e.w, e.h);
+    }
     for (const Entry &e : f->entries) {
-        if (direct_out) break;
+        if (!f->stacked_out()) break;
         for (int i = 0; i < e.nplanes; ++i) {
             if (!((e.proc_mask >> i) & 1)) continue;
             const int p = e.planes[i];
-            if (f->stacked_out()) {
-                const float *src = down + e.dst_off + (size_t)i * f->tw * 2 * e.plane_elems;
-                copy_plane_out(dst->ptr[p], dst->stride[p], src, e.pitch, e.w, e.h * 2 * f->tw);
-            } else {
-                copy_plane_out(dst->ptr[p], dst->stride[p], down + e.dst_off + (size_t)i * e.plane_elems, e.pitch,
-                               e.w, e.h);
-            }
+            const float *src = down + e.dst_off + (size_t)i * f->tw * 2 * e.plane_elems;
+            copy_plane_out(dst->ptr[p], dst->stride[p], src, e.pitch, e.w, e.h * 2 * f->tw);
         }
     }
     if (f->stacked_out() && f->zero_init) {

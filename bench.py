@@ -55,10 +55,11 @@ def plane_dims():
     return [(W, H), (W // 2, H // 2), (W // 2, H // 2)]
 
 
-def synth_frames(clip: int, count: int):
+def synth_frames(clip: int, count: int, first: int = 0):
+    """Frames first .. first + count - 1 of a synthetic clip (three planes each)."""
     from zb3d import synth
     out = []
-    for f in range(count):
+    for f in range(first, first + count):
         out.append([synth.noisy_plane(w, h, SIGMA, clip=clip, frame=f, plane=p)
                     for p, (w, h) in enumerate(plane_dims())])
     return out
@@ -911,8 +912,15 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     from zb3d import _native as N
+    from zb3d import shard
     N.lib()
-    frames = synth_frames(rank, DISTINCT)
+    # one clip of FRAMES_PER_GPU frames per rank, sharded into contiguous output ranges
+    # (radius 0: a rank's source frames are its output frames); each rank stages the first
+    # DISTINCT frames of its range and cycles them through its FRAMES_PER_GPU buffers
+    clip_frames = FRAMES_PER_GPU * world
+    first, last = shard.source_range(clip_frames, world, rank)
+    assert (first, last) == shard.output_range(clip_frames, world, rank) and last - first == FRAMES_PER_GPU
+    frames = synth_frames(0, DISTINCT, first=first)
     pipe = DevicePipeline(torch, args.streams)
     pipe.upload(frames, FRAMES_PER_GPU)
     # warm-up: every frame buffer once (each buffer pair's launch graph is captured on first
@@ -963,7 +971,8 @@ def main():
                       "frames_per_gpu": FRAMES_PER_GPU, "batch_frames_per_step": BATCH,
                       "l2": f"inputs larger than L2: {FRAMES_PER_GPU} distinct frame buffers "
                             f"({FRAMES_PER_GPU * 2 * 12.4:.0f} MB) cycled",
-                      "parallelism": f"frame shards over {world} GPU(s), no collective",
+                      "parallelism": f"frame shards of one {FRAMES_PER_GPU * world}-frame clip over {world} "
+                                     f"GPU(s) (zb3d.shard ranges), no collective",
                       "streams": pipe.ns},
            "gpu_launches": pipe.launches_per_frame() * args.steps * BATCH,
            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
@@ -1039,7 +1048,7 @@ def main():
             pipe.close()
             pipe = None
         # timed over the same K steps as the plain form (8 frames each)
-        out["pilot_form"] = run_pilot_form(torch, frames, rank, args.steps, 1, nstreams=args.streams,
+        out["pilot_form"] = run_pilot_form(torch, frames, 0, args.steps, 1, nstreams=args.streams,
                                            weights=args.pilot_weights, conv_ctas_per_sm=args.pilot_conv_ctas)
         if not args.no_e2e and args.pilot_weights is None:
             # the pilot form through the C ABI (zb3d_args.pilot, shipped file and gate) on host frames
@@ -1057,7 +1066,7 @@ def main():
         if args.pilot_weights is None:
             # the 48-channel, 10-layer net of the learned-pilot configuration, on the same frames
             from zb3d import pilot as P
-            out["pilot_form_w48_l10"] = run_pilot_form(torch, frames, rank, args.steps, 1, nstreams=args.streams,
+            out["pilot_form_w48_l10"] = run_pilot_form(torch, frames, 0, args.steps, 1, nstreams=args.streams,
                                                        weights=P.WEIGHTS_W48_L10,
                                                        conv_ctas_per_sm=args.pilot_conv_ctas)
     if rank == 0 and not args.no_ref_cuda:

@@ -873,6 +873,8 @@ def main():
     ap.add_argument("--no-ref-cuda", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other block-matching form")
     ap.add_argument("--no-pilot", action="store_true", help="skip the learned-pilot form")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="skip the short runs of the other workloads (gray640, vbm3d, batched, pilot4k)")
     ap.add_argument("--pilot-weights", default=None, help="pilot weights (.npz) instead of the shipped ones")
     ap.add_argument("--pilot-conv-ctas", type=int, default=4,
                     help="cap on the CTAs per SM of the pilot's convolutions (1 leaves room for step 2 of "
@@ -1101,6 +1103,18 @@ def main():
             out["vs_reference_cuda"] = vs
     if pipe is not None:
         pipe.close()
+    if rank == 0 and not args.no_workloads:
+        # the other configurations of the path, each a short run of its own workload (the same
+        # functions as --workload <name>), so that one default run carries their figures
+        others = {}
+        for name, fn in (("gray640", run_gray640), ("vbm3d", run_vbm3d), ("batched", run_batched),
+                         ("pilot4k", run_pilot4k)):
+            torch.cuda.empty_cache()
+            t0 = time.perf_counter()
+            r = fn(torch, 4, 3)
+            r["wall_s"] = round(time.perf_counter() - t0, 1)
+            others[name] = r
+        out["other_workloads"] = others
     if rank == 0 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(frames)
     if dist:

@@ -339,10 +339,12 @@ template <bool SHARED>
 __device__ __forceinline__ void tiled2_chunk(const float4 (&X)[8], const float4 (&Y)[8], int m, int R, int row,
                                              int xb, int lo, int hi, const float2 (&nc)[4][4], float (&e)[8],
                                              int (&q)[8]) {
+    // the chunk's four distances first (no branch between them, so their FMA chains
+    // interleave), then the insertions in scan order; a displacement past R is computed
+    // from the tile's padding columns and discarded
+    float err[4];
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
-        const int dx = -R + 4 * m + s;
-        if (dx > R) break;
         float sj[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -355,13 +357,19 @@ __device__ __forceinline__ void tiled2_chunk(const float4 (&X)[8], const float4 
             }
             sj[j] = acc.x + acc.y;
         }
-        const float hd = (sj[0] + sj[1]) + (sj[2] + sj[3]);
-        float err;
+        err[s] = (sj[0] + sj[1]) + (sj[2] + sj[3]);
+    }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
         if constexpr (SHARED)
-            err = hd + __shfl_down_sync(kFull, hd, 1);
+            err[s] += __shfl_down_sync(kFull, err[s], 1);
         else
-            err = hd + __shfl_xor_sync(kFull, hd, 1);
-        if (dx >= lo && dx <= hi && err < e[7]) top8_insert(e, q, err, pack_pos(xb + dx, row));
+            err[s] += __shfl_xor_sync(kFull, err[s], 1);
+    }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const int dx = -R + 4 * m + s;
+        if (dx <= R && dx >= lo && dx <= hi && err[s] < e[7]) top8_insert(e, q, err[s], pack_pos(xb + dx, row));
     }
 }
 

@@ -843,6 +843,42 @@ def run_batched(torch, steps: int, warmup: int, nstreams: int = 4):
     for ci, a, z in recs:
         lat[ci].append(a.elapsed_time(z))
     px = sum(c["w"] * c["h"] * nfr for c in clips) * steps
+    # the same step through zb3d_process_batch: one call per 16 windows (a frame of every clip
+    # x 4 frames), each a persistent work-list launch over the windows' eligible planes (the
+    # r1 clip's planes run entry by entry inside the call); latency per call
+    from zb3d.device import process_batch
+    bst = torch.cuda.Stream()
+    per_call = 16
+    calls = [order[i:i + per_call] for i in range(0, len(order), per_call)]
+
+    def bstep(record=None):
+        for call in calls:
+            a = torch.cuda.Event(enable_timing=True)
+            a.record(bst)
+            # windows spread over each clip's filter instances as in the graph form, so that the
+            # entries the batch kernel does not take (the r1 clip) run on several slots at once
+            process_batch([(clips[ci]["filters"][n % nstreams], clips[ci]["src"][n].data_ptr(),
+                            clips[ci]["dst"][n].data_ptr()) for ci, n in call], bst.cuda_stream)
+            z = torch.cuda.Event(enable_timing=True)
+            z.record(bst)
+            if record is not None:
+                record.append((a, z))
+
+    for _ in range(max(warmup, 1)):
+        bstep()
+    torch.cuda.synchronize()
+    brec = []
+    bt0 = time.perf_counter()
+    for _ in range(steps):
+        bstep(brec)
+    torch.cuda.synchronize()
+    bwall = time.perf_counter() - bt0
+    blat = np.array([a.elapsed_time(z) for a, z in brec])
+    batch_form = {"value": px / bwall / 1e6, "unit": "Mpix/s", "ms_per_step": bwall * 1e3 / steps,
+                  "calls_per_step": len(calls), "windows_per_call": per_call,
+                  "latency_ms_p50": float(np.percentile(blat, 50)), "latency_ms_p99": float(np.percentile(blat, 99)),
+                  "how": f"zb3d_process_batch (synchronous) per {per_call} windows on one stream; value by wall "
+                         "clock over the timed steps, latency by CUDA events around each call"}
     per_clip = []
     for ci, c in enumerate(clips):
         l = np.array(lat[ci])
@@ -859,7 +895,8 @@ def run_batched(torch, steps: int, warmup: int, nstreams: int = 4):
                                    "YUV420 r1 (stacked output), 3840x2160 YUV420 r0; sigma U[5,20] per clip; "
                                    "block_step 4, bm_range 12, single pass", "streams": nstreams,
                        "launch": "one CUDA graph per window (all planes' memsets, matching, filtering, finishing)",
-                       "per_clip": per_clip}}
+                       "per_clip": per_clip},
+            "batch_form": batch_form}
 
 
 def main():

@@ -282,6 +282,33 @@ int zb3d_agg_z(int i, int n, int nframes, int radius);
 void *zb3d_host_alloc(size_t bytes);
 void zb3d_host_free(void *p);
 
+/* ---- batches (not in the reference) ---------------------------------------------
+ *
+ * One window (the zb3d_process_device layout: d_src, d_dst of that filter) of each job,
+ * all on the filters' device, in one call: the plane entries of every job that use SSD
+ * matching at block_step 4 or 8 (FP32 scan), radius 0 and the DCT in both dimensions are
+ * matched and filtered by one persistent launch per filter step over a work list (match
+ * tiles of every entry, then filter chunks, each chunk waiting, bounded, for its entry's
+ * matching), then finished; any other entry runs on its own as in zb3d_process_device.
+ * The call returns when the outputs are written (it synchronises `stream`).  Returns 0,
+ * or -1 with the reason in err; a chunk that gave up waiting (about half a second)
+ * reports "gave up waiting ... status 1" and leaves that batch's outputs incomplete, the
+ * device stays usable.  Calls on one device are serialised; a filter in a batch must not
+ * be used by another call at the same time.
+ * Replaces: the per-frame launch sequence of vszipcu src/bm3d.zig:375-401 for many
+ * windows at once. */
+typedef struct zb3d_batch_job {
+    zb3d_filter *filter;
+    const float *d_src;
+    float *d_dst;
+} zb3d_batch_job;
+int zb3d_process_batch(const zb3d_batch_job *jobs, int njobs, void *stream, char *err, size_t errlen);
+/* The same with the wait bound in polls (about 0.1 us each; 0 = the default, 2^22) and a
+ * testing switch that makes the first entry's filter chunks wait for one match tile more
+ * than exists, so that their waits run out. */
+int zb3d_process_batch_ex(const zb3d_batch_job *jobs, int njobs, void *stream, unsigned wait_polls,
+                          int unsatisfiable, char *err, size_t errlen);
+
 /* ---- learned pilot (not in the reference) -------------------------------------
  *
  * Kernels of the residual conv net that can replace the BM3D step-1 estimate as

@@ -52,6 +52,31 @@ struct FilterArgs {
     long long acc_plane_stride, acc_frame_stride;
 };
 
+// One plane entry of a batch (zb3d_process_batch): its matching and filtering arguments
+// (own list and accumulators) and its place in the batch's work list.  Items are numbered
+// match tiles first (all entries), then filter chunks (all entries).
+struct BatchEntry {
+    MatchArgs m;                      // tile_pitch, chunks and self_incl set; bs 4 or 8
+    FilterArgs f;
+    int tiles_x;                      // match tiles per tile row (31 or 16 block columns each)
+    int match_items;                  // match tiles (4 block rows each)
+    int filter_items;                 // filter chunks (kBatchGroups groups each)
+    long long first_match, first_filter;  // first item number of each kind
+};
+
+struct BatchArgs {
+    const BatchEntry *entries;
+    int nentries;
+    long long match_total, items_total;   // match items, all items
+    unsigned long long *next;         // next item to take (starts at 0)
+    unsigned *match_done;             // [nentries] match tiles finished
+    int *status;                      // 0, or 1 when a filter chunk gave up waiting for its matching
+    unsigned wait_polls;              // polls (about 0.1 us apart) before a wait gives up
+    int unsatisfiable;                // testing: entry 0's chunks wait for one tile more than it has
+};
+
+constexpr int kBatchGroups = 128;     // groups per filter chunk
+
 // Fixed-point scale of the accumulators: value * 2^32 held in a signed 64-bit sum.
 constexpr float kFixScale = 4294967296.0f;
 constexpr float kFixInv = 2.3283064365386962890625e-10f;

@@ -40,6 +40,12 @@ cudaError_t launch_tc_fallback(MatchArgs a, cudaStream_t st);
 int tc_debug_cols(const MatchArgs &a);
 int pilot_device(const zb3d_pilot *p);
 size_t match_tile_bytes(const MatchArgs &a, int rows_per_cta);
+size_t match_tile2_bytes_rows(const MatchArgs &a, int rows_per_cta);
+size_t batch_match_smem(const MatchArgs &m);
+size_t batch_filter_smem(bool final_);
+cudaError_t launch_batch(BatchArgs b, bool final_, int t2d, int t1d, size_t match_smem, size_t filter_smem,
+                         bool split, cudaStream_t st);
+cudaError_t launch_clamped_column(MatchArgs a, cudaStream_t st);
 cudaError_t launch_filter(const FilterArgs &a, bool final_, int t2d, int t1d, cudaStream_t st);
 cudaError_t launch_finish(const unsigned long long *num, const unsigned long long *den, long long acc_plane_stride,
                           long long acc_frame_stride, int w, int h, int pitch, int nplanes, int tw,
@@ -843,6 +849,52 @@ HostPool &host_pool() {
 using zb::Entry;
 using zb::Filter;
 
+// ---- batches: one persistent launch over the plane entries of many windows ----
+
+namespace zb {
+namespace {
+
+// Device scratch of the batch path, per device, grown on demand: per-entry match lists and
+// accumulators, the entry table, item counters and the status word.
+struct BatchCtx {
+    std::mutex mu;
+    char *arena = nullptr;
+    size_t arena_bytes = 0;
+    BatchEntry *h_entries = nullptr;  // page-locked
+    size_t h_cap = 0;
+    int *h_status = nullptr;          // page-locked
+    cudaEvent_t ev_start = nullptr;   // the caller's stream at the start of a call
+};
+
+BatchCtx &batch_ctx(int dev) {
+    static BatchCtx *ctx = new BatchCtx[64];  // never destroyed: device memory may outlive static destructors
+    return ctx[dev];
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// The batch's match items and filter items run as two stream-ordered persistent launches,
+// each kernel with the register budget of its own work (the matcher needs about 168
+// registers, the filter 72); the filter chunks still check, bounded, that their entry's
+// matching is complete.
+constexpr bool kBatchSplit = true;
+
+// Entries the batch kernel takes: spatial SSD matching at block_step 4 or 8 on the FP32
+// scan with the tiled kernel, radius 0, DCT in both dimensions, no pilot.
+bool batch_eligible(const Filter *f, const Entry &en) {
+    if (f->pilot || f->radius != 0 || en.metric != M_SSD || (en.bs != 4 && en.bs != 8) || en.form != 0) return false;
+    if (en.t2d != 0 || en.t1d != 0) return false;
+    MatchArgs m{};
+    m.bs = en.bs;
+    m.range = en.range;
+    m.chunks = (2 * en.range + 1 + 3) / 4;
+    m.tile_pitch = 128 + 4 * m.chunks;
+    return match_tile2_bytes_rows(m, 4) <= 200 * 1024;
+}
+
+}  // namespace
+}  // namespace zb
+
 extern "C" {
 
 void zb3d_args_init(zb3d_args *a) {
@@ -1288,6 +1340,240 @@ int zb3d_entry_layout_get(const zb3d_filter *fp, int e, zb3d_entry_layout *o) {
 
 size_t zb3d_src_elems(const zb3d_filter *fp) { return reinterpret_cast<const Filter *>(fp)->sum_src; }
 size_t zb3d_dst_elems(const zb3d_filter *fp) { return reinterpret_cast<const Filter *>(fp)->sum_dst; }
+
+int zb3d_process_batch_ex(const zb3d_batch_job *jobs, int njobs, void *stream, unsigned wait_polls,
+                          int unsatisfiable, char *err, size_t errlen) {
+    using namespace zb;
+    if (njobs <= 0 || !jobs) {
+        set_err(err, errlen, "zb3d_process_batch: no jobs.");
+        return -1;
+    }
+    const Filter *f0 = reinterpret_cast<const Filter *>(jobs[0].filter);
+    for (int j = 0; j < njobs; ++j) {
+        const Filter *f = reinterpret_cast<const Filter *>(jobs[j].filter);
+        if (!f || f->passthrough || f->slots.empty() || !jobs[j].d_src || !jobs[j].d_dst) {
+            set_err(err, errlen, "zb3d_process_batch: job %d has no filter to run or no buffers.", j);
+            return -1;
+        }
+        if (f->device != f0->device) {
+            set_err(err, errlen, "zb3d_process_batch: the jobs' filters are on different devices.");
+            return -1;
+        }
+    }
+    const int dev = f0->device;
+    cudaSetDevice(dev);
+    const cudaStream_t st = (cudaStream_t)stream;
+    BatchCtx &ctx = batch_ctx(dev);
+    std::lock_guard<std::mutex> lk(ctx.mu);
+
+    // the work list: eligible entries grouped by filter step (hard threshold, Wiener)
+    struct Item {
+        int job;
+        const Entry *en;
+    };
+    std::vector<Item> groups[2], fallback;
+    for (int j = 0; j < njobs; ++j) {
+        const Filter *f = reinterpret_cast<const Filter *>(jobs[j].filter);
+        for (const Entry &en : f->entries) {
+            if (batch_eligible(f, en)) groups[f->final_ ? 1 : 0].push_back({j, &en});
+            else fallback.push_back({j, &en});
+        }
+    }
+    // scratch layout: [counters | status | entries | lists | accumulators]
+    const int nent = (int)(groups[0].size() + groups[1].size());
+    const size_t counters = align256(32 + 4 * (size_t)nent);
+    size_t need = counters + 256 + align256(sizeof(BatchEntry) * (size_t)std::max(nent, 1));
+    std::vector<size_t> list_off, acc_off;
+    for (int g = 0; g < 2; ++g)
+        for (const Item &it : groups[g]) {
+            list_off.push_back(need);
+            need += align256((size_t)it.en->nblocks * 8 * sizeof(int2));
+        }
+    for (int g = 0; g < 2; ++g)
+        for (const Item &it : groups[g]) {
+            acc_off.push_back(need);
+            need += 2 * align256((size_t)it.en->nplanes * it.en->plane_elems * 8);
+        }
+    if (need > ctx.arena_bytes) {
+        cudaStreamSynchronize(st);
+        cudaFree(ctx.arena);
+        ctx.arena = nullptr;
+        ctx.arena_bytes = 0;
+        if (cudaMalloc(&ctx.arena, need) != cudaSuccess) {
+            cudaGetLastError();
+            set_err(err, errlen, "zb3d_process_batch: out of device memory (%zu MiB of scratch).", need >> 20);
+            return -1;
+        }
+        ctx.arena_bytes = need;
+    }
+    if ((size_t)nent > ctx.h_cap || !ctx.h_status) {
+        cudaStreamSynchronize(st);
+        if (ctx.h_entries) cudaFreeHost(ctx.h_entries);
+        ctx.h_entries = nullptr;
+        ctx.h_cap = 0;
+        const size_t cap = std::max<size_t>(nent, 16);
+        if (cudaHostAlloc((void **)&ctx.h_entries, cap * sizeof(BatchEntry), cudaHostAllocDefault) != cudaSuccess ||
+            (!ctx.h_status && cudaHostAlloc((void **)&ctx.h_status, sizeof(int), cudaHostAllocDefault) != cudaSuccess)) {
+            cudaGetLastError();
+            set_err(err, errlen, "zb3d_process_batch: out of page-locked host memory.");
+            return -1;
+        }
+        ctx.h_cap = cap;
+    }
+    char *arena = ctx.arena;
+    unsigned long long *d_next = reinterpret_cast<unsigned long long *>(arena);  // [2][2]: group, kind
+    unsigned *d_done = reinterpret_cast<unsigned *>(arena + 32);                 // [nent]
+    int *d_status = reinterpret_cast<int *>(arena + counters);
+    BatchEntry *d_entries = reinterpret_cast<BatchEntry *>(arena + counters + 256);
+
+    if (!ctx.ev_start && cudaEventCreateWithFlags(&ctx.ev_start, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        set_err(err, errlen, "zb3d_process_batch: cannot create an event.");
+        return -1;
+    }
+    // entries the batch kernel does not take run on their own, each filter's on the stream of
+    // one slot of that filter held for the call, after what `stream` holds so far and
+    // alongside the batch launch; `stream` waits for them at the end
+    cudaError_t ce = cudaEventRecord(ctx.ev_start, st);
+    std::map<Filter *, int> held;
+    for (const Item &it : fallback) {
+        if (ce != cudaSuccess) break;
+        Filter *f = reinterpret_cast<Filter *>(jobs[it.job].filter);
+        auto h = held.find(f);
+        if (h == held.end()) {
+            h = held.emplace(f, acquire_slot(f)).first;
+            ce = cudaStreamWaitEvent(f->slots[h->second].st, ctx.ev_start, 0);
+            if (ce != cudaSuccess) break;
+        }
+        Slot &s = f->slots[h->second];
+        ce = run_entry_steps(f, s, *it.en, jobs[it.job].d_src + it.en->src_off, jobs[it.job].d_dst + it.en->dst_off);
+    }
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(arena, 0, counters + 256, st);
+    // accumulators start at zero
+    if (ce == cudaSuccess && nent > 0) ce = cudaMemsetAsync(arena + acc_off[0], 0, need - acc_off[0], st);
+    size_t smem[2] = {0, 0};  // per group: matching tiles
+    long long totals[2][2] = {{0, 0}, {0, 0}};  // [group] (match items, all items)
+    int idx = 0;
+    for (int g = 0; g < 2 && ce == cudaSuccess; ++g) {
+        long long nm = 0;
+        const int first = idx;
+        for (const Item &it : groups[g]) {
+            const Filter *f = reinterpret_cast<const Filter *>(jobs[it.job].filter);
+            const Entry &en = *it.en;
+            const float *src = jobs[it.job].d_src + en.src_off;
+            BatchEntry &B = ctx.h_entries[idx];
+            B = BatchEntry{};
+            int2 *list = reinterpret_cast<int2 *>(arena + list_off[idx]);
+            unsigned long long *num = reinterpret_cast<unsigned long long *>(arena + acc_off[idx]);
+            unsigned long long *den = reinterpret_cast<unsigned long long *>(
+                arena + acc_off[idx] + align256((size_t)en.nplanes * en.plane_elems * 8));
+            MatchArgs &m = B.m;
+            m.frames = src;  // clip 0, plane 0: the matching plane
+            m.fstride = (long long)en.plane_elems;
+            m.w = en.w;
+            m.h = en.h;
+            m.pitch = en.pitch;
+            m.bs = en.bs;
+            m.range = en.range;
+            m.nbx = en.nbx;
+            m.nby = en.nby;
+            m.nbx_al = en.nbx_al;
+            m.chunks = (2 * en.range + 1 + 3) / 4;
+            m.tile_pitch = 128 + 4 * m.chunks;
+            m.list = list;
+            m.self_incl = 1;
+            FilterArgs &fa = B.f;
+            fa.src = src;
+            fa.plane_stride = (long long)en.plane_elems;
+            fa.clip_stride = (long long)en.nplanes * fa.plane_stride;
+            fa.frame_stride = (long long)en.plane_elems;
+            fa.w = en.w;
+            fa.h = en.h;
+            fa.pitch = en.pitch;
+            fa.nplanes = en.nplanes;
+            fa.chroma = f->chroma;
+            fa.list = list;
+            fa.nblocks = (int)en.nblocks;
+            for (int i = 0; i < 3; ++i) fa.sigma[i] = en.sigma[i];
+            fa.extractor = f->extractor;
+            fa.num = num;
+            fa.den = den;
+            fa.acc_frame_stride = (long long)en.plane_elems;
+            fa.acc_plane_stride = (long long)en.plane_elems;
+            const int nbw = en.bs == 4 ? 31 : 16;
+            B.tiles_x = (en.nbx_al + nbw - 1) / nbw;
+            B.match_items = B.tiles_x * ((en.nby + 3) / 4);
+            B.filter_items = (int)((en.nblocks + kBatchGroups - 1) / kBatchGroups);
+            B.first_match = nm;
+            nm += B.match_items;
+            smem[g] = std::max(smem[g], batch_match_smem(m));
+            // the clamped last column, before the batch launch (the batch's lists are complete
+            // when its filter chunks read them)
+            if (en.nbx_al != en.nbx && (ce = launch_clamped_column(m, st)) != cudaSuccess) break;
+            ++idx;
+        }
+        long long nf = nm;
+        for (int i = first; i < idx; ++i) {
+            ctx.h_entries[i].first_filter = nf;
+            nf += ctx.h_entries[i].filter_items;
+        }
+        totals[g][0] = nm;
+        totals[g][1] = nf;
+    }
+    if (ce == cudaSuccess && nent > 0)
+        ce = cudaMemcpyAsync(d_entries, ctx.h_entries, sizeof(BatchEntry) * (size_t)nent, cudaMemcpyHostToDevice, st);
+    for (int g = 0, base = 0; g < 2 && ce == cudaSuccess; base += (int)groups[g].size(), ++g) {
+        if (groups[g].empty()) continue;
+        BatchArgs b{};
+        b.entries = d_entries + base;
+        b.nentries = (int)groups[g].size();
+        b.match_total = totals[g][0];
+        b.items_total = totals[g][1];
+        b.next = d_next + 2 * g;
+        b.match_done = d_done + base;
+        b.status = d_status;
+        b.wait_polls = wait_polls ? wait_polls : (1u << 22);
+        b.unsatisfiable = unsatisfiable && g == (groups[0].empty() ? 1 : 0);
+        ce = launch_batch(b, g == 1, 0, 0, smem[g], batch_filter_smem(g == 1), kBatchSplit, st);
+        for (int i = 0; i < (int)groups[g].size() && ce == cudaSuccess; ++i) {
+            const Item &it = groups[g][i];
+            const Entry &en = *it.en;
+            const BatchEntry &B = ctx.h_entries[base + i];
+            ce = launch_finish(B.f.num, B.f.den, B.f.acc_plane_stride, B.f.acc_frame_stride, en.w, en.h, en.pitch,
+                               en.nplanes, 1, en.proc_mask, jobs[it.job].d_dst + en.dst_off, en.pitch,
+                               (long long)en.plane_elems, 0, st);
+        }
+    }
+    for (auto &h : held) {
+        if (ce != cudaSuccess) break;
+        Slot &s = h.first->slots[h.second];
+        ce = cudaEventRecord(s.ev_up, s.st);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, s.ev_up, 0);
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(ctx.h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    const cudaError_t cs = cudaStreamSynchronize(st);
+    if (ce == cudaSuccess) ce = cs;
+    for (auto &h : held) {
+        cudaStreamSynchronize(h.first->slots[h.second].st);  // also on an error path
+        release_slot(h.first, h.second);
+    }
+    if (ce != cudaSuccess) {
+        set_err(err, errlen, "zb3d_process_batch: %s.", cudaGetErrorString(ce));
+        return -1;
+    }
+    if (*ctx.h_status != 0) {
+        set_err(err, errlen,
+                "zb3d_process_batch: a filter chunk gave up waiting for its entry's matching (status %d); the "
+                "outputs of this batch are incomplete.",
+                *ctx.h_status);
+        return -1;
+    }
+    return 0;
+}
+
+int zb3d_process_batch(const zb3d_batch_job *jobs, int njobs, void *stream, char *err, size_t errlen) {
+    return zb3d_process_batch_ex(jobs, njobs, stream, 0, 0, err, errlen);
+}
 
 int zb3d_process_device(zb3d_filter *fp, const float *d_src, float *d_dst, void *stream, char *err, size_t errlen) {
     Filter *f = reinterpret_cast<Filter *>(fp);

@@ -22,6 +22,7 @@
 //    per patch at its origin and expanded by an 8x8 box sum in the finish pass.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "zb3d_args.h"
@@ -373,16 +374,18 @@ __device__ __forceinline__ void tiled2_chunk(const float4 (&X)[8], const float4 
     }
 }
 
+// One tile of the packed FP32x2 SSD matcher: block columns [31 bx, 31 bx + 31) (SHARED)
+// or [16 bx, ...), block rows [nw by, nw by + nw), nw = the CTA's warps; `tile` is the
+// dynamic shared-memory tile (match_tile2_bytes).
 template <bool SHARED, int BS>
-__global__ void __launch_bounds__(128) zb_match_tiled2(MatchArgs a) {
-    extern __shared__ __align__(16) float tile[];
+__device__ __forceinline__ void match_tiled2_tile(const MatchArgs &a, int bx, int by_cta, float *tile) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     constexpr int NBW = SHARED ? 31 : 16;
     const int R = a.range, W = a.w, H = a.h, tp = a.tile_pitch;
     const int pp = pair_pitch(tp);
-    const int kx0 = blockIdx.x * NBW;
+    const int kx0 = bx * NBW;
     const int x0 = kx0 * BS;
-    const int by0 = blockIdx.y * nw;
+    const int by0 = by_cta * nw;
     const int by_last = min(by0 + nw - 1, a.nby - 1);
     const int y_first = min(BS * by0, H - 8);
     const int y_last = min(BS * by_last, H - 8);
@@ -477,6 +480,12 @@ __global__ void __launch_bounds__(128) zb_match_tiled2(MatchArgs a) {
 
     if (!blk || (!SHARED && hh)) return;
     store_list(a, (long long)by * a.nbx + kx, xb, y, e, q);
+}
+
+template <bool SHARED, int BS>
+__global__ void __launch_bounds__(128) zb_match_tiled2(MatchArgs a) {
+    extern __shared__ __align__(16) float tile[];
+    match_tiled2_tile<SHARED, BS>(a, blockIdx.x, blockIdx.y, tile);
 }
 
 // ---------------------------------------------------------------------------
@@ -798,17 +807,16 @@ __device__ __forceinline__ void gather16(float (&d)[32], const float *plane, con
     }
 }
 
+// Groups g0 + threadIdx.x / 16 (16 lanes each) of one entry; tbuf: kFilterWarps * 2 *
+// kGroupBuf floats, cbuf (Wiener): (blockDim.x / 16) * kCoeffBuf floats.
 template <bool FINAL, int T2D, int T1D>
-__global__ void __launch_bounds__(kFilterWarps * 32) zb_filter16(FilterArgs a) {
+__device__ __forceinline__ void filter16_groups(const FilterArgs &a, long long g0, float *tbuf, float *cbuf) {
     using T2 = typename TransformOf<T2D>::type;
     using T1 = typename TransformOf<T1D>::type;
-    __shared__ float tbuf[kFilterWarps * 2 * kGroupBuf];
-    // Wiener: the group's 512 coefficients at [spectrum * 72 + row * 8 + column]
-    extern __shared__ float cbuf[];
     const int lane = threadIdx.x & 31;
     const int j = lane & 7, h = (lane >> 3) & 1, gw = lane >> 4;
     const unsigned gm = 0xffffu << (lane & 16);
-    const long long grp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+    const long long grp = g0 + (threadIdx.x >> 4);
     if (grp >= a.nblocks) return;
     float *gb = tbuf + ((threadIdx.x >> 5) * 2 + gw) * kGroupBuf;
     float *cb = cbuf + (threadIdx.x >> 4) * kCoeffBuf;
@@ -913,6 +921,14 @@ __global__ void __launch_bounds__(kFilterWarps * 32) zb_filter16(FilterArgs a) {
     }
 }
 
+template <bool FINAL, int T2D, int T1D>
+__global__ void __launch_bounds__(kFilterWarps * 32) zb_filter16(FilterArgs a) {
+    __shared__ float tbuf[kFilterWarps * 2 * kGroupBuf];
+    // Wiener: the group's 512 coefficients at [spectrum * 72 + row * 8 + column]
+    extern __shared__ float cbuf[];
+    filter16_groups<FINAL, T2D, T1D>(a, (long long)blockIdx.x * (blockDim.x >> 4), tbuf, cbuf);
+}
+
 // ---------------------------------------------------------------------------
 // Finish: fixed point -> float.  The weight at a pixel is the 8x8 box sum of the
 // origin weights whose patch covers it.  mode 0 writes num/den (radius 0,
@@ -967,6 +983,86 @@ __global__ void __launch_bounds__(256) zb_finish(FinishArgs a) {
         float *o = a.dst + plane * a.dst_plane_stride + (long long)slot * 2 * a.h * a.dst_pitch;
         o[(long long)y * a.dst_pitch + x] = nf;
         o[(long long)(a.h + y) * a.dst_pitch + x] = df;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Batch: one persistent launch over a work list of several plane entries (of any sizes)
+// that share the filter kind.  CTAs of 128 threads take items in order from a global
+// counter: every match tile of every entry, then every filter chunk.  A filter chunk of an
+// entry waits until all of that entry's match tiles are done (a bounded spin on its
+// counter; on timeout the chunk is skipped and the status word set).  Match items never
+// wait, and every item a CTA waits on was taken earlier by a running CTA, so the list
+// always drains.  Lists are written and read within the launch with ordinary loads and a
+// fence on both sides of the counter.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int batch_entry_of(const BatchArgs &b, long long item, bool filter) {
+    int lo = 0, hi = b.nentries - 1;  // last entry whose first item <= item
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const long long f = filter ? b.entries[mid].first_filter : b.entries[mid].first_match;
+        if (f <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// PHASE 0: the whole list in one launch; 1: match items only; 2: filter items only (the
+// items of the other kind are skipped, so two stream-ordered launches cover the list, each
+// kernel with the register budget of its own kind of work).
+template <bool FINAL, int T2D, int T1D, int PHASE>
+__global__ void __launch_bounds__(128) zb_batch(BatchArgs b) {
+    extern __shared__ __align__(16) float dyn[];  // matching tile, or the Wiener coefficient buffer
+    __shared__ float tbuf[PHASE == 1 ? 1 : kFilterWarps * 2 * kGroupBuf];
+    __shared__ long long s_item;
+    __shared__ int s_ok;
+    const long long first = PHASE == 2 ? b.match_total : 0;
+    const long long last = PHASE == 1 ? b.match_total : b.items_total;
+    for (;;) {
+        __syncthreads();  // the previous item is done with shared memory
+        if (threadIdx.x == 0) s_item = first + (long long)atomicAdd(b.next, 1ull);
+        __syncthreads();
+        const long long item = s_item;
+        if (item >= last) break;
+        if constexpr (PHASE == 2) {
+        } else if (item < b.match_total) {
+            const int e = batch_entry_of(b, item, false);
+            const BatchEntry &E = b.entries[e];
+            const int local = (int)(item - E.first_match);
+            const int bx = local % E.tiles_x, by = local / E.tiles_x;
+            if (E.m.bs == 4)
+                match_tiled2_tile<true, 4>(E.m, bx, by, dyn);
+            else
+                match_tiled2_tile<false, 8>(E.m, bx, by, dyn);
+            __threadfence();  // each thread's list stores before the tile's count
+            __syncthreads();
+            if (threadIdx.x == 0) atomicAdd(&b.match_done[e], 1u);
+            continue;
+        }
+        if constexpr (PHASE != 1) {
+            const int e = batch_entry_of(b, item, true);
+            const BatchEntry &E = b.entries[e];
+            if (threadIdx.x == 0) {
+                const unsigned need = (unsigned)E.match_items + ((b.unsatisfiable && e == 0) ? 1u : 0u);
+                volatile unsigned *done = b.match_done + e;
+                int ok = 0;
+                for (unsigned i = 0; i < b.wait_polls; ++i) {
+                    if (*done >= need) {
+                        ok = 1;
+                        break;
+                    }
+                    __nanosleep(100);
+                }
+                if (!ok) atomicCAS(b.status, 0, 1);
+                s_ok = ok;
+            }
+            __syncthreads();
+            if (!s_ok) continue;  // this chunk is left out; the status tells the host
+            __threadfence();      // the count before the lists, for every reading thread
+            const long long g0 = (item - E.first_filter) * kBatchGroups;
+            for (int g = 0; g < kBatchGroups; g += 128 / 16)
+                filter16_groups<FINAL, T2D, T1D>(E.f, g0 + g, tbuf, dyn);
+        }
     }
 }
 
@@ -1157,6 +1253,50 @@ cudaError_t launch_finish(const unsigned long long *num, const unsigned long lon
     dim3 grid((w + 31) / 32, (h + 7) / 8, nplanes * a.tw);
     zb_finish<<<grid, dim3(32, 8), 0, st>>>(a);
     return cudaGetLastError();
+}
+
+// The clamped last block column of an entry (x = w - 8), which the tiled kernels leave out.
+cudaError_t launch_clamped_column(MatchArgs a, cudaStream_t st) {
+    a.self_incl = a.radius == 0;
+    a.gen_mode = 1;
+    return launch_global_m<M_SSD>(a, st);
+}
+
+size_t match_tile2_bytes_rows(const MatchArgs &a, int rows_per_cta) { return match_tile2_bytes(a, rows_per_cta); }
+
+// Bytes of dynamic shared memory a batch entry needs: its matching tile (4 block rows),
+// and the Wiener coefficient buffer of its filter chunks.
+size_t batch_match_smem(const MatchArgs &m) { return match_tile2_bytes(m, 4); }
+size_t batch_filter_smem(bool final_) { return final_ ? (size_t)(128 / 16) * kCoeffBuf * sizeof(float) : 0; }
+
+template <class K>
+static cudaError_t launch_batch_k(K k, const BatchArgs &b, size_t smem, cudaStream_t st) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, 128, smem) != cudaSuccess || per < 1) per = 1;
+    k<<<sms * per, 128, smem, st>>>(b);
+    return cudaGetLastError();
+}
+
+// The batch kernels for the filter kind (final, t2d, t1d); only the DCT in both dimensions
+// is built in (other kinds run entry by entry).  split: the match items and the filter
+// items as two launches (b.next must point at two counters), else the whole list in one.
+// match_smem / filter_smem: dynamic shared memory of each kind of item.
+cudaError_t launch_batch(BatchArgs b, bool final_, int t2d, int t1d, size_t match_smem, size_t filter_smem,
+                         bool split, cudaStream_t st) {
+    if (t2d != T_DCT || t1d != T_DCT) return cudaErrorNotSupported;
+    if (!split)
+        return launch_batch_k(final_ ? zb_batch<true, T_DCT, T_DCT, 0> : zb_batch<false, T_DCT, T_DCT, 0>, b,
+                              std::max(match_smem, filter_smem), st);
+    cudaError_t e = launch_batch_k(final_ ? zb_batch<true, T_DCT, T_DCT, 1> : zb_batch<false, T_DCT, T_DCT, 1>, b,
+                                   match_smem, st);
+    if (e != cudaSuccess) return e;
+    b.next += 1;
+    return launch_batch_k(final_ ? zb_batch<true, T_DCT, T_DCT, 2> : zb_batch<false, T_DCT, T_DCT, 2>, b,
+                          filter_smem > 0 ? filter_smem : 16, st);
 }
 
 }  // namespace zb

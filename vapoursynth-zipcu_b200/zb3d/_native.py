@@ -50,6 +50,10 @@ class FrameOut(ctypes.Structure):
     _fields_ = [("ptr", c_void_p * 3), ("stride", ctypes.c_ssize_t * 3)]
 
 
+class BatchJob(ctypes.Structure):
+    _fields_ = [("filter", c_void_p), ("d_src", c_void_p), ("d_dst", c_void_p)]
+
+
 class EntryLayout(ctypes.Structure):
     _fields_ = [("nplanes", c_int), ("plane", c_int * 3), ("width", c_int), ("height", c_int), ("pitch", c_int),
                 ("tw", c_int), ("nclips", c_int), ("src_offset", c_size_t), ("src_elems", c_size_t),
@@ -120,6 +124,8 @@ EXPORTS = {
     "zb3d_pilot_workspace_bytes": (c_size_t, [c_void_p, c_int, c_int]),
     "zb3d_pilot_run": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_void_p, c_int, c_void_p,
                                c_void_p, c_void_p]),
+    "zb3d_process_batch": (c_int, [c_void_p, c_int, c_void_p, c_char_p, c_size_t]),
+    "zb3d_process_batch_ex": (c_int, [c_void_p, c_int, c_void_p, ctypes.c_uint, c_int, c_char_p, c_size_t]),
     "zb3d_host_alloc": (c_void_p, [c_size_t]),
     "zb3d_host_free": (None, [c_void_p]),
 }

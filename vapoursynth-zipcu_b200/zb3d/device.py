@@ -108,3 +108,14 @@ def unpack_list(raw: np.ndarray) -> np.ndarray:
     y = raw[..., 1] & 0xFFFFFF
     z = (raw[..., 1].astype(np.int64) >> 24) & 0xFF
     return np.stack([x, y, z.astype(np.int32)], axis=-1)
+
+
+def process_batch(jobs, stream: int = 0, wait_polls: int = 0, unsatisfiable: bool = False):
+    """One window of each job in one call (zb3d_process_batch): jobs = [(DeviceFilter, src_ptr,
+    dst_ptr), ...].  Synchronous; raises Error with the library's reason on failure."""
+    arr = (N.BatchJob * len(jobs))(*[N.BatchJob(f.h, s, d) for f, s, d in jobs])
+    err = N.err_buf()
+    rc = N.lib().zb3d_process_batch_ex(arr, len(jobs), stream or None, int(wait_polls), int(bool(unsatisfiable)),
+                                       err, len(err))
+    if rc != 0:
+        raise Error(err.value.decode())

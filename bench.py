@@ -508,18 +508,22 @@ def reference_arm(args, rank: int, world: int):
     return 0
 
 
-def run_vbm3d(torch, steps: int, warmup: int):
+def run_vbm3d(torch, steps: int, warmup: int, filter_form: int = 0):
     """1080p GRAYS VBM3D through BM3Dv2's fused path on the device: radius 2, sigma 15,
     default block_step / bm_range, moving synthetic scene, 120 frames in HBM.  Per
     output frame one window (2r+1 frames) is filtered into an accumulator stack and
-    the 2r+1 stacks around it are aggregated; a step is 8 output frames."""
+    the 2r+1 stacks around it are aggregated; a step is 8 output frames.
+    filter_form 1: the precision form (2D transforms on the tensor cores in split TF32);
+    then one window's accumulators are also compared with the plain form's and with the
+    FP64 oracle's."""
     import ctypes
     from zb3d import _native as N
     from zb3d import synth
     from zb3d.device import DeviceFilter
     r, nf, sigma = 2, 120, 15.0
     tw = 2 * r + 1
-    f = DeviceFilter(W, H, num_frames=nf, sigma=[sigma], radius=r, extractor_exp=EXTRACTOR_EXP, num_streams=1)
+    f = DeviceFilter(W, H, num_frames=nf, sigma=[sigma], radius=r, extractor_exp=EXTRACTOR_EXP, num_streams=1,
+                     filter_form=filter_form)
     lay = f.entries[0]
     pe = lay.height * lay.pitch
     distinct = 16
@@ -571,12 +575,58 @@ def run_vbm3d(torch, steps: int, warmup: int):
         z.record(st)
         z.synchronize()
     ms = a.elapsed_time(z)
+    res = {"metric": "VBM3D 1080p Mpix/s (BM3Dv2 radius 2, fused)", "value": W * H * steps * BATCH / ms * 1e3 / 1e6,
+           "unit": "Mpix/s", "ms_per_step": ms / steps, "steps": steps, "warmup": warmup,
+           "config": {"workload": "GRAYS 1920x1080, radius 2, sigma 15, block_step 8, bm_range 9, ps_num 2, "
+                                  "ps_range 4, extractor_exp 3, moving scene, 120 frames, one window + one "
+                                  "temporal aggregation per output frame", "batch_frames_per_step": BATCH,
+                      "filter": "precision: 2D transforms on tcgen05, split TF32" if filter_form else
+                                "plain: FP32 transforms, bit for bit the reference's"}}
+    if filter_form:
+        res["precision_error"] = vbm3d_window_errors(torch, f, frames, r, sigma)
     f.close()
-    return {"metric": "VBM3D 1080p Mpix/s (BM3Dv2 radius 2, fused)", "value": W * H * steps * BATCH / ms * 1e3 / 1e6,
-            "unit": "Mpix/s", "ms_per_step": ms / steps, "steps": steps, "warmup": warmup,
-            "config": {"workload": "GRAYS 1920x1080, radius 2, sigma 15, block_step 8, bm_range 9, ps_num 2, "
-                                   "ps_range 4, extractor_exp 3, moving scene, 120 frames, one window + one "
-                                   "temporal aggregation per output frame", "batch_frames_per_step": BATCH}}
+    return res
+
+
+def vbm3d_window_errors(torch, f, frames, r, sigma, centre: int = 10):
+    """The accumulator stack of one window (centre `centre`) from the filter f, from the same
+    filter in the plain form, and from the FP64 oracle: each slot's estimate num / den where
+    den > 0, compared (max and mean absolute difference)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    import ref_configs as rc
+    from zb3d.device import DeviceFilter
+    lay = f.entries[0]
+    tw = 2 * r + 1
+    pe = lay.height * lay.pitch
+    plain = DeviceFilter(W, H, num_frames=120, sigma=[sigma], radius=r, extractor_exp=EXTRACTOR_EXP, num_streams=1)
+    outs = []
+    for flt in (f, plain):
+        st = torch.empty(tw * 2 * pe, dtype=torch.float32, device="cuda")
+        flt.run_entry(0, frames[centre].data_ptr(), st.data_ptr())
+        torch.cuda.synchronize()
+        v = st.view(tw, 2, H, lay.pitch)[..., :W].cpu().numpy().astype(np.float64)
+        outs.append(v)
+    plain.close()
+    win = frames[centre:centre + tw].cpu().numpy()  # [tw][H][pitch]
+    cfg = orc.make_cfg(W, H, lay.pitch, [rc.scaled_sigma(sigma, False)], 8, 9, r, 2, 4, 0, 0,
+                       extractor_exp=EXTRACTOR_EXP)
+    t0 = time.perf_counter()
+    num, den, _ = orc.bm3d_pass(cfg, np.ascontiguousarray(win[None, None], np.float32), want_matches=False)
+    oracle_s = time.perf_counter() - t0
+    ref = np.where(den[0] > 0, num[0] / np.where(den[0] > 0, den[0], 1), np.nan)
+
+    def est(v):
+        return np.where(v[:, 1] > 0, v[:, 0] / np.where(v[:, 1] > 0, v[:, 1], 1), np.nan)
+
+    def cmp(a, b):
+        d = np.abs(a - b)
+        d = d[np.isfinite(d)]
+        return {"max_abs": float(d.max()), "mean_abs": float(d.mean())}
+    p, q = est(outs[0]), est(outs[1])
+    return {"window": f"centre frame {centre}, {tw} frames, every slot's estimate num/den where den > 0",
+            "precision_vs_fp64_oracle": cmp(p, ref), "plain_vs_fp64_oracle": cmp(q, ref),
+            "precision_vs_plain": cmp(p, q), "oracle_s": round(oracle_s, 1)}
 
 
 def run_pilot4k(torch, steps: int, warmup: int, nstreams: int = 4):
@@ -920,6 +970,9 @@ def main():
     ap.add_argument("--match-form", type=int, choices=[-1, 0, 1], default=-1,
                     help="block matching: -1 = the library's autotuned choice per plane, 0 = FP32 scan of every "
                          "candidate, 1 = tensor-core bound + exact re-rank")
+    ap.add_argument("--precision", action="store_true",
+                    help="vbm3d: the precision form of the filter (2D transforms on the tensor cores, split TF32), "
+                         "with its error against the plain form and the FP64 oracle")
     ap.add_argument("--workload", choices=["twopass1080", "vbm3d", "gray640", "batched", "pilot4k", "dct_tf32"],
                     default="twopass1080",
                     help="twopass1080 is the metric's workload; the others print their own line")
@@ -939,7 +992,8 @@ def main():
     if args.workload != "twopass1080":
         fn = {"vbm3d": run_vbm3d, "gray640": run_gray640, "batched": run_batched, "pilot4k": run_pilot4k,
               "dct_tf32": run_dct_tf32}[args.workload]
-        out = fn(torch, args.steps, args.warmup)
+        out = fn(torch, args.steps, args.warmup, filter_form=1) if args.precision and args.workload == "vbm3d" \
+            else fn(torch, args.steps, args.warmup)
         for k, v in {"n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic"}.items():
             out.setdefault(k, v)
         print(json.dumps(out))
@@ -1144,8 +1198,9 @@ def main():
         # the other configurations of the path, each a short run of its own workload (the same
         # functions as --workload <name>), so that one default run carries their figures
         others = {}
-        for name, fn in (("gray640", run_gray640), ("vbm3d", run_vbm3d), ("batched", run_batched),
-                         ("pilot4k", run_pilot4k)):
+        for name, fn in (("gray640", run_gray640), ("vbm3d", run_vbm3d),
+                         ("vbm3d_precision", lambda t, s, w: run_vbm3d(t, s, w, filter_form=1)),
+                         ("batched", run_batched), ("pilot4k", run_pilot4k)):
             torch.cuda.empty_cache()
             t0 = time.perf_counter()
             r = fn(torch, 4, 3)

@@ -76,6 +76,12 @@ typedef struct zb3d_args {
      * step 1 replaced.  BM3Dv2 only, no "ref" clip, radius 0, the pilot on device_id;
      * the filter does not own the pilot, which must outlive it.  NULL = off. */
     const struct zb3d_pilot *pilot;
+    /* Not in the reference.  The collaborative filter's 2D transforms: 0 (not given) = the
+     * FP32 SIMT transforms, bit for bit the reference's; 1 = the precision form, the 2D DCT
+     * of every group's patches on the tensor cores in TF32 with the hi/lo split (FP32-level
+     * error, not bitwise: a coefficient within rounding of the hard threshold may go either
+     * way).  DCT in both dimensions only. */
+    int filter_form;
 } zb3d_args;
 
 /* Fills `a` with "nothing given" (all defaults). */

@@ -37,9 +37,9 @@ def to_product_layout(f: DeviceFilter, src_ref_layout: np.ndarray) -> np.ndarray
     return out
 
 
-def run_product(spec, src_np, runs: int = 1):
+def run_product(spec, src_np, runs: int = 1, **over):
     import torch
-    f = product_filter(spec)
+    f = product_filter(spec, **over)
     lay = f.entries[0]
     d_src = torch.from_numpy(to_product_layout(f, src_np)).cuda()
     outs = []

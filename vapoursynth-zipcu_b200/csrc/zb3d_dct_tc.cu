@@ -53,8 +53,10 @@ static_assert(STAGES * 64 <= (int)TMEM_COLS, "accumulators exceed the tensor-mem
 // both K-major, N = 64 (bits 17-22 = N >> 3), M = 128 (bits 24-28 = M >> 4)
 constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((uint32_t)(TILE >> 4) << 24);
 
-// (T (x) T) as [output coefficient r * 8 + c][input pixel i * 8 + j]: TF32 high parts, remainders
-__device__ float g_kron[2][64 * 64];
+// [direction][hi, lo][output index][input index]: direction 0 is (T (x) T) as [coefficient
+// r * 8 + c][pixel i * 8 + j], direction 1 its transpose (the inverse transform, up to the
+// factor 256 of the unnormalised pair); TF32 high parts and remainders
+__device__ float g_kron[2][2][64 * 64];
 
 // Byte offset of element (row, k) in a K-major operand without swizzle: core matrices
 // of 8 rows x 16 bytes (4 elements), 8-row groups 128 bytes apart, 4-element K chunks
@@ -129,7 +131,7 @@ __device__ __forceinline__ bool wait_phase(uint32_t mbar, uint32_t parity, volat
 
 __global__ void __launch_bounds__(THREADS, 1) dct2d_tf32(const __grid_constant__ CUtensorMap map_x,
                                                        const __grid_constant__ CUtensorMap map_y, long long n,
-                                                       int split, int *status) {
+                                                       int split, int inverse, int *status) {
     extern __shared__ uint8_t sm_raw[];
     // 1024-byte aligned base: the SW128 boxes and the swizzle phase of the MMA operands need it
     const uint32_t raw_u32 = smem_u32(sm_raw);
@@ -149,8 +151,8 @@ __global__ void __launch_bounds__(THREADS, 1) dct2d_tf32(const __grid_constant__
 
     for (int i = tid; i < 64 * 64; i += THREADS) {
         const int row = i >> 6, k = i & 63;
-        *reinterpret_cast<float *>(b_hi + kmaj(row, k, 64)) = g_kron[0][i];
-        *reinterpret_cast<float *>(b_lo + kmaj(row, k, 64)) = g_kron[1][i];
+        *reinterpret_cast<float *>(b_hi + kmaj(row, k, 64)) = g_kron[inverse][0][i];
+        *reinterpret_cast<float *>(b_lo + kmaj(row, k, 64)) = g_kron[inverse][1][i];
     }
     if (tid == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -346,7 +348,7 @@ bool patch_map(CUtensorMap *map, const float *p, long long n) {
 }
 
 std::once_flag g_host_once;
-float g_host_kron[2][64 * 64];
+float g_host_kron[2][2][64 * 64];
 std::once_flag g_dev_once[64];
 cudaError_t g_dev_err[64];
 
@@ -366,8 +368,10 @@ cudaError_t init_matrix(int dev) {
                     for (int j = 0; j < 8; ++j) {
                         const float v = (float)(T[r][i] * T[c][j]);
                         const float hi = tf32_high(v);
-                        g_host_kron[0][(r * 8 + c) * 64 + i * 8 + j] = hi;
-                        g_host_kron[1][(r * 8 + c) * 64 + i * 8 + j] = v - hi;
+                        g_host_kron[0][0][(r * 8 + c) * 64 + i * 8 + j] = hi;
+                        g_host_kron[0][1][(r * 8 + c) * 64 + i * 8 + j] = v - hi;
+                        g_host_kron[1][0][(i * 8 + j) * 64 + r * 8 + c] = hi;
+                        g_host_kron[1][1][(i * 8 + j) * 64 + r * 8 + c] = v - hi;
                     }
     });
     std::call_once(g_dev_once[dev], [dev] {
@@ -378,11 +382,19 @@ cudaError_t init_matrix(int dev) {
 }
 
 }  // namespace
-}  // namespace zb
 
-extern "C" int zb3d_dct2d_tf32(const float *d_x, float *d_y, long long npatches, int split, int *d_status,
-                               void *stream) {
-    using namespace zb;
+// The matrices on device `dev` (once per process and device; synchronous, so call it
+// before any stream capture).
+cudaError_t dct_tc_init(int dev) {
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    return init_matrix(dev);
+}
+
+// y = (T (x) T) x per patch, or with inverse the transposed matrix (T^T (x) T^T); x == y is
+// allowed (each tile is loaded before it is stored, and tiles do not overlap).  Returns 0,
+// 1 for bad arguments, 2 for a CUDA error.
+int dct2d_tf32_run(const float *d_x, float *d_y, long long npatches, int split, int inverse, int *d_status,
+                   cudaStream_t stream) {
     if (npatches < 0 || (npatches > 0 && (!d_x || !d_y || !d_status))) return 1;
     // TMA: both matrices 16-byte aligned (rows are 256 bytes apart)
     if (((uintptr_t)d_y & 15) != 0 || ((uintptr_t)d_x & 15) != 0) return 1;
@@ -396,6 +408,13 @@ extern "C" int zb3d_dct2d_tf32(const float *d_x, float *d_y, long long npatches,
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long ntiles = (npatches + TILE - 1) / TILE;
     const int grid = (int)(ntiles < sms ? ntiles : sms);
-    dct2d_tf32<<<grid, THREADS, SMEM, (cudaStream_t)stream>>>(mx, my, npatches, split, d_status);
+    dct2d_tf32<<<grid, THREADS, SMEM, stream>>>(mx, my, npatches, split, inverse ? 1 : 0, d_status);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+}  // namespace zb
+
+extern "C" int zb3d_dct2d_tf32(const float *d_x, float *d_y, long long npatches, int split, int *d_status,
+                               void *stream) {
+    return zb::dct2d_tf32_run(d_x, d_y, npatches, split, 0, d_status, (cudaStream_t)stream);
 }

@@ -46,6 +46,10 @@ size_t batch_filter_smem(bool final_);
 cudaError_t launch_batch(BatchArgs b, bool final_, int t2d, int t1d, size_t match_smem, size_t filter_smem,
                          bool split, cudaStream_t st);
 cudaError_t launch_clamped_column(MatchArgs a, cudaStream_t st);
+cudaError_t filter_precision_init(int dev);
+size_t filter_precision_stack_floats(long long nblocks);
+cudaError_t launch_filter_precision(const FilterArgs &a, bool final_, float *stack, float *basic, float *weight,
+                                    int *status, cudaStream_t st);
 cudaError_t launch_filter(const FilterArgs &a, bool final_, int t2d, int t1d, cudaStream_t st);
 cudaError_t launch_finish(const unsigned long long *num, const unsigned long long *den, long long acc_plane_stride,
                           long long acc_frame_stride, int w, int h, int pitch, int nplanes, int tw,
@@ -266,8 +270,9 @@ struct Slot {
     float *h_stage = nullptr;
     size_t stage_up = 0, stage_down = 0;
     void *pilot_ws = nullptr;         // pilot form: the network's activations
-    int *pilot_status = nullptr;      // pilot form: convolution pipeline status (device)
-    int *h_pilot_status = nullptr;    // its page-locked read-back
+    int *dev_status = nullptr;        // tensor-core pipelines (pilot, precision filter): wait status (device)
+    int *h_dev_status = nullptr;      // its page-locked read-back
+    float *pf_stack = nullptr, *pf_basic = nullptr, *pf_weight = nullptr;  // precision filter stacks
 
     void destroy() {
         if (st) cudaStreamDestroy(st);
@@ -282,9 +287,12 @@ struct Slot {
         cudaFree(tc_ws);
         cudaFree(tc_stats);
         cudaFree(pilot_ws);
-        cudaFree(pilot_status);
+        cudaFree(dev_status);
+        cudaFree(pf_stack);
+        cudaFree(pf_basic);
+        cudaFree(pf_weight);
         if (h_stage) cudaFreeHost(h_stage);
-        if (h_pilot_status) cudaFreeHost(h_pilot_status);
+        if (h_dev_status) cudaFreeHost(h_dev_status);
         *this = Slot();
     }
 };
@@ -296,6 +304,7 @@ struct Filter {
     bool v2 = false, passthrough = false;
     bool final_ = false, chroma = false, fused = false, zero_init = true;
     int match_form = -1;           // -1: chosen per entry by the autotuner; 0 / 1: forced
+    int filter_form = 0;           // 0: FP32 SIMT transforms (bitwise); 1: tensor-core TF32-split 2D transforms
     const zb3d_pilot *pilot = nullptr;  // pilot form (BM3Dv2 two-pass in one call), not owned
     size_t pilot_ws_bytes = 0;
     int radius = 0, tw = 1;
@@ -371,12 +380,18 @@ bool alloc_slot(Filter *f, Slot &s) {
         if (!ok(cudaMalloc(&s.tc_stats, 4 * sizeof(unsigned long long)))) return false;
         if (!ok(cudaMemset(s.tc_stats, 0, 4 * sizeof(unsigned long long)))) return false;
     }
-    if (f->pilot) {
-        if (f->pilot_ws_bytes && !ok(cudaMalloc(&s.pilot_ws, f->pilot_ws_bytes))) return false;
-        if (!ok(cudaMalloc(&s.pilot_status, sizeof(int)))) return false;
-        if (!ok(cudaMemset(s.pilot_status, 0, sizeof(int)))) return false;
-        if (!ok(cudaHostAlloc((void **)&s.h_pilot_status, sizeof(int), cudaHostAllocDefault))) return false;
-        *s.h_pilot_status = 0;
+    if (f->pilot && f->pilot_ws_bytes && !ok(cudaMalloc(&s.pilot_ws, f->pilot_ws_bytes))) return false;
+    if (f->filter_form == 1) {
+        const size_t fl = filter_precision_stack_floats(f->max_blocks);
+        if (!ok(cudaMalloc(&s.pf_stack, fl * sizeof(float)))) return false;
+        if (f->final_ && !ok(cudaMalloc(&s.pf_basic, fl * sizeof(float)))) return false;
+        if (!ok(cudaMalloc(&s.pf_weight, (size_t)f->max_blocks * sizeof(float)))) return false;
+    }
+    if (f->pilot || f->filter_form == 1) {
+        if (!ok(cudaMalloc(&s.dev_status, sizeof(int)))) return false;
+        if (!ok(cudaMemset(s.dev_status, 0, sizeof(int)))) return false;
+        if (!ok(cudaHostAlloc((void **)&s.h_dev_status, sizeof(int), cudaHostAllocDefault))) return false;
+        *s.h_dev_status = 0;
     }
     s.stage_up = f->v2 && f->radius > 0 ? f->frame_elems : src;
     s.stage_down = dst;
@@ -659,7 +674,7 @@ cudaError_t run_entry_steps(Filter *f, Slot &s, const Entry &en, const float *sr
                 if (!((en.proc_mask >> i) & 1)) continue;
                 if (zb3d_pilot_run(f->pilot, noisy + (size_t)i * en.plane_elems, en.w, en.h, en.pitch,
                                    en.sigma_raw[i], ref + (size_t)i * en.plane_elems, en.pitch, s.pilot_ws,
-                                   s.pilot_status, s.st) != 0)
+                                   s.dev_status, s.st) != 0)
                     e = cudaErrorLaunchFailure;
             }
         } else {
@@ -701,7 +716,12 @@ cudaError_t run_entry(Filter *f, Slot &s, const Entry &en, const float *src, flo
         fa.acc_frame_stride = (long long)en.plane_elems;
         fa.acc_plane_stride = (long long)f->tw * en.plane_elems;
         if (f->profile) prof_event(f, f->prof_filter, s.st);
-        if ((e = launch_filter(fa, f->final_ && !basic, en.t2d, en.t1d, s.st)) != cudaSuccess) return e;
+        if (f->filter_form == 1)
+            e = launch_filter_precision(fa, f->final_ && !basic, s.pf_stack, s.pf_basic, s.pf_weight, s.dev_status,
+                                        s.st);
+        else
+            e = launch_filter(fa, f->final_ && !basic, en.t2d, en.t1d, s.st);
+        if (e != cudaSuccess) return e;
         if (f->profile) prof_event(f, f->prof_filter, s.st);
         if (f->radius == 0) {
             e = launch_finish(s.num, s.den, fa.acc_plane_stride, fa.acc_frame_stride, en.w, en.h, en.pitch,
@@ -882,7 +902,9 @@ constexpr bool kBatchSplit = true;
 // Entries the batch kernel takes: spatial SSD matching at block_step 4 or 8 on the FP32
 // scan with the tiled kernel, radius 0, DCT in both dimensions, no pilot.
 bool batch_eligible(const Filter *f, const Entry &en) {
-    if (f->pilot || f->radius != 0 || en.metric != M_SSD || (en.bs != 4 && en.bs != 8) || en.form != 0) return false;
+    if (f->pilot || f->filter_form != 0 || f->radius != 0 || en.metric != M_SSD || (en.bs != 4 && en.bs != 8) ||
+        en.form != 0)
+        return false;
     if (en.t2d != 0 || en.t1d != 0) return false;
     MatchArgs m{};
     m.bs = en.bs;
@@ -900,7 +922,7 @@ extern "C" {
 void zb3d_args_init(zb3d_args *a) {
     memset(a, 0, sizeof *a);
     a->radius = a->chroma = a->device_id = a->num_streams = a->extractor_exp = ZB3D_UNSET;
-    a->zero_init = a->fast_fused = a->match_form = ZB3D_UNSET;
+    a->zero_init = a->fast_fused = a->match_form = a->filter_form = ZB3D_UNSET;
 }
 
 const char *zb3d_version(void) { return "zb3d 0.1.0 (sm_100a)"; }
@@ -1075,6 +1097,11 @@ static Filter *create_impl(const zb3d_video_info *clip, const zb3d_args *a, int 
         set_err(err, errlen, "BM3D: \"match_form\" must be 0 or 1.");
         return nullptr;
     }
+    f->filter_form = pick(a->filter_form, 0);
+    if (f->filter_form != 0 && f->filter_form != 1) {
+        set_err(err, errlen, "BM3D: \"filter_form\" must be 0 or 1.");
+        return nullptr;
+    }
     const int extractor_exp = pick(a->extractor_exp, 0);
     f->extractor = extractor_exp != 0 ? std::ldexp(1.0f, extractor_exp) : 0.0f;
 
@@ -1126,6 +1153,12 @@ static Filter *create_impl(const zb3d_video_info *clip, const zb3d_args *a, int 
         return nullptr;
     }
     f->nclips = f->final_ ? 2 : 1;
+    if (f->filter_form == 1)
+        for (int i = 0; i < 3; ++i)
+            if (f->process[i] && (t2d[i] != 0 || t1d[i] != 0)) {
+                set_err(err, errlen, "BM3D: \"filter_form\" 1 needs the DCT in both dimensions.");
+                return nullptr;
+            }
 
     auto fill_geom = [&](Entry &e) {
         e.pitch = round_up(e.w, 32);
@@ -1249,6 +1282,11 @@ static Filter *create_impl(const zb3d_video_info *clip, const zb3d_args *a, int 
         return nullptr;
     }
     cudaSetDevice(f->device);
+    if (f->filter_form == 1 && filter_precision_init(f->device) != cudaSuccess) {
+        cudaGetLastError();
+        set_err(err, errlen, "BM3D: the precision filter could not be set up on the device.");
+        return nullptr;
+    }
     f->slots.resize(f->num_streams);
     int made = 0;
     for (auto &s : f->slots) {
@@ -1815,8 +1853,8 @@ static int get_frame_window(Filter *f, int n, const zb3d_frame *clip_frames, con
     if (ce == cudaSuccess)
         ce = run_graphed(f, s, std::make_tuple((const void *)s.d_src, (const void *)s.d_dst, -1), s.st,
                          [&](Slot &x) { return run_window(f, x, x.d_src, x.d_dst); });
-    if (ce == cudaSuccess && f->pilot && s.pilot_status)
-        ce = cudaMemcpyAsync(s.h_pilot_status, s.pilot_status, sizeof(int), cudaMemcpyDeviceToHost, s.st);
+    if (ce == cudaSuccess && s.dev_status)
+        ce = cudaMemcpyAsync(s.h_dev_status, s.dev_status, sizeof(int), cudaMemcpyDeviceToHost, s.st);
     // page-locked output planes receive the result directly, the others through staging
     // (denoised planes; the stacked accumulator layout always goes through staging)
     float *down = s.h_stage + s.stage_up;
@@ -1848,13 +1886,13 @@ static int get_frame_window(Filter *f, int n, const zb3d_frame *clip_frames, con
         set_err(err, errlen, "BM3D: process frame failed. (%s)", cudaGetErrorString(ce));
         return -1;
     }
-    if (f->pilot && s.h_pilot_status && *s.h_pilot_status != 0) {
-        // a convolution pipeline wait ran out: the frame's reference is incomplete
-        *s.h_pilot_status = 0;
-        cudaMemsetAsync(s.pilot_status, 0, sizeof(int), s.st);
+    if (s.h_dev_status && *s.h_dev_status != 0) {
+        // a tensor-core pipeline wait ran out: the frame is incomplete
+        *s.h_dev_status = 0;
+        cudaMemsetAsync(s.dev_status, 0, sizeof(int), s.st);
         cudaStreamSynchronize(s.st);
         release_slot(f, slot);
-        set_err(err, errlen, "BM3D: process frame failed. (pilot convolution pipeline timed out)");
+        set_err(err, errlen, "BM3D: process frame failed. (a tensor-core pipeline timed out)");
         return -1;
     }
     for (const auto &pe : staged_out) {
@@ -1998,7 +2036,14 @@ static int get_frame_temporal(Filter *f, int n, const zb3d_frame *clip_frames, c
                          (long long)e.plane_elems, s.st);
     }
     if (ce == cudaSuccess) ce = cudaMemcpyAsync(down, s.d_dst, f->sum_out * sizeof(float), cudaMemcpyDeviceToHost, s.st);
+    if (ce == cudaSuccess && s.dev_status)
+        ce = cudaMemcpyAsync(s.h_dev_status, s.dev_status, sizeof(int), cudaMemcpyDeviceToHost, s.st);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(s.st);
+    if (ce == cudaSuccess && s.h_dev_status && *s.h_dev_status != 0) {
+        *s.h_dev_status = 0;
+        cudaMemsetAsync(s.dev_status, 0, sizeof(int), s.st);
+        ce = cudaErrorLaunchTimeout;  // a tensor-core pipeline wait ran out: the frame is incomplete
+    }
     // claims are dropped only after the streams drained (released slots may be reloaded at once)
     if (ce != cudaSuccess) {
         cudaStreamSynchronize(s.cst);

@@ -212,7 +212,7 @@ class _NativeFilter:
 
 def _make_args(ref, sigma, block_step, bm_range, radius, ps_num, ps_range, chroma, device_id, num_streams,
                extractor_exp, bm_error_s, transform_2d_s, transform_1d_s, zero_init, fast_fused, keep,
-               match_form=None, pilot=None):
+               match_form=None, pilot=None, filter_form=None):
     a = N.Args()
     N.lib().zb3d_args_init(ctypes.byref(a))
     if ref is not None:
@@ -236,7 +236,8 @@ def _make_args(ref, sigma, block_step, bm_range, radius, ps_num, ps_range, chrom
             setattr(a, "n_" + name, n)
     for name, val in (("radius", radius), ("chroma", chroma), ("device_id", device_id),
                       ("num_streams", num_streams), ("extractor_exp", extractor_exp),
-                      ("zero_init", zero_init), ("fast_fused", fast_fused), ("match_form", match_form)):
+                      ("zero_init", zero_init), ("fast_fused", fast_fused), ("match_form", match_form),
+                      ("filter_form", filter_form)):
         if val is not None:
             setattr(a, name, int(val))
     if pilot is not None:
@@ -303,16 +304,19 @@ def _filter_clip(nf: _NativeFilter, clip: Clip, ref: Optional[Clip]) -> Clip:
 def BM3D(clip: Clip, ref: Optional[Clip] = None, sigma=None, block_step=None, bm_range=None, radius=None,
          ps_num=None, ps_range=None, chroma=None, device_id=None, num_streams=None, extractor_exp=None,
          bm_error_s=None, transform_2d_s=None, transform_1d_s=None, zero_init=None, fast_fused=None,
-         match_form=None) -> Clip:
+         match_form=None, filter_form=None) -> Clip:
     """vszipcu BM3D (src/bm3d.zig:965): with radius > 0 it returns the stacked
     accumulator clip (height * 2 * (2r+1)) that VAggregate consumes.  fast_fused is
     accepted and ignored, as in the reference (src/plugin.zig:83).  match_form (not
     in the reference): 0 (default) = FP32 scan of every candidate, 1 = tensor-core
-    distance bound + exact FP32 re-rank; both give the same lists."""
+    distance bound + exact FP32 re-rank; both give the same lists.  filter_form (not in the
+    reference): 0 (default) = FP32 transforms, bit for bit the reference's; 1 = the precision
+    form, 2D transforms on the tensor cores in split TF32 (FP32-level error, not bitwise)."""
     nf = _create(0, clip, ref, sigma=sigma, block_step=block_step, bm_range=bm_range, radius=radius,
                  ps_num=ps_num, ps_range=ps_range, chroma=chroma, device_id=device_id, num_streams=num_streams,
                  extractor_exp=extractor_exp, bm_error_s=bm_error_s, transform_2d_s=transform_2d_s,
-                 transform_1d_s=transform_1d_s, zero_init=zero_init, fast_fused=None, match_form=match_form)
+                 transform_1d_s=transform_1d_s, zero_init=zero_init, fast_fused=None, match_form=match_form,
+                 filter_form=filter_form)
     return _filter_clip(nf, clip, ref)
 
 
@@ -330,7 +334,7 @@ def _processed_planes(sigma, num_planes):
 def BM3Dv2(clip: Clip, ref: Optional[Clip] = None, sigma=None, block_step=None, bm_range=None, radius=None,
            ps_num=None, ps_range=None, chroma=None, device_id=None, num_streams=None, extractor_exp=None,
            bm_error_s=None, transform_2d_s=None, transform_1d_s=None, zero_init=None, fast_fused=None,
-           match_form=None, pilot: Optional[Pilot] = None) -> Clip:
+           match_form=None, pilot: Optional[Pilot] = None, filter_form=None) -> Clip:
     """vszipcu BM3Dv2 (src/bm3d.zig:1432-1501): pass-through when no plane is
     processed; radius 0 = BM3D; radius > 0 = BM3D + VAggregate, or the fused
     device path with fast_fused (same output bytes).  match_form as in BM3D.
@@ -345,12 +349,12 @@ def BM3Dv2(clip: Clip, ref: Optional[Clip] = None, sigma=None, block_step=None, 
                      ps_num=ps_num, ps_range=ps_range, chroma=chroma, device_id=device_id, num_streams=num_streams,
                      extractor_exp=extractor_exp, bm_error_s=bm_error_s, transform_2d_s=transform_2d_s,
                      transform_1d_s=transform_1d_s, zero_init=zero_init, fast_fused=None, match_form=match_form,
-                     pilot=pilot)
+                     pilot=pilot, filter_form=filter_form)
         return _filter_clip(nf, clip, None)
     kw = dict(sigma=sigma, block_step=block_step, bm_range=bm_range, radius=radius, ps_num=ps_num,
               ps_range=ps_range, chroma=chroma, device_id=device_id, num_streams=num_streams,
               extractor_exp=extractor_exp, bm_error_s=bm_error_s, transform_2d_s=transform_2d_s,
-              transform_1d_s=transform_1d_s, zero_init=zero_init, match_form=match_form)
+              transform_1d_s=transform_1d_s, zero_init=zero_init, match_form=match_form, filter_form=filter_form)
     r = 0 if radius is None else int(radius)
     if r > 0 and fast_fused:
         nf = _create(1, clip, ref, fast_fused=1, **kw)

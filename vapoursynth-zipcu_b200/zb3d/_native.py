@@ -38,7 +38,7 @@ class Args(ctypes.Structure):
         ("transform_2d_s", ctypes.POINTER(c_char_p)), ("n_transform_2d_s", c_int),
         ("transform_1d_s", ctypes.POINTER(c_char_p)), ("n_transform_1d_s", c_int),
         ("zero_init", c_int), ("fast_fused", c_int), ("match_form", c_int),
-        ("pilot", c_void_p),
+        ("pilot", c_void_p), ("filter_form", c_int),
     ]
 
 

@@ -29,6 +29,7 @@ UNITS = [
     ("zb3d_pilot.cu", ARCH),
     ("zb3d_pilot_tc.cu", ARCH),
     ("zb3d_dct_tc.cu", ARCH),
+    ("zb3d_filter_tc.cu", ARCH),
     ("zb3d_host.cpp", ARCH),
     ("zb3d_pilot_net.cpp", ARCH),
     ("zb3d_noalloc.cu", ARCH),

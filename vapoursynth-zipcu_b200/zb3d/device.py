@@ -48,7 +48,7 @@ class DeviceFilter:
     def _defaults(kw):
         names = ("sigma", "block_step", "bm_range", "radius", "ps_num", "ps_range", "chroma", "device_id",
                  "num_streams", "extractor_exp", "bm_error_s", "transform_2d_s", "transform_1d_s", "zero_init",
-                 "fast_fused", "match_form")
+                 "fast_fused", "match_form", "filter_form")
         return {n: kw.get(n) for n in names}
 
     def run(self, src_ptr: int, dst_ptr: int, stream: int = 0):

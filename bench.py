@@ -629,7 +629,7 @@ def vbm3d_window_errors(torch, f, frames, r, sigma, centre: int = 10):
             "precision_vs_plain": cmp(p, q), "oracle_s": round(oracle_s, 1)}
 
 
-def run_pilot4k(torch, steps: int, warmup: int, nstreams: int = 4):
+def run_pilot4k(torch, steps: int, warmup: int, nstreams: int = 4, weights: Optional[str] = None):
     """Learned-pilot BM3Dv2 on GRAYS 3840x2160: 4 clips of 8 frames, sigma per clip from
     U[5, 25], block_step 4, bm_range 12, with the 48-channel, 10-layer pilot trained on 4K
     planes (shipped weights).  Per clip, the two-pass PSNR against the clean frames is
@@ -644,7 +644,7 @@ def run_pilot4k(torch, steps: int, warmup: int, nstreams: int = 4):
     from zb3d.device import DeviceFilter
     w, h, nclips, nfr = 3840, 2160, 4, 8
     kw = dict(block_step=4, bm_range=12, extractor_exp=EXTRACTOR_EXP)
-    net = P.PilotNet.load(P.WEIGHTS_4K)
+    net = P.PilotNet.load(weights or P.WEIGHTS_4K)
     gate = P.PilotGate(net)
     gate.calibrate([5.0, 10.0, 15.0, 20.0, 25.0], frames=1, size=(w, h), **kw)
     rng = np.random.default_rng(4040)

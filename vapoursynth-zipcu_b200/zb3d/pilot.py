@@ -480,10 +480,10 @@ def calibrate_file(weights_npz: str, out: str, sigmas=GATE_SIGMAS, sizes=GATE_SI
 # 32 ch x 7 layers, trained by `python -m zb3d.pilot train` with its defaults
 WEIGHTS = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_bs4_r12.npz")
 # the 48-channel, 10-layer net, trained by
-# `python -m zb3d.pilot train --width 48 --layers 10 --frames 6 --dims 1920x1080,960x540 --steps 12500`
+# `python -m zb3d.pilot train --width 48 --layers 10` (the default data, steps and detail weighting)
 WEIGHTS_W48_L10 = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_w48_l10_bs4_r12.npz")
 # 48 ch x 10 layers trained on 3840x2160 planes:
-# `python -m zb3d.pilot train --width 48 --layers 10 --dims 3840x2160 --frames 4 --steps 12500`
+# `python -m zb3d.pilot train --width 48 --layers 10 --dims 3840x2160 --frames 8`
 WEIGHTS_4K = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "pilot_w48_l10_4k_bs4_r12.npz")
 # the default net with its gate, for the C ABI: `python -m zb3d.pilot export` (gate measured
 # on 16 held-out 1920x1080 and 960x540 planes per level)

@@ -40,18 +40,19 @@ __device__ __forceinline__ unsigned long long pf_to_fix(float v) {
     return (unsigned long long)__float2ll_rn(v * kFixScale);
 }
 
-// S[g][p][row * 8 + j] = plane[z][y + row][x + j] of patch p of group g: one thread per row
+// S[g][p][row * 8 + j] = plane[z][y + row][x + j] of patch p of group g: one thread per
+// patch column j, so that consecutive lanes read and write consecutive pixels
 __global__ void pf_gather(const float *__restrict__ plane, long long frame_stride, int pitch,
                           const int2 *__restrict__ list, long long nblocks, float *__restrict__ stack) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nblocks * 64) return;
     const long long gp = i >> 3;  // group * 8 + patch
-    const int row = (int)(i & 7);
+    const int j = (int)(i & 7);
     const int2 v = list[gp];
-    const float *s = plane + ((unsigned)v.y >> 24) * frame_stride + (long long)((v.y & 0xffffff) + row) * pitch + v.x;
-    float4 *d = reinterpret_cast<float4 *>(stack + gp * 64 + row * 8);
-    d[0] = make_float4(__ldg(s), __ldg(s + 1), __ldg(s + 2), __ldg(s + 3));
-    d[1] = make_float4(__ldg(s + 4), __ldg(s + 5), __ldg(s + 6), __ldg(s + 7));
+    const float *s = plane + ((unsigned)v.y >> 24) * frame_stride + (long long)(v.y & 0xffffff) * pitch + v.x + j;
+    float *d = stack + gp * 64 + j;
+#pragma unroll
+    for (int row = 0; row < 8; ++row) d[row * 8] = __ldg(s + (long long)row * pitch);
 }
 
 // One warp per group; lane handles 2D coefficients lane and lane + 32 across the 8 patches.
@@ -112,24 +113,24 @@ __global__ void pf_shrink(float *__restrict__ stack, const float *__restrict__ b
 }
 
 // num[z][y + row][x + j] += w * S[g][p][row * 8 + j] (extractor rounding of the plain form);
-// den at the patch origin += w.  One thread per patch row.
+// den at the patch origin += w.  One thread per patch column j: a warp's atomics fall on
+// 4 patch rows of 8 consecutive pixels each.
 __global__ void pf_aggregate(const float *__restrict__ stack, const float *__restrict__ weight,
                              const int2 *__restrict__ list, long long nblocks, unsigned long long *num,
                              unsigned long long *den, long long frame_stride, int pitch, float E) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nblocks * 64) return;
     const long long gp = i >> 3;
-    const int row = (int)(i & 7);
+    const int j = (int)(i & 7);
     const float w = weight[gp >> 3];
     const int2 v = list[gp];
     const long long o = ((unsigned)v.y >> 24) * frame_stride + (long long)(v.y & 0xffffff) * pitch + v.x;
-    const float4 a = reinterpret_cast<const float4 *>(stack + gp * 64 + row * 8)[0];
-    const float4 b = reinterpret_cast<const float4 *>(stack + gp * 64 + row * 8)[1];
-    const float d[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-    unsigned long long *q = num + o + (long long)row * pitch;
+    const float *d = stack + gp * 64 + j;
+    unsigned long long *q = num + o + j;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) atomicAdd(q + j, pf_to_fix(__fmaf_rn(w, d[j], E) - E));
-    if (row == 0) atomicAdd(den + o, pf_to_fix((w + E) - E));
+    for (int row = 0; row < 8; ++row)
+        atomicAdd(q + (long long)row * pitch, pf_to_fix(__fmaf_rn(w, d[row * 8], E) - E));
+    if (j == 0) atomicAdd(den + o, pf_to_fix((w + E) - E));
 }
 
 std::once_flag g_t8_host;

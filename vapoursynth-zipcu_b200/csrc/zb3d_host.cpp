@@ -1399,6 +1399,10 @@ int zb3d_process_batch_ex(const zb3d_batch_job *jobs, int njobs, void *stream, u
         }
     }
     const int dev = f0->device;
+    if (dev < 0 || dev >= 64) {
+        set_err(err, errlen, "zb3d_process_batch: device %d is beyond the 64 devices the batch path serves.", dev);
+        return -1;
+    }
     cudaSetDevice(dev);
     const cudaStream_t st = (cudaStream_t)stream;
     BatchCtx &ctx = batch_ctx(dev);

@@ -33,7 +33,8 @@ def _create(info, v2=0, ref=None, **kw):
     keep = []
     a = zb3d._make_args(ref, keep=keep, **{k: kw.get(k) for k in (
         "sigma", "block_step", "bm_range", "radius", "ps_num", "ps_range", "chroma", "device_id", "num_streams",
-        "extractor_exp", "bm_error_s", "transform_2d_s", "transform_1d_s", "zero_init", "fast_fused")})
+        "extractor_exp", "bm_error_s", "transform_2d_s", "transform_1d_s", "zero_init", "fast_fused", "match_form",
+        "filter_form")})
     err = N.err_buf()
     h = N.lib().zb3d_create(ctypes.byref(info), ctypes.byref(a), v2, err, len(err))
     if h:
@@ -75,6 +76,11 @@ CASES = [
     (dict(sigma=[0.0]), "BM3D: all planes have sigma < FLT_EPSILON (nothing to process)."),
     (dict(info=_info(w=7)), "BM3D: every processed plane must be at least 8x8."),
     (dict(info=_info(w=30, h=30, fam=N.YUV, ss=(2, 2))), "BM3D: every processed plane must be at least 8x8."),
+    # additions with no reference counterpart
+    (dict(match_form=2), 'BM3D: "match_form" must be 0 or 1.'),
+    (dict(filter_form=2), 'BM3D: "filter_form" must be 0 or 1.'),
+    (dict(filter_form=1, transform_2d_s=["haar"]), 'BM3D: "filter_form" 1 needs the DCT in both dimensions.'),
+    (dict(filter_form=1, transform_1d_s=["wht"]), 'BM3D: "filter_form" 1 needs the DCT in both dimensions.'),
 ]
 
 
@@ -183,3 +189,14 @@ def test_dct2d_tf32_argument_checks_need_no_gpu():
     assert lib.zb3d_dct2d_tf32(None, None, 5, 1, None, None) == 1    # missing buffers
     assert lib.zb3d_dct2d_tf32(None, None, -1, 1, None, None) == 1   # negative count
     assert lib.zb3d_dct2d_tf32(16, 20, 5, 1, 32, None) == 1          # output not 16-byte aligned
+
+
+def test_batch_entry_points_check_their_jobs_before_any_cuda_call():
+    """zb3d_process_batch refuses an empty job list and jobs without a filter or buffers."""
+    lib = N.lib()
+    err = N.err_buf()
+    assert lib.zb3d_process_batch(None, 0, None, err, len(err)) == -1
+    assert "no jobs" in err.value.decode()
+    jobs = (N.BatchJob * 2)(N.BatchJob(None, 0x10000, 0x10000), N.BatchJob(None, 0x10000, 0x10000))
+    assert lib.zb3d_process_batch_ex(jobs, 2, None, 0, 0, err, len(err)) == -1
+    assert "job 0 has no filter" in err.value.decode()

@@ -929,6 +929,63 @@ def run_batched(torch, steps: int, warmup: int, nstreams: int = 4):
                   "latency_ms_p50": float(np.percentile(blat, 50)), "latency_ms_p99": float(np.percentile(blat, 99)),
                   "how": f"zb3d_process_batch (synchronous) per {per_call} windows on one stream; value by wall "
                          "clock over the timed steps, latency by CUDA events around each call"}
+    # the same step as 4 batches captured once as CUDA graphs (zb3d_batch_create), replayed
+    # asynchronously round-robin on 2 streams; the r1 clip's windows use filters of their
+    # own with a slot per live batch (each batch holds one slot of such a filter)
+    from zb3d.device import Batch
+    gfil = {ci: [DeviceFilter(c["w"], c["h"], family=c["fam"], subsampling=c["sub"], num_streams=len(calls),
+                              num_frames=nfr, sigma=[c["sigma"]] * 3, chroma=c["chroma"], radius=c["radius"],
+                              block_step=4, bm_range=12, extractor_exp=EXTRACTOR_EXP) for _ in range(nstreams)]
+            for ci, c in enumerate(clips) if c["radius"] > 0}
+
+    def gfilter(ci, n):
+        return gfil[ci][n % nstreams] if ci in gfil else clips[ci]["filters"][n % nstreams]
+    batches = [Batch([(gfilter(ci, n), clips[ci]["src"][n].data_ptr(), clips[ci]["dst"][n].data_ptr())
+                      for ci, n in call]) for call in calls]
+    gst = [torch.cuda.Stream() for _ in range(2)]
+
+    def gstep(record=None):
+        for k, bt in enumerate(batches):
+            s_ = gst[k % 2]
+            a = torch.cuda.Event(enable_timing=True)
+            a.record(s_)
+            bt.launch(s_.cuda_stream)
+            z = torch.cuda.Event(enable_timing=True)
+            z.record(s_)
+            if record is not None:
+                record.append((a, z))
+
+    for _ in range(max(warmup, 1)):
+        gstep()
+    torch.cuda.synchronize()
+    for bt in batches:
+        bt.status()
+    g0 = torch.cuda.Event(enable_timing=True)
+    g0.record(gst[0])
+    gst[1].wait_event(g0)
+    grec = []
+    for _ in range(steps):
+        gstep(grec)
+    e1 = torch.cuda.Event()
+    e1.record(gst[1])
+    gst[0].wait_event(e1)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g1.record(gst[0])
+    g1.synchronize()
+    for bt in batches:
+        bt.status()
+    gms = g0.elapsed_time(g1)
+    glat = np.array([a.elapsed_time(z) for a, z in grec])
+    batch_form["graph"] = {"value": px / (gms / 1e3) / 1e6, "unit": "Mpix/s", "ms_per_step": gms / steps,
+                           "latency_ms_p50": float(np.percentile(glat, 50)),
+                           "latency_ms_p99": float(np.percentile(glat, 99)),
+                           "how": f"{len(batches)} batches of {per_call} windows captured once each "
+                                  "(zb3d_batch_create), replayed round-robin on 2 streams; CUDA events"}
+    for bt in batches:
+        bt.close()
+    for fl in gfil.values():
+        for f in fl:
+            f.close()
     per_clip = []
     for ci, c in enumerate(clips):
         l = np.array(lat[ci])

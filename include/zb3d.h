@@ -315,6 +315,21 @@ int zb3d_process_batch(const zb3d_batch_job *jobs, int njobs, void *stream, char
 int zb3d_process_batch_ex(const zb3d_batch_job *jobs, int njobs, void *stream, unsigned wait_polls,
                           int unsatisfiable, char *err, size_t errlen);
 
+/* The same batch captured once into a CUDA graph (work-list launches, finishes, the
+ * entries outside the work list and the status read-back), with scratch of its own:
+ * zb3d_batch_launch replays it on `stream` asynchronously, for the same jobs and buffers.
+ * Launches of one batch must not overlap on the GPU; different batches may.  After the
+ * caller has synchronised the stream, zb3d_batch_status returns 0, or -1 with the reason
+ * when a filter chunk of the last launch gave up waiting.  Creation holds one slot of each
+ * filter whose entries run outside the work list until zb3d_batch_free (waiting for a free
+ * one), so such a filter needs a slot per live batch that uses it beside its own callers'.
+ * NULL with the reason in err on failure. */
+typedef struct zb3d_batch zb3d_batch;
+zb3d_batch *zb3d_batch_create(const zb3d_batch_job *jobs, int njobs, char *err, size_t errlen);
+int zb3d_batch_launch(zb3d_batch *b, void *stream, char *err, size_t errlen);
+int zb3d_batch_status(zb3d_batch *b, char *err, size_t errlen);
+void zb3d_batch_free(zb3d_batch *b);
+
 /* ---- learned pilot (not in the reference) -------------------------------------
  *
  * Kernels of the residual conv net that can replace the BM3D step-1 estimate as

@@ -874,16 +874,29 @@ using zb::Filter;
 namespace zb {
 namespace {
 
-// Device scratch of the batch path, per device, grown on demand: per-entry match lists and
-// accumulators, the entry table, item counters and the status word.
-struct BatchCtx {
-    std::mutex mu;
+// Scratch of a batch: per-entry match lists and accumulators, the entry table, item
+// counters and the status word.  The synchronous call shares one per device (grown on
+// demand); a graph handle owns its own.
+struct BatchBuffers {
     char *arena = nullptr;
     size_t arena_bytes = 0;
     BatchEntry *h_entries = nullptr;  // page-locked
     size_t h_cap = 0;
     int *h_status = nullptr;          // page-locked
-    cudaEvent_t ev_start = nullptr;   // the caller's stream at the start of a call
+    cudaEvent_t ev_start = nullptr;   // the launching stream at the start of a batch
+
+    void release() {
+        cudaFree(arena);
+        if (h_entries) cudaFreeHost(h_entries);
+        if (h_status) cudaFreeHost(h_status);
+        if (ev_start) cudaEventDestroy(ev_start);
+        *this = BatchBuffers();
+    }
+};
+
+struct BatchCtx {
+    std::mutex mu;
+    BatchBuffers buf;
 };
 
 BatchCtx &batch_ctx(int dev) {
@@ -914,6 +927,250 @@ bool batch_eligible(const Filter *f, const Entry &en) {
     return match_tile2_bytes_rows(m, 4) <= 200 * 1024;
 }
 
+
+struct BatchItem {
+    int job;
+    const Entry *en;
+};
+
+// A batch's work list and scratch layout: eligible entries grouped by filter step (hard
+// threshold, Wiener), the others run on their own.
+struct BatchPlan {
+    std::vector<zb3d_batch_job> jobs;
+    int device = 0;
+    std::vector<BatchItem> groups[2], fallback;
+    int nent = 0;
+    size_t counters = 0, need = 0;
+    std::vector<size_t> list_off, acc_off;
+};
+
+bool plan_batch(const zb3d_batch_job *jobs, int njobs, BatchPlan &p, char *err, size_t errlen) {
+    if (njobs <= 0 || !jobs) {
+        set_err(err, errlen, "zb3d_process_batch: no jobs.");
+        return false;
+    }
+    const Filter *f0 = reinterpret_cast<const Filter *>(jobs[0].filter);
+    for (int j = 0; j < njobs; ++j) {
+        const Filter *f = reinterpret_cast<const Filter *>(jobs[j].filter);
+        if (!f || f->passthrough || f->slots.empty() || !jobs[j].d_src || !jobs[j].d_dst) {
+            set_err(err, errlen, "zb3d_process_batch: job %d has no filter to run or no buffers.", j);
+            return false;
+        }
+        if (f->device != f0->device) {
+            set_err(err, errlen, "zb3d_process_batch: the jobs' filters are on different devices.");
+            return false;
+        }
+    }
+    p.device = f0->device;
+    if (p.device < 0 || p.device >= 64) {
+        set_err(err, errlen, "zb3d_process_batch: device %d is beyond the 64 devices the batch path serves.",
+                p.device);
+        return false;
+    }
+    p.jobs.assign(jobs, jobs + njobs);
+    for (int j = 0; j < njobs; ++j) {
+        const Filter *f = reinterpret_cast<const Filter *>(jobs[j].filter);
+        for (const Entry &en : f->entries) {
+            if (batch_eligible(f, en)) p.groups[f->final_ ? 1 : 0].push_back({j, &en});
+            else p.fallback.push_back({j, &en});
+        }
+    }
+    // scratch layout: [counters | status | entries | lists | accumulators]
+    p.nent = (int)(p.groups[0].size() + p.groups[1].size());
+    p.counters = align256(32 + 4 * (size_t)p.nent);
+    p.need = p.counters + 256 + align256(sizeof(BatchEntry) * (size_t)std::max(p.nent, 1));
+    for (int g = 0; g < 2; ++g)
+        for (const BatchItem &it : p.groups[g]) {
+            p.list_off.push_back(p.need);
+            p.need += align256((size_t)it.en->nblocks * 8 * sizeof(int2));
+        }
+    for (int g = 0; g < 2; ++g)
+        for (const BatchItem &it : p.groups[g]) {
+            p.acc_off.push_back(p.need);
+            p.need += 2 * align256((size_t)it.en->nplanes * it.en->plane_elems * 8);
+        }
+    return true;
+}
+
+// Scratch of at least the plan's size (grown when smaller; `st` is synchronised first).
+bool ensure_buffers(BatchBuffers &b, const BatchPlan &p, cudaStream_t st, char *err, size_t errlen) {
+    if (p.need > b.arena_bytes) {
+        cudaStreamSynchronize(st);
+        cudaFree(b.arena);
+        b.arena = nullptr;
+        b.arena_bytes = 0;
+        if (cudaMalloc(&b.arena, p.need) != cudaSuccess) {
+            cudaGetLastError();
+            set_err(err, errlen, "zb3d_process_batch: out of device memory (%zu MiB of scratch).", p.need >> 20);
+            return false;
+        }
+        b.arena_bytes = p.need;
+    }
+    if ((size_t)p.nent > b.h_cap || !b.h_status) {
+        cudaStreamSynchronize(st);
+        if (b.h_entries) cudaFreeHost(b.h_entries);
+        b.h_entries = nullptr;
+        b.h_cap = 0;
+        const size_t cap = std::max<size_t>(p.nent, 16);
+        if (cudaHostAlloc((void **)&b.h_entries, cap * sizeof(BatchEntry), cudaHostAllocDefault) != cudaSuccess ||
+            (!b.h_status && cudaHostAlloc((void **)&b.h_status, sizeof(int), cudaHostAllocDefault) != cudaSuccess)) {
+            cudaGetLastError();
+            set_err(err, errlen, "zb3d_process_batch: out of page-locked host memory.");
+            return false;
+        }
+        b.h_cap = cap;
+    }
+    if (!b.ev_start && cudaEventCreateWithFlags(&b.ev_start, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        set_err(err, errlen, "zb3d_process_batch: cannot create an event.");
+        return false;
+    }
+    return true;
+}
+
+// One slot of each filter whose entries run outside the work list (waits for a free one).
+std::map<Filter *, int> hold_slots(const BatchPlan &p) {
+    std::map<Filter *, int> held;
+    for (const BatchItem &it : p.fallback) {
+        Filter *f = reinterpret_cast<Filter *>(p.jobs[it.job].filter);
+        if (!held.count(f)) held.emplace(f, acquire_slot(f));
+    }
+    return held;
+}
+
+void release_slots(std::map<Filter *, int> &held) {
+    for (auto &h : held) {
+        cudaStreamSynchronize(h.first->slots[h.second].st);
+        release_slot(h.first, h.second);
+    }
+    held.clear();
+}
+
+// The whole batch on `st`: entries outside the work list on the held slots' streams (after
+// what `st` holds so far, joined back at the end), the work-list launches and the finishes,
+// then the status word into b.h_status.  Builds the entry table in b.h_entries; with stream
+// capture the copy of that table is part of the graph and the table must stay as it is.
+cudaError_t enqueue_batch(const BatchPlan &p, BatchBuffers &b, std::map<Filter *, int> &held, unsigned wait_polls,
+                          int unsatisfiable, cudaStream_t st) {
+    cudaError_t ce = cudaEventRecord(b.ev_start, st);
+    for (auto &h : held)
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(h.first->slots[h.second].st, b.ev_start, 0);
+    for (const BatchItem &it : p.fallback) {
+        if (ce != cudaSuccess) break;
+        Filter *f = reinterpret_cast<Filter *>(p.jobs[it.job].filter);
+        Slot &s = f->slots[held.at(f)];
+        ce = run_entry_steps(f, s, *it.en, p.jobs[it.job].d_src + it.en->src_off, p.jobs[it.job].d_dst + it.en->dst_off);
+    }
+    char *arena = b.arena;
+    unsigned long long *d_next = reinterpret_cast<unsigned long long *>(arena);  // [2][2]: group, kind
+    unsigned *d_done = reinterpret_cast<unsigned *>(arena + 32);                 // [nent]
+    int *d_status = reinterpret_cast<int *>(arena + p.counters);
+    BatchEntry *d_entries = reinterpret_cast<BatchEntry *>(arena + p.counters + 256);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(arena, 0, p.counters + 256, st);
+    // accumulators start at zero
+    if (ce == cudaSuccess && p.nent > 0) ce = cudaMemsetAsync(arena + p.acc_off[0], 0, p.need - p.acc_off[0], st);
+    size_t smem[2] = {0, 0};  // per group: matching tiles
+    long long totals[2][2] = {{0, 0}, {0, 0}};  // [group] (match items, all items)
+    int idx = 0;
+    for (int g = 0; g < 2 && ce == cudaSuccess; ++g) {
+        long long nm = 0;
+        const int first = idx;
+        for (const BatchItem &it : p.groups[g]) {
+            const Filter *f = reinterpret_cast<const Filter *>(p.jobs[it.job].filter);
+            const Entry &en = *it.en;
+            const float *src = p.jobs[it.job].d_src + en.src_off;
+            BatchEntry &B = b.h_entries[idx];
+            B = BatchEntry{};
+            int2 *list = reinterpret_cast<int2 *>(arena + p.list_off[idx]);
+            unsigned long long *num = reinterpret_cast<unsigned long long *>(arena + p.acc_off[idx]);
+            unsigned long long *den = reinterpret_cast<unsigned long long *>(
+                arena + p.acc_off[idx] + align256((size_t)en.nplanes * en.plane_elems * 8));
+            MatchArgs &m = B.m;
+            m.frames = src;  // clip 0, plane 0: the matching plane
+            m.fstride = (long long)en.plane_elems;
+            m.w = en.w;
+            m.h = en.h;
+            m.pitch = en.pitch;
+            m.bs = en.bs;
+            m.range = en.range;
+            m.nbx = en.nbx;
+            m.nby = en.nby;
+            m.nbx_al = en.nbx_al;
+            m.chunks = (2 * en.range + 1 + 3) / 4;
+            m.tile_pitch = 128 + 4 * m.chunks;
+            m.list = list;
+            m.self_incl = 1;
+            FilterArgs &fa = B.f;
+            fa.src = src;
+            fa.plane_stride = (long long)en.plane_elems;
+            fa.clip_stride = (long long)en.nplanes * fa.plane_stride;
+            fa.frame_stride = (long long)en.plane_elems;
+            fa.w = en.w;
+            fa.h = en.h;
+            fa.pitch = en.pitch;
+            fa.nplanes = en.nplanes;
+            fa.chroma = f->chroma;
+            fa.list = list;
+            fa.nblocks = (int)en.nblocks;
+            for (int i = 0; i < 3; ++i) fa.sigma[i] = en.sigma[i];
+            fa.extractor = f->extractor;
+            fa.num = num;
+            fa.den = den;
+            fa.acc_frame_stride = (long long)en.plane_elems;
+            fa.acc_plane_stride = (long long)en.plane_elems;
+            const int nbw = en.bs == 4 ? 31 : 16;
+            B.tiles_x = (en.nbx_al + nbw - 1) / nbw;
+            B.match_items = B.tiles_x * ((en.nby + 3) / 4);
+            B.filter_items = (int)((en.nblocks + kBatchGroups - 1) / kBatchGroups);
+            B.first_match = nm;
+            nm += B.match_items;
+            smem[g] = std::max(smem[g], batch_match_smem(m));
+            // the clamped last column, before the batch launch (the batch's lists are complete
+            // when its filter chunks read them)
+            if (en.nbx_al != en.nbx && (ce = launch_clamped_column(m, st)) != cudaSuccess) break;
+            ++idx;
+        }
+        long long nf = nm;
+        for (int i = first; i < idx; ++i) {
+            b.h_entries[i].first_filter = nf;
+            nf += b.h_entries[i].filter_items;
+        }
+        totals[g][0] = nm;
+        totals[g][1] = nf;
+    }
+    if (ce == cudaSuccess && p.nent > 0)
+        ce = cudaMemcpyAsync(d_entries, b.h_entries, sizeof(BatchEntry) * (size_t)p.nent, cudaMemcpyHostToDevice, st);
+    for (int g = 0, base = 0; g < 2 && ce == cudaSuccess; base += (int)p.groups[g].size(), ++g) {
+        if (p.groups[g].empty()) continue;
+        BatchArgs a{};
+        a.entries = d_entries + base;
+        a.nentries = (int)p.groups[g].size();
+        a.match_total = totals[g][0];
+        a.items_total = totals[g][1];
+        a.next = d_next + 2 * g;
+        a.match_done = d_done + base;
+        a.status = d_status;
+        a.wait_polls = wait_polls ? wait_polls : (1u << 22);
+        a.unsatisfiable = unsatisfiable && g == (p.groups[0].empty() ? 1 : 0);
+        ce = launch_batch(a, g == 1, 0, 0, smem[g], batch_filter_smem(g == 1), kBatchSplit, st);
+        for (int i = 0; i < (int)p.groups[g].size() && ce == cudaSuccess; ++i) {
+            const BatchItem &it = p.groups[g][i];
+            const Entry &en = *it.en;
+            const BatchEntry &B = b.h_entries[base + i];
+            ce = launch_finish(B.f.num, B.f.den, B.f.acc_plane_stride, B.f.acc_frame_stride, en.w, en.h, en.pitch,
+                               en.nplanes, 1, en.proc_mask, p.jobs[it.job].d_dst + en.dst_off, en.pitch,
+                               (long long)en.plane_elems, 0, st);
+        }
+    }
+    for (auto &h : held) {
+        if (ce != cudaSuccess) break;
+        Slot &s = h.first->slots[h.second];
+        ce = cudaEventRecord(s.ev_up, s.st);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, s.ev_up, 0);
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(b.h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    return ce;
+}
 }  // namespace
 }  // namespace zb
 
@@ -1382,235 +1639,117 @@ size_t zb3d_dst_elems(const zb3d_filter *fp) { return reinterpret_cast<const Fil
 int zb3d_process_batch_ex(const zb3d_batch_job *jobs, int njobs, void *stream, unsigned wait_polls,
                           int unsatisfiable, char *err, size_t errlen) {
     using namespace zb;
-    if (njobs <= 0 || !jobs) {
-        set_err(err, errlen, "zb3d_process_batch: no jobs.");
-        return -1;
-    }
-    const Filter *f0 = reinterpret_cast<const Filter *>(jobs[0].filter);
-    for (int j = 0; j < njobs; ++j) {
-        const Filter *f = reinterpret_cast<const Filter *>(jobs[j].filter);
-        if (!f || f->passthrough || f->slots.empty() || !jobs[j].d_src || !jobs[j].d_dst) {
-            set_err(err, errlen, "zb3d_process_batch: job %d has no filter to run or no buffers.", j);
-            return -1;
-        }
-        if (f->device != f0->device) {
-            set_err(err, errlen, "zb3d_process_batch: the jobs' filters are on different devices.");
-            return -1;
-        }
-    }
-    const int dev = f0->device;
-    if (dev < 0 || dev >= 64) {
-        set_err(err, errlen, "zb3d_process_batch: device %d is beyond the 64 devices the batch path serves.", dev);
-        return -1;
-    }
-    cudaSetDevice(dev);
+    BatchPlan p;
+    if (!plan_batch(jobs, njobs, p, err, errlen)) return -1;
+    cudaSetDevice(p.device);
     const cudaStream_t st = (cudaStream_t)stream;
-    BatchCtx &ctx = batch_ctx(dev);
+    BatchCtx &ctx = batch_ctx(p.device);
     std::lock_guard<std::mutex> lk(ctx.mu);
-
-    // the work list: eligible entries grouped by filter step (hard threshold, Wiener)
-    struct Item {
-        int job;
-        const Entry *en;
-    };
-    std::vector<Item> groups[2], fallback;
-    for (int j = 0; j < njobs; ++j) {
-        const Filter *f = reinterpret_cast<const Filter *>(jobs[j].filter);
-        for (const Entry &en : f->entries) {
-            if (batch_eligible(f, en)) groups[f->final_ ? 1 : 0].push_back({j, &en});
-            else fallback.push_back({j, &en});
-        }
-    }
-    // scratch layout: [counters | status | entries | lists | accumulators]
-    const int nent = (int)(groups[0].size() + groups[1].size());
-    const size_t counters = align256(32 + 4 * (size_t)nent);
-    size_t need = counters + 256 + align256(sizeof(BatchEntry) * (size_t)std::max(nent, 1));
-    std::vector<size_t> list_off, acc_off;
-    for (int g = 0; g < 2; ++g)
-        for (const Item &it : groups[g]) {
-            list_off.push_back(need);
-            need += align256((size_t)it.en->nblocks * 8 * sizeof(int2));
-        }
-    for (int g = 0; g < 2; ++g)
-        for (const Item &it : groups[g]) {
-            acc_off.push_back(need);
-            need += 2 * align256((size_t)it.en->nplanes * it.en->plane_elems * 8);
-        }
-    if (need > ctx.arena_bytes) {
-        cudaStreamSynchronize(st);
-        cudaFree(ctx.arena);
-        ctx.arena = nullptr;
-        ctx.arena_bytes = 0;
-        if (cudaMalloc(&ctx.arena, need) != cudaSuccess) {
-            cudaGetLastError();
-            set_err(err, errlen, "zb3d_process_batch: out of device memory (%zu MiB of scratch).", need >> 20);
-            return -1;
-        }
-        ctx.arena_bytes = need;
-    }
-    if ((size_t)nent > ctx.h_cap || !ctx.h_status) {
-        cudaStreamSynchronize(st);
-        if (ctx.h_entries) cudaFreeHost(ctx.h_entries);
-        ctx.h_entries = nullptr;
-        ctx.h_cap = 0;
-        const size_t cap = std::max<size_t>(nent, 16);
-        if (cudaHostAlloc((void **)&ctx.h_entries, cap * sizeof(BatchEntry), cudaHostAllocDefault) != cudaSuccess ||
-            (!ctx.h_status && cudaHostAlloc((void **)&ctx.h_status, sizeof(int), cudaHostAllocDefault) != cudaSuccess)) {
-            cudaGetLastError();
-            set_err(err, errlen, "zb3d_process_batch: out of page-locked host memory.");
-            return -1;
-        }
-        ctx.h_cap = cap;
-    }
-    char *arena = ctx.arena;
-    unsigned long long *d_next = reinterpret_cast<unsigned long long *>(arena);  // [2][2]: group, kind
-    unsigned *d_done = reinterpret_cast<unsigned *>(arena + 32);                 // [nent]
-    int *d_status = reinterpret_cast<int *>(arena + counters);
-    BatchEntry *d_entries = reinterpret_cast<BatchEntry *>(arena + counters + 256);
-
-    if (!ctx.ev_start && cudaEventCreateWithFlags(&ctx.ev_start, cudaEventDisableTiming) != cudaSuccess) {
-        cudaGetLastError();
-        set_err(err, errlen, "zb3d_process_batch: cannot create an event.");
-        return -1;
-    }
-    // entries the batch kernel does not take run on their own, each filter's on the stream of
-    // one slot of that filter held for the call, after what `stream` holds so far and
-    // alongside the batch launch; `stream` waits for them at the end
-    cudaError_t ce = cudaEventRecord(ctx.ev_start, st);
-    std::map<Filter *, int> held;
-    for (const Item &it : fallback) {
-        if (ce != cudaSuccess) break;
-        Filter *f = reinterpret_cast<Filter *>(jobs[it.job].filter);
-        auto h = held.find(f);
-        if (h == held.end()) {
-            h = held.emplace(f, acquire_slot(f)).first;
-            ce = cudaStreamWaitEvent(f->slots[h->second].st, ctx.ev_start, 0);
-            if (ce != cudaSuccess) break;
-        }
-        Slot &s = f->slots[h->second];
-        ce = run_entry_steps(f, s, *it.en, jobs[it.job].d_src + it.en->src_off, jobs[it.job].d_dst + it.en->dst_off);
-    }
-    if (ce == cudaSuccess) ce = cudaMemsetAsync(arena, 0, counters + 256, st);
-    // accumulators start at zero
-    if (ce == cudaSuccess && nent > 0) ce = cudaMemsetAsync(arena + acc_off[0], 0, need - acc_off[0], st);
-    size_t smem[2] = {0, 0};  // per group: matching tiles
-    long long totals[2][2] = {{0, 0}, {0, 0}};  // [group] (match items, all items)
-    int idx = 0;
-    for (int g = 0; g < 2 && ce == cudaSuccess; ++g) {
-        long long nm = 0;
-        const int first = idx;
-        for (const Item &it : groups[g]) {
-            const Filter *f = reinterpret_cast<const Filter *>(jobs[it.job].filter);
-            const Entry &en = *it.en;
-            const float *src = jobs[it.job].d_src + en.src_off;
-            BatchEntry &B = ctx.h_entries[idx];
-            B = BatchEntry{};
-            int2 *list = reinterpret_cast<int2 *>(arena + list_off[idx]);
-            unsigned long long *num = reinterpret_cast<unsigned long long *>(arena + acc_off[idx]);
-            unsigned long long *den = reinterpret_cast<unsigned long long *>(
-                arena + acc_off[idx] + align256((size_t)en.nplanes * en.plane_elems * 8));
-            MatchArgs &m = B.m;
-            m.frames = src;  // clip 0, plane 0: the matching plane
-            m.fstride = (long long)en.plane_elems;
-            m.w = en.w;
-            m.h = en.h;
-            m.pitch = en.pitch;
-            m.bs = en.bs;
-            m.range = en.range;
-            m.nbx = en.nbx;
-            m.nby = en.nby;
-            m.nbx_al = en.nbx_al;
-            m.chunks = (2 * en.range + 1 + 3) / 4;
-            m.tile_pitch = 128 + 4 * m.chunks;
-            m.list = list;
-            m.self_incl = 1;
-            FilterArgs &fa = B.f;
-            fa.src = src;
-            fa.plane_stride = (long long)en.plane_elems;
-            fa.clip_stride = (long long)en.nplanes * fa.plane_stride;
-            fa.frame_stride = (long long)en.plane_elems;
-            fa.w = en.w;
-            fa.h = en.h;
-            fa.pitch = en.pitch;
-            fa.nplanes = en.nplanes;
-            fa.chroma = f->chroma;
-            fa.list = list;
-            fa.nblocks = (int)en.nblocks;
-            for (int i = 0; i < 3; ++i) fa.sigma[i] = en.sigma[i];
-            fa.extractor = f->extractor;
-            fa.num = num;
-            fa.den = den;
-            fa.acc_frame_stride = (long long)en.plane_elems;
-            fa.acc_plane_stride = (long long)en.plane_elems;
-            const int nbw = en.bs == 4 ? 31 : 16;
-            B.tiles_x = (en.nbx_al + nbw - 1) / nbw;
-            B.match_items = B.tiles_x * ((en.nby + 3) / 4);
-            B.filter_items = (int)((en.nblocks + kBatchGroups - 1) / kBatchGroups);
-            B.first_match = nm;
-            nm += B.match_items;
-            smem[g] = std::max(smem[g], batch_match_smem(m));
-            // the clamped last column, before the batch launch (the batch's lists are complete
-            // when its filter chunks read them)
-            if (en.nbx_al != en.nbx && (ce = launch_clamped_column(m, st)) != cudaSuccess) break;
-            ++idx;
-        }
-        long long nf = nm;
-        for (int i = first; i < idx; ++i) {
-            ctx.h_entries[i].first_filter = nf;
-            nf += ctx.h_entries[i].filter_items;
-        }
-        totals[g][0] = nm;
-        totals[g][1] = nf;
-    }
-    if (ce == cudaSuccess && nent > 0)
-        ce = cudaMemcpyAsync(d_entries, ctx.h_entries, sizeof(BatchEntry) * (size_t)nent, cudaMemcpyHostToDevice, st);
-    for (int g = 0, base = 0; g < 2 && ce == cudaSuccess; base += (int)groups[g].size(), ++g) {
-        if (groups[g].empty()) continue;
-        BatchArgs b{};
-        b.entries = d_entries + base;
-        b.nentries = (int)groups[g].size();
-        b.match_total = totals[g][0];
-        b.items_total = totals[g][1];
-        b.next = d_next + 2 * g;
-        b.match_done = d_done + base;
-        b.status = d_status;
-        b.wait_polls = wait_polls ? wait_polls : (1u << 22);
-        b.unsatisfiable = unsatisfiable && g == (groups[0].empty() ? 1 : 0);
-        ce = launch_batch(b, g == 1, 0, 0, smem[g], batch_filter_smem(g == 1), kBatchSplit, st);
-        for (int i = 0; i < (int)groups[g].size() && ce == cudaSuccess; ++i) {
-            const Item &it = groups[g][i];
-            const Entry &en = *it.en;
-            const BatchEntry &B = ctx.h_entries[base + i];
-            ce = launch_finish(B.f.num, B.f.den, B.f.acc_plane_stride, B.f.acc_frame_stride, en.w, en.h, en.pitch,
-                               en.nplanes, 1, en.proc_mask, jobs[it.job].d_dst + en.dst_off, en.pitch,
-                               (long long)en.plane_elems, 0, st);
-        }
-    }
-    for (auto &h : held) {
-        if (ce != cudaSuccess) break;
-        Slot &s = h.first->slots[h.second];
-        ce = cudaEventRecord(s.ev_up, s.st);
-        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, s.ev_up, 0);
-    }
-    if (ce == cudaSuccess) ce = cudaMemcpyAsync(ctx.h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (!ensure_buffers(ctx.buf, p, st, err, errlen)) return -1;
+    std::map<Filter *, int> held = hold_slots(p);
+    cudaError_t ce = enqueue_batch(p, ctx.buf, held, wait_polls, unsatisfiable, st);
     const cudaError_t cs = cudaStreamSynchronize(st);
     if (ce == cudaSuccess) ce = cs;
-    for (auto &h : held) {
-        cudaStreamSynchronize(h.first->slots[h.second].st);  // also on an error path
-        release_slot(h.first, h.second);
-    }
+    release_slots(held);
     if (ce != cudaSuccess) {
         set_err(err, errlen, "zb3d_process_batch: %s.", cudaGetErrorString(ce));
         return -1;
     }
-    if (*ctx.h_status != 0) {
+    if (*ctx.buf.h_status != 0) {
         set_err(err, errlen,
                 "zb3d_process_batch: a filter chunk gave up waiting for its entry's matching (status %d); the "
                 "outputs of this batch are incomplete.",
-                *ctx.h_status);
+                *ctx.buf.h_status);
         return -1;
     }
     return 0;
+}
+
+// A batch captured once into a CUDA graph with its own scratch; replays are launches.
+struct zb3d_batch {
+    zb::BatchPlan plan;
+    zb::BatchBuffers buf;
+    std::map<Filter *, int> held;
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+zb3d_batch *zb3d_batch_create(const zb3d_batch_job *jobs, int njobs, char *err, size_t errlen) {
+    using namespace zb;
+    std::unique_ptr<zb3d_batch> b(new zb3d_batch());
+    if (!plan_batch(jobs, njobs, b->plan, err, errlen)) return nullptr;
+    cudaSetDevice(b->plan.device);
+    auto fail = [&](const char *what, cudaError_t e) -> zb3d_batch * {
+        cudaGetLastError();
+        set_err(err, errlen, "zb3d_batch_create: %s (%s).", what, cudaGetErrorString(e));
+        if (b->cap) cudaStreamSynchronize(b->cap);
+        release_slots(b->held);
+        if (b->exec) cudaGraphExecDestroy(b->exec);
+        if (b->cap) cudaStreamDestroy(b->cap);
+        b->buf.release();
+        return nullptr;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail("cannot create a stream", e);
+    if (!ensure_buffers(b->buf, b->plan, b->cap, err, errlen)) {
+        cudaStreamDestroy(b->cap);
+        b->buf.release();
+        return nullptr;
+    }
+    b->held = hold_slots(b->plan);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return fail("cannot capture", e);
+    const cudaError_t e1 = enqueue_batch(b->plan, b->buf, b->held, 0, 0, b->cap);
+    e = cudaStreamEndCapture(b->cap, &g);
+    if (e1 != cudaSuccess) e = e1;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail("the batch could not be captured as a graph", e);
+    *b->buf.h_status = 0;
+    return b.release();
+}
+
+int zb3d_batch_launch(zb3d_batch *b, void *stream, char *err, size_t errlen) {
+    if (!b || !b->exec) {
+        zb::set_err(err, errlen, "zb3d_batch_launch: no batch.");
+        return -1;
+    }
+    cudaSetDevice(b->plan.device);
+    const cudaError_t e = cudaGraphLaunch(b->exec, (cudaStream_t)stream);
+    if (e != cudaSuccess) {
+        zb::set_err(err, errlen, "zb3d_batch_launch: %s.", cudaGetErrorString(e));
+        return -1;
+    }
+    return 0;
+}
+
+int zb3d_batch_status(zb3d_batch *b, char *err, size_t errlen) {
+    if (!b || !b->buf.h_status) {
+        zb::set_err(err, errlen, "zb3d_batch_status: no batch.");
+        return -1;
+    }
+    const int st = *b->buf.h_status;
+    if (st != 0) {
+        zb::set_err(err, errlen,
+                    "zb3d_batch_status: a filter chunk gave up waiting for its entry's matching (status %d); the "
+                    "outputs of the last launch are incomplete.",
+                    st);
+        return -1;
+    }
+    return 0;
+}
+
+void zb3d_batch_free(zb3d_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->plan.device);
+    if (b->cap) cudaStreamSynchronize(b->cap);
+    cudaDeviceSynchronize();  // replays may still run on the callers' streams
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    zb::release_slots(b->held);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    b->buf.release();
+    delete b;
 }
 
 int zb3d_process_batch(const zb3d_batch_job *jobs, int njobs, void *stream, char *err, size_t errlen) {

@@ -126,6 +126,10 @@ EXPORTS = {
                                c_void_p, c_void_p]),
     "zb3d_process_batch": (c_int, [c_void_p, c_int, c_void_p, c_char_p, c_size_t]),
     "zb3d_process_batch_ex": (c_int, [c_void_p, c_int, c_void_p, ctypes.c_uint, c_int, c_char_p, c_size_t]),
+    "zb3d_batch_create": (c_void_p, [c_void_p, c_int, c_char_p, c_size_t]),
+    "zb3d_batch_launch": (c_int, [c_void_p, c_void_p, c_char_p, c_size_t]),
+    "zb3d_batch_status": (c_int, [c_void_p, c_char_p, c_size_t]),
+    "zb3d_batch_free": (None, [c_void_p]),
     "zb3d_host_alloc": (c_void_p, [c_size_t]),
     "zb3d_host_free": (None, [c_void_p]),
 }

@@ -119,3 +119,38 @@ def process_batch(jobs, stream: int = 0, wait_polls: int = 0, unsatisfiable: boo
                                        err, len(err))
     if rc != 0:
         raise Error(err.value.decode())
+
+
+class Batch:
+    """A batch captured once as a CUDA graph (zb3d_batch_create): jobs = [(DeviceFilter, src_ptr,
+    dst_ptr), ...].  launch() replays it on a stream asynchronously; status() after the stream
+    was synchronised raises Error if a filter chunk of the last launch gave up waiting."""
+
+    def __init__(self, jobs):
+        arr = (N.BatchJob * len(jobs))(*[N.BatchJob(f.h, s, d) for f, s, d in jobs])
+        err = N.err_buf()
+        self.h = N.lib().zb3d_batch_create(arr, len(jobs), err, len(err))
+        if not self.h:
+            raise Error(err.value.decode())
+        self._filters = [f for f, _, _ in jobs]  # the filters outlive the batch
+
+    def launch(self, stream: int = 0):
+        err = N.err_buf()
+        if N.lib().zb3d_batch_launch(self.h, stream or None, err, len(err)) != 0:
+            raise Error(err.value.decode())
+
+    def status(self):
+        err = N.err_buf()
+        if N.lib().zb3d_batch_status(self.h, err, len(err)) != 0:
+            raise Error(err.value.decode())
+
+    def close(self):
+        if self.h:
+            N.lib().zb3d_batch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -437,7 +437,7 @@ cudaError_t run_match(Filter *f, Slot &s, const Entry &en, const float *src) {
 // fastest launch configuration of the matching stage for a plane geometry,
 // timed on this GPU.  Every candidate gives bit-identical lists, so the choice
 // never changes results.  Cache file: $ZB3D_TUNE_CACHE, else
-// $XDG_CACHE_HOME/zb3d/tune-v1.txt or ~/.cache/zb3d/tune-v1.txt; one line per key
+// $XDG_CACHE_HOME/zb3d/tune-v2.txt or ~/.cache/zb3d/tune-v2.txt; one line per key
 // "key form rows".  ZB3D_AUTOTUNE=0 turns the timing off (defaults are used).
 struct TuneCache {
     std::mutex mu;
@@ -455,9 +455,9 @@ std::string tune_path() {
     const char *p = getenv("ZB3D_TUNE_CACHE");
     if (p && *p) return p;
     const char *x = getenv("XDG_CACHE_HOME");
-    if (x && *x) return std::string(x) + "/zb3d/tune-v1.txt";
+    if (x && *x) return std::string(x) + "/zb3d/tune-v2.txt";
     const char *h = getenv("HOME");
-    if (h && *h) return std::string(h) + "/.cache/zb3d/tune-v1.txt";
+    if (h && *h) return std::string(h) + "/.cache/zb3d/tune-v2.txt";
     return "";
 }
 
@@ -488,8 +488,20 @@ void tune_store(TuneCache &c, const std::string &key, int form, int rows) {
     fclose(fp);
 }
 
+// Whether the packed SSD kernel's tile for `rows` block rows per CTA fits (that kernel
+// takes up to 8 warps; the other tiled kernels take at most 4).
+bool tiled2_rows_fit(const Entry &e, int rows) {
+    if (e.metric != M_SSD || (e.bs != 4 && e.bs != 8)) return false;
+    MatchArgs t{};
+    t.bs = e.bs;
+    t.range = e.range;
+    t.chunks = (2 * e.range + 1 + 3) / 4;
+    t.tile_pitch = 128 + 4 * t.chunks;
+    return match_tile2_bytes_rows(t, rows) <= 200 * 1024;
+}
+
 // Chooses e.form / e.rows: FP32 scan with 2 or 4 block rows per CTA (tiled block
-// steps 4 and 8; the kernels take at most 4 warps) or the tensor-core form (ssd,
+// steps 4 and 8), also 8 for the packed SSD kernel, or the tensor-core form (ssd,
 // where eligible), by timing
 // each on a synthetic plane of the entry's geometry with slot s's buffers.
 void tune_entry(Filter *f, Slot &s, Entry &e) {
@@ -506,6 +518,7 @@ void tune_entry(Filter *f, Slot &s, Entry &e) {
     if (f->match_form != 1 || !tc_ok) {
         if (tiled)
             for (int r : {2, 4}) cands.push_back({0, r});
+        if (tiled2_rows_fit(e, 8)) cands.push_back({0, 8});
     }
     if (tc_ok && f->match_form != 0) cands.push_back({1, 4});
     if (cands.size() < 2) return;
@@ -529,7 +542,7 @@ void tune_entry(Filter *f, Slot &s, Entry &e) {
     auto it = c.best.find(key);
     if (it != c.best.end()) {
         const int form = it->second.first, rows = it->second.second;
-        if ((form == 0 && (rows == 2 || rows == 4)) || (form == 1 && tc_ok)) {
+        if ((form == 0 && (rows == 2 || rows == 4 || (rows == 8 && tiled2_rows_fit(e, 8)))) || (form == 1 && tc_ok)) {
             e.form = form;
             e.rows = rows;
         }

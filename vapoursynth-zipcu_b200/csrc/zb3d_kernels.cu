@@ -330,36 +330,44 @@ __host__ __device__ constexpr int pair_pitch(int tile_pitch) {  // floats per pa
 __device__ __forceinline__ float2 f4lo(const float4 &v) { return make_float2(v.x, v.y); }
 __device__ __forceinline__ float2 f4hi(const float4 &v) { return make_float2(v.z, v.w); }
 
-// window column `col` (0..7 across the two chunk halves) of pair row k
-__device__ __forceinline__ float2 win_col(const float4 (&X)[8], const float4 (&Y)[8], int k, int col) {
-    const float4 &v = col < 4 ? ((col & 2) ? X[2 * k + 1] : X[2 * k]) : ((col & 2) ? Y[2 * k + 1] : Y[2 * k]);
-    return (col & 1) ? f4hi(v) : f4lo(v);
-}
-
+// One chunk: displacements dx = -R + 4m + s (s = 0..3) of candidate row `row`.  The
+// chunk reads window columns c0 .. c0 + 6 (c0 = the lane's tile column at dx = -R, plus
+// 4m) of the four pair rows from prow.  They are loaded one column pair at a time, just
+// before the sums that use them: column col feeds the (s, j = col - s) chains, each
+// of which runs over its pair rows k = 0..3 in order, so every sum is the reference's.
+// Keeping no window in registers holds the kernel at 116 registers.  The four distances
+// come first (no branch between their FMA chains), then the insertions in scan order;
+// a displacement past R is computed from the tile's padding columns and discarded.
 template <bool SHARED>
-__device__ __forceinline__ void tiled2_chunk(const float4 (&X)[8], const float4 (&Y)[8], int m, int R, int row,
-                                             int xb, int lo, int hi, const float2 (&nc)[4][4], float (&e)[8],
-                                             int (&q)[8]) {
-    // the chunk's four distances first (no branch between them, so their FMA chains
-    // interleave), then the insertions in scan order; a displacement past R is computed
-    // from the tile's padding columns and discarded
+__device__ __forceinline__ void tiled2_chunk(const float *prow, int pp, int c0, int m, int R, int row, int xb,
+                                             int lo, int hi, const float2 (&nc)[4][4], float (&e)[8], int (&q)[8]) {
+    float sj[4][4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        float4 v[4];  // columns (2p, 2p + 1) of pair rows k: (row 2k, row 2k + 1) of each
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(c0 + 2 * p));
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int col = 2 * p + h;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const int j = col - s;
+                if (j < 0 || j > 3) continue;
+                float2 d = __fadd2_rn(h ? f4hi(v[0]) : f4lo(v[0]), nc[0][j]);
+                float2 acc = __fmul2_rn(d, d);
+#pragma unroll
+                for (int k = 1; k < 4; ++k) {
+                    d = __fadd2_rn(h ? f4hi(v[k]) : f4lo(v[k]), nc[k][j]);
+                    acc = __ffma2_rn(d, d, acc);
+                }
+                sj[s][j] = acc.x + acc.y;
+            }
+        }
+    }
     float err[4];
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        float sj[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            float2 d = __fadd2_rn(win_col(X, Y, 0, j + s), nc[0][j]);
-            float2 acc = __fmul2_rn(d, d);
-#pragma unroll
-            for (int k = 1; k < 4; ++k) {
-                d = __fadd2_rn(win_col(X, Y, k, j + s), nc[k][j]);
-                acc = __ffma2_rn(d, d, acc);
-            }
-            sj[j] = acc.x + acc.y;
-        }
-        err[s] = (sj[0] + sj[1]) + (sj[2] + sj[3]);
-    }
+    for (int s = 0; s < 4; ++s) err[s] = (sj[s][0] + sj[s][1]) + (sj[s][2] + sj[s][3]);
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
         if constexpr (SHARED)
@@ -451,39 +459,16 @@ __device__ __forceinline__ void match_tiled2_tile(const MatchArgs &a, int bx, in
     for (int row = top; row <= bottom; ++row) {
         const int t0 = row - r0;
         const float *prow = (t0 & 1) ? tO + ((t0 - 1) >> 1) * pp : tE + (t0 >> 1) * pp;
-        // X[2k] = columns (0,1), X[2k+1] = columns (2,3) of pair row k, for the chunk's 4 columns
-        float4 A[8], B[8];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            A[2 * k] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(uo));
-            A[2 * k + 1] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(uo + 2));
-        }
-        for (int m = 0; m < chunks; m += 2) {
-            const int c1 = uo + 4 * (m + 1);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                B[2 * k] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(c1));
-                B[2 * k + 1] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(c1 + 2));
-            }
-            tiled2_chunk<SHARED>(A, B, m, R, row, xb, lo, hi, nc, e, q);
-            if (m + 1 < chunks) {
-                const int c2 = uo + 4 * (m + 2);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    A[2 * k] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(c2));
-                    A[2 * k + 1] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(c2 + 2));
-                }
-                tiled2_chunk<SHARED>(B, A, m + 1, R, row, xb, lo, hi, nc, e, q);
-            }
-        }
+        for (int m = 0; m < chunks; ++m) tiled2_chunk<SHARED>(prow, pp, uo + 4 * m, m, R, row, xb, lo, hi, nc, e, q);
     }
 
     if (!blk || (!SHARED && hh)) return;
     store_list(a, (long long)by * a.nbx + kx, xb, y, e, q);
 }
 
+// Up to 8 block rows (warps) per CTA; 2 CTAs of 8 warps fit the register file.
 template <bool SHARED, int BS>
-__global__ void __launch_bounds__(128) zb_match_tiled2(MatchArgs a) {
+__global__ void __launch_bounds__(256, 2) zb_match_tiled2(MatchArgs a) {
     extern __shared__ __align__(16) float tile[];
     match_tiled2_tile<SHARED, BS>(a, blockIdx.x, blockIdx.y, tile);
 }

@@ -195,7 +195,7 @@ int zb3d_match_device(zb3d_filter *f, int e, const float *d_src, int32_t *d_list
  * The matching configuration the autotuner chose for entry e at creation: form
  * (0 FP32 scan, 1 tensor-core) and block rows per CTA of the tiled FP32 kernels.
  * The choice is timed once per GPU and plane geometry and cached in
- * $ZB3D_TUNE_CACHE (default ~/.cache/zb3d/tune-v1.txt); ZB3D_AUTOTUNE=0 skips the
+ * $ZB3D_TUNE_CACHE (default ~/.cache/zb3d/tune-v2.txt); ZB3D_AUTOTUNE=0 skips the
  * timing.  It replaces the reference's per-configuration module cache
  * (src/bm3d.zig:57-70, 780-835).  Returns 0, or -1 for no such entry.
  */

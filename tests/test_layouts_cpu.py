@@ -1,7 +1,7 @@
 """Shared-memory layouts of the kernels, checked on the CPU.
 
-The index maps below restate the device code (csrc/zb3d_kernels.cu: pair_off and
-pair_pitch of the packed matching tile, move_tr / move_bc / move_cd and the Wiener
+The index maps below restate the device code (csrc/zb3d_kernels.cu: split_off and
+tile2_g of the packed matching tile, move_tr / move_bc / move_cd and the Wiener
 coefficient buffer of zb_filter16; csrc/zb3d_dct_tc.cu: kmaj and the staging order).
 For every map these tests check the properties that the kernels rely on:
 
@@ -28,31 +28,44 @@ def conflict_free_words(addrs):
 
 
 # ---------------------------------------------------------------------------
-# packed FP32x2 matching tile: pair rows of 16-byte chunks, chunk c at c ^ ((c >> 3) & 1)
+# packed FP32x2 matching tile: pair rows of two half-planes of g 16-byte chunks
 # ---------------------------------------------------------------------------
-def pair_off(col):
-    c = col >> 1
-    return 4 * (c ^ ((c >> 3) & 1)) + 2 * (col & 1)
+TILE2_G = 40
 
 
-def pair_pitch(tp):
-    return (2 * tp + 31) & ~31
+def tile2_g(tp, chunks):
+    return TILE2_G if chunks <= (4 * TILE2_G - 128) // 4 else tp // 4
 
 
-@pytest.mark.parametrize("bm_range", [1, 4, 9, 12, 16, 24])
-def test_matching_tile_swizzle(bm_range):
+def split_off(col, g):
+    return ((col >> 1) & 1) * 4 * g + 4 * (col >> 2) + 2 * (col & 1)
+
+
+@pytest.mark.parametrize("bm_range", [1, 4, 9, 12, 15, 16, 24, 40])
+@pytest.mark.parametrize("block_step", [4, 8])
+def test_matching_tile_split_layout(bm_range, block_step):
     chunks = (2 * bm_range + 1 + 3) // 4
     tp = 128 + 4 * chunks
-    offs = [pair_off(c) for c in range(tp)]
-    assert len(set(offs)) == tp
-    assert max(offs) + 2 <= pair_pitch(tp) and pair_pitch(tp) % 32 == 0
+    g = tile2_g(tp, chunks)
+    pp = 8 * g
+    assert g >= tp // 4 and (pp * 4) % 16 == 0
+    offs = [split_off(c, g) for c in range(tp)]
+    assert len(set(offs)) == tp and max(offs) + 2 <= pp
     for c in range(0, tp, 2):  # a float4 holds columns c, c + 1 of a row pair
-        assert pair_off(c) % 4 == 0 and pair_off(c + 1) == pair_off(c) + 2
-    # lane l reads the float4 of columns 4 l + off (and + 2): 8 lanes per 16-byte phase
-    for off in range(0, tp - 128, 2):
-        for phase in range(4):
-            quads = {(pair_off(4 * lane + off) // 4) % 8 for lane in range(8 * phase, 8 * phase + 8)}
-            assert len(quads) == 8
+        assert split_off(c, g) % 4 == 0 and split_off(c + 1, g) == split_off(c, g) + 2
+    # lane tile column at dx = -R: 4 b (shared halves, block_step 4) or 8 b + 4 hh (block_step 8)
+    uo = [4 * l for l in range(32)] if block_step == 4 else [8 * (l >> 1) + 4 * (l & 1) for l in range(32)]
+    assert all(u % 4 == 0 for u in uo)
+    for m in range(chunks):
+        for p in range(4):
+            # the kernel's address: column uo + 4 m + 2 p, as (uo + 4 m) + (p & 1) 4 g + 4 (p >> 1)
+            cols = [u + 4 * m + 2 * p for u in uo]
+            assert all(c + 1 < tp for c in cols)
+            got = [u + 4 * m + (p & 1) * 4 * g + 4 * (p >> 1) for u in uo]
+            assert got == [split_off(c, g) for c in cols]
+            for phase in range(4):  # 16-byte loads: 8 lanes per phase, distinct bank quads
+                quads = {(got[l] // 4) % 8 for l in range(8 * phase, 8 * phase + 8)}
+                assert len(quads) == 8
 
 
 # ---------------------------------------------------------------------------

@@ -312,41 +312,50 @@ __global__ void __launch_bounds__(128) zb_match_tiled(MatchArgs a) {
 // and odd-row partial sums, which advance together: acc = fma2(d, d, acc)
 // computes the reference's e0 and e1 chains in one instruction and acc.x + acc.y
 // is their join.  d = n + (-c) = -(c - n) exactly, so d*d is the reference's
-// square.  A pair row is a run of 16-byte chunks (two columns each), 128-byte
-// aligned; chunk c sits at c ^ ((c >> 3) & 1), so in the odd 128-byte lines of a
-// row the chunks of a pair swap places.  Eight lanes reading every second chunk
-// from any start then hit eight distinct bank quads: their float4 loads do not
-// collide on banks.
+// square.  A pair row holds the tile's columns as 16-byte chunks of two columns
+// each, in two half-planes of g chunks: columns 4u, 4u+1 form chunk u of the first,
+// columns 4u+2, 4u+3 chunk u of the second.  A lane's block half starts at a column
+// that is a multiple of 4, so at every step the lanes of a quarter warp read eight
+// consecutive chunks of one half-plane (float4 loads free of bank conflicts), and a
+// lane's address advances by one chunk per displacement chunk.  With g fixed at
+// compile time (kTile2G, for up to 8 chunks of displacements: bm_range <= 15) every
+// other offset is an immediate.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int pair_off(int col) {  // float offset of column `col` in a pair row
-    const int c = col >> 1;
-    return 4 * (c ^ ((c >> 3) & 1)) + 2 * (col & 1);
+constexpr int kTile2G = 40;  // half-plane chunks of the fixed layout (tile pitch <= 160)
+
+__host__ __device__ constexpr int tile2_g(int tile_pitch, bool fixed) {  // chunks per half-plane
+    return fixed ? kTile2G : tile_pitch / 4;
 }
 
-__host__ __device__ constexpr int pair_pitch(int tile_pitch) {  // floats per pair row
-    return (2 * tile_pitch + 31) & ~31;
-}
+__host__ __device__ constexpr bool tile2_fixed(int chunks) { return chunks <= (4 * kTile2G - 128) / 4; }
+
+// float offset of column `col` in a pair row of half-plane size g
+__device__ __forceinline__ int split_off(int col, int g) { return ((col >> 1) & 1) * 4 * g + 4 * (col >> 2) + 2 * (col & 1); }
 
 __device__ __forceinline__ float2 f4lo(const float4 &v) { return make_float2(v.x, v.y); }
 __device__ __forceinline__ float2 f4hi(const float4 &v) { return make_float2(v.z, v.w); }
 
 // One chunk: displacements dx = -R + 4m + s (s = 0..3) of candidate row `row`.  The
 // chunk reads window columns c0 .. c0 + 6 (c0 = the lane's tile column at dx = -R, plus
-// 4m) of the four pair rows from prow.  They are loaded one column pair at a time, just
+// 4m; a multiple of 4) of the four pair rows; pc points at column c0 of the first pair
+// row.  GF: half-plane chunks when fixed at compile time, else 0 (pp_rt and g_rt give
+// the pitch and half-plane size).  The columns are loaded one column pair at a time, just
 // before the sums that use them: column col feeds the (s, j = col - s) chains, each
 // of which runs over its pair rows k = 0..3 in order, so every sum is the reference's.
 // Keeping no window in registers holds the kernel at 116 registers.  The four distances
 // come first (no branch between their FMA chains), then the insertions in scan order;
 // a displacement past R is computed from the tile's padding columns and discarded.
-template <bool SHARED>
-__device__ __forceinline__ void tiled2_chunk(const float *prow, int pp, int c0, int m, int R, int row, int xb,
+template <bool SHARED, int GF>
+__device__ __forceinline__ void tiled2_chunk(const float *pc, int pp_rt, int g_rt, int m, int R, int row, int xb,
                                              int lo, int hi, const float2 (&nc)[4][4], float (&e)[8], int (&q)[8]) {
+    const int pp = GF ? 8 * GF : pp_rt, g = GF ? GF : g_rt;
     float sj[4][4];
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
         float4 v[4];  // columns (2p, 2p + 1) of pair rows k: (row 2k, row 2k + 1) of each
 #pragma unroll
-        for (int k = 0; k < 4; ++k) v[k] = *reinterpret_cast<const float4 *>(prow + k * pp + pair_off(c0 + 2 * p));
+        for (int k = 0; k < 4; ++k)
+            v[k] = *reinterpret_cast<const float4 *>(pc + k * pp + (p & 1) * 4 * g + 4 * (p >> 1));
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int col = 2 * p + h;
@@ -385,12 +394,12 @@ __device__ __forceinline__ void tiled2_chunk(const float *prow, int pp, int c0, 
 // One tile of the packed FP32x2 SSD matcher: block columns [31 bx, 31 bx + 31) (SHARED)
 // or [16 bx, ...), block rows [nw by, nw by + nw), nw = the CTA's warps; `tile` is the
 // dynamic shared-memory tile (match_tile2_bytes).
-template <bool SHARED, int BS>
-__device__ __forceinline__ void match_tiled2_tile(const MatchArgs &a, int bx, int by_cta, float *tile) {
+template <bool SHARED, int BS, bool FIXED>
+__device__ __forceinline__ void match_tiled2_tile_g(const MatchArgs &a, int bx, int by_cta, float *tile) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     constexpr int NBW = SHARED ? 31 : 16;
     const int R = a.range, W = a.w, H = a.h, tp = a.tile_pitch;
-    const int pp = pair_pitch(tp);
+    const int g = tile2_g(tp, FIXED), pp = 8 * g;
     const int kx0 = bx * NBW;
     const int x0 = kx0 * BS;
     const int by0 = by_cta * nw;
@@ -412,9 +421,9 @@ __device__ __forceinline__ void match_tiled2_tile(const MatchArgs &a, int bx, in
             for (int c = lane; c < tp; c += 32) {
                 const int gx = gx0 + c;
                 const bool ok = gx >= 0 && gx < W;
-                const float *g = srow + (ok ? gx : 0);
-                cp_async_f32(de + pair_off(c), g, ok);
-                if (dq) cp_async_f32(dq + pair_off(c), g, ok);
+                const float *gs = srow + (ok ? gx : 0);
+                cp_async_f32(de + split_off(c, g), gs, ok);
+                if (dq) cp_async_f32(dq + split_off(c, g), gs, ok);
             }
         }
     }
@@ -428,7 +437,7 @@ __device__ __forceinline__ void match_tiled2_tile(const MatchArgs &a, int bx, in
     const int hh = SHARED ? 0 : (lane & 1);
     const int kx = kx0 + b;
     const int xb = BS * kx;
-    const int uo = BS * b + 4 * hh;  // tile column of this half at dx = -R (even)
+    const int uo = BS * b + 4 * hh;  // tile column of this half at dx = -R (a multiple of 4)
     const bool blk = (SHARED ? lane < 31 : true) && kx < a.nbx_al;
 
     // negated reference half as row pairs (2k, 2k+1) of each of its 4 columns
@@ -440,7 +449,7 @@ __device__ __forceinline__ void match_tiled2_tile(const MatchArgs &a, int bx, in
         for (int k = 0; k < 4; ++k)
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const float2 v = *reinterpret_cast<const float2 *>(base + k * pp + pair_off(uo + R + j));
+                const float2 v = *reinterpret_cast<const float2 *>(base + k * pp + split_off(uo + R + j, g));
                 nc[k][j] = make_float2(-v.x, -v.y);
             }
     }
@@ -459,11 +468,22 @@ __device__ __forceinline__ void match_tiled2_tile(const MatchArgs &a, int bx, in
     for (int row = top; row <= bottom; ++row) {
         const int t0 = row - r0;
         const float *prow = (t0 & 1) ? tO + ((t0 - 1) >> 1) * pp : tE + (t0 >> 1) * pp;
-        for (int m = 0; m < chunks; ++m) tiled2_chunk<SHARED>(prow, pp, uo + 4 * m, m, R, row, xb, lo, hi, nc, e, q);
+        const float *pc = prow + uo;  // column uo: chunk uo / 4 of the first half-plane
+        for (int m = 0; m < chunks; ++m, pc += 4)
+            tiled2_chunk<SHARED, FIXED ? kTile2G : 0>(pc, pp, g, m, R, row, xb, lo, hi, nc, e, q);
     }
 
     if (!blk || (!SHARED && hh)) return;
     store_list(a, (long long)by * a.nbx + kx, xb, y, e, q);
+}
+
+// The tile with the fixed half-plane size where the displacements allow it.
+template <bool SHARED, int BS>
+__device__ __forceinline__ void match_tiled2_tile(const MatchArgs &a, int bx, int by_cta, float *tile) {
+    if (tile2_fixed(a.chunks))
+        match_tiled2_tile_g<SHARED, BS, true>(a, bx, by_cta, tile);
+    else
+        match_tiled2_tile_g<SHARED, BS, false>(a, bx, by_cta, tile);
 }
 
 // Up to 8 block rows (warps) per CTA; 2 CTAs of 8 warps fit the register file.
@@ -1071,7 +1091,8 @@ static cudaError_t launch_tiled_t(const MatchArgs &a, int rows_per_cta, cudaStre
 
 // packed FP32x2 SSD kernel: two pair-interleaved copies of the tile (swizzled pair rows)
 static size_t match_tile2_bytes(const MatchArgs &a, int rows_per_cta) {
-    return (size_t)((rows_per_cta - 1) * a.bs + 2 * a.range + 8) * pair_pitch(a.tile_pitch) * sizeof(float);
+    return (size_t)((rows_per_cta - 1) * a.bs + 2 * a.range + 8) * 8 * tile2_g(a.tile_pitch, tile2_fixed(a.chunks)) *
+           sizeof(float);
 }
 
 template <bool SHARED, int BS>

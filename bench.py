@@ -820,6 +820,76 @@ def run_dct_tf32(torch, steps: int, warmup: int):
     return out
 
 
+def run_match1080(torch, steps: int, warmup: int):
+    """Block matching alone, the dominant kernel of the metric's workload: the Y, U and V
+    entries of a 1920x1080 YUV420 BM3Dv2 filter (block_step 4, bm_range 12), each matched
+    with the configuration the autotuner chose (zb3d_match_device), timed per launch with
+    CUDA events on the launching stream.  The plane stays resident in L2 between launches
+    (the kernel reads it once per launch and is bound by arithmetic, not by HBM)."""
+    from zb3d import _native as N
+    from zb3d import synth
+    from zb3d.device import DeviceFilter
+    f = DeviceFilter(W, H, family=N.YUV, subsampling=(1, 1), num_streams=1, **KW)
+    src = np.zeros(f.src_elems, np.float32)
+    lists, flops, names = [], [], []
+    for e, lay in enumerate(f.entries):
+        view = src[lay.src_offset:lay.src_offset + lay.src_elems].reshape(lay.height, lay.pitch)
+        view[:, :lay.width] = synth.noisy_plane(lay.width, lay.height, SIGMA, plane=e)
+        nbx = (lay.width - 8 + BLOCK_STEP - 1) // BLOCK_STEP + 1
+        nby = (lay.height - 8 + BLOCK_STEP - 1) // BLOCK_STEP + 1
+        lists.append(torch.zeros((nby, nbx, 8, 2), dtype=torch.int32, device="cuda"))
+        flops.append(match_flops(lay.width, lay.height, BLOCK_STEP, BM_RANGE))
+        names.append(f"{'YUV'[e]} {lay.width}x{lay.height}")
+    d_src = torch.from_numpy(src).cuda()
+    st = torch.cuda.Stream()
+    torch.cuda.synchronize()
+
+    def step(rec=None):
+        for e in range(len(lists)):
+            a = torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            f.match(e, d_src.data_ptr(), lists[e].data_ptr(), st.cuda_stream)
+            z = torch.cuda.Event(enable_timing=True)
+            z.record(st)
+            if rec is not None:
+                rec.append((e, a, z))
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    rec = []
+    g0 = torch.cuda.Event(enable_timing=True)
+    g0.record(st)
+    for _ in range(steps):
+        step(rec)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g1.record(st)
+    g1.synchronize()
+    ms = g0.elapsed_time(g1) / steps
+    per = {}
+    for e, a, z in rec:
+        per.setdefault(e, []).append(a.elapsed_time(z))
+    planes = {}
+    for e in per:
+        t = float(np.median(per[e]))
+        form, rows = f.tuning(e)
+        planes[names[e]] = {"ms": t, "TFLOP_per_s": flops[e] / t / 1e9, "form": FORM_KEYS.get(form, form),
+                            "rows_per_cta": rows}
+    peak = 148 * 128 * 2 * 1965e6 / 1e12
+    achieved = sum(flops) / (ms / 1e3) / 1e12
+    f.close()
+    return {"metric": "block matching of one 1920x1080 YUV420 frame (Y, U, V), luma Mpix/s", "unit": "Mpix/s",
+            "value": W * H / (ms / 1e3) / 1e6, "ms_per_step": ms, "steps": steps, "warmup": warmup,
+            "planes": planes,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "how": "192 FLOP per candidate over every block's clipped window, 3 launches per step "
+                                "/ CUDA-event time; peak: 148 SMs x 128 FP32 lanes x 2 x 1965 MHz (nominal)"},
+            "config": {"workload": "zb3d_match_device on the Y, U and V entries of BM3Dv2 YUV420 1920x1080 / "
+                                   "960x540, block_step 4, bm_range 12, ssd; autotuned configuration",
+                       "l2": "plane resident in L2 between launches (arithmetic-bound kernel)"}}
+
+
 def run_batched(torch, steps: int, warmup: int, nstreams: int = 4):
     """Uneven batch: 720x480, 1280x720 and 3840x2160 clips of 16 frames, YUV420 per plane or
     YUV444 CBM3D (chroma=1, matched on Y), radius 0 or 1 (stacked output), sigma drawn per
@@ -1030,7 +1100,8 @@ def main():
     ap.add_argument("--precision", action="store_true",
                     help="vbm3d: the precision form of the filter (2D transforms on the tensor cores, split TF32), "
                          "with its error against the plain form and the FP64 oracle")
-    ap.add_argument("--workload", choices=["twopass1080", "vbm3d", "gray640", "batched", "pilot4k", "dct_tf32"],
+    ap.add_argument("--workload", choices=["twopass1080", "vbm3d", "gray640", "batched", "pilot4k", "dct_tf32",
+                                           "match1080"],
                     default="twopass1080",
                     help="twopass1080 is the metric's workload; the others print their own line")
     args = ap.parse_args()
@@ -1048,7 +1119,7 @@ def main():
     torch.cuda.set_device(local)
     if args.workload != "twopass1080":
         fn = {"vbm3d": run_vbm3d, "gray640": run_gray640, "batched": run_batched, "pilot4k": run_pilot4k,
-              "dct_tf32": run_dct_tf32}[args.workload]
+              "dct_tf32": run_dct_tf32, "match1080": run_match1080}[args.workload]
         out = fn(torch, args.steps, args.warmup, filter_form=1) if args.precision and args.workload == "vbm3d" \
             else fn(torch, args.steps, args.warmup)
         for k, v in {"n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic"}.items():

@@ -59,7 +59,7 @@ struct BatchEntry {
     MatchArgs m;                      // tile_pitch, chunks and self_incl set; bs 4 or 8
     FilterArgs f;
     int tiles_x;                      // match tiles per tile row (31 or 16 block columns each)
-    int match_items;                  // match tiles (4 block rows each)
+    int match_items;                  // match tiles (kBatchMatchRows block rows each)
     int filter_items;                 // filter chunks (kBatchGroups groups each)
     long long first_match, first_filter;  // first item number of each kind
 };
@@ -76,6 +76,7 @@ struct BatchArgs {
 };
 
 constexpr int kBatchGroups = 128;     // groups per filter chunk
+constexpr int kBatchMatchRows = 8;    // block rows (warps) per match tile
 
 // Fixed-point scale of the accumulators: value * 2^32 held in a signed 64-bit sum.
 constexpr float kFixScale = 4294967296.0f;

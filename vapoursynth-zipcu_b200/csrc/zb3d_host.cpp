@@ -44,7 +44,7 @@ size_t match_tile2_bytes_rows(const MatchArgs &a, int rows_per_cta);
 size_t batch_match_smem(const MatchArgs &m);
 size_t batch_filter_smem(bool final_);
 cudaError_t launch_batch(BatchArgs b, bool final_, int t2d, int t1d, size_t match_smem, size_t filter_smem,
-                         bool split, cudaStream_t st);
+                         cudaStream_t st);
 cudaError_t launch_clamped_column(MatchArgs a, cudaStream_t st);
 cudaError_t filter_precision_init(int dev);
 size_t filter_precision_stack_floats(long long nblocks);
@@ -919,12 +919,6 @@ BatchCtx &batch_ctx(int dev) {
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// The batch's match items and filter items run as two stream-ordered persistent launches,
-// each kernel with the register budget of its own work (the matcher needs about 168
-// registers, the filter 72); the filter chunks still check, bounded, that their entry's
-// matching is complete.
-constexpr bool kBatchSplit = true;
-
 // Entries the batch kernel takes: spatial SSD matching at block_step 4 or 8 on the FP32
 // scan with the tiled kernel, radius 0, DCT in both dimensions, no pilot.
 bool batch_eligible(const Filter *f, const Entry &en) {
@@ -937,7 +931,7 @@ bool batch_eligible(const Filter *f, const Entry &en) {
     m.range = en.range;
     m.chunks = (2 * en.range + 1 + 3) / 4;
     m.tile_pitch = 128 + 4 * m.chunks;
-    return match_tile2_bytes_rows(m, 4) <= 200 * 1024;
+    return match_tile2_bytes_rows(m, kBatchMatchRows) <= 200 * 1024;
 }
 
 
@@ -1133,7 +1127,7 @@ cudaError_t enqueue_batch(const BatchPlan &p, BatchBuffers &b, std::map<Filter *
             fa.acc_plane_stride = (long long)en.plane_elems;
             const int nbw = en.bs == 4 ? 31 : 16;
             B.tiles_x = (en.nbx_al + nbw - 1) / nbw;
-            B.match_items = B.tiles_x * ((en.nby + 3) / 4);
+            B.match_items = B.tiles_x * ((en.nby + kBatchMatchRows - 1) / kBatchMatchRows);
             B.filter_items = (int)((en.nblocks + kBatchGroups - 1) / kBatchGroups);
             B.first_match = nm;
             nm += B.match_items;
@@ -1165,7 +1159,7 @@ cudaError_t enqueue_batch(const BatchPlan &p, BatchBuffers &b, std::map<Filter *
         a.status = d_status;
         a.wait_polls = wait_polls ? wait_polls : (1u << 22);
         a.unsatisfiable = unsatisfiable && g == (p.groups[0].empty() ? 1 : 0);
-        ce = launch_batch(a, g == 1, 0, 0, smem[g], batch_filter_smem(g == 1), kBatchSplit, st);
+        ce = launch_batch(a, g == 1, 0, 0, smem[g], batch_filter_smem(g == 1), st);
         for (int i = 0; i < (int)p.groups[g].size() && ce == cudaSuccess; ++i) {
             const BatchItem &it = p.groups[g][i];
             const Entry &en = *it.en;

@@ -1015,12 +1015,19 @@ __device__ __forceinline__ int batch_entry_of(const BatchArgs &b, long long item
 // PHASE 0: the whole list in one launch; 1: match items only; 2: filter items only (the
 // items of the other kind are skipped, so two stream-ordered launches cover the list, each
 // kernel with the register budget of its own kind of work).
+// PHASE 1: the match tiles (kBatchMatchRows warps per CTA); PHASE 2: the filter chunks
+// (4 warps per CTA).  Each phase is one persistent launch with its own register budget;
+// the filter phase's occupancy hint (5 CTAs per SM hard, 6 Wiener, as shared memory
+// allows) gives it the registers of the per-window filter kernels (96 / 80), where the
+// compiler's own choice (72 / 64 with a spill) ran its chunks about 1.4x slower.
 template <bool FINAL, int T2D, int T1D, int PHASE>
-__global__ void __launch_bounds__(128) zb_batch(BatchArgs b) {
+__global__ void __launch_bounds__(PHASE == 1 ? kBatchMatchRows * 32 : 128, PHASE == 1 ? 2 : (FINAL ? 6 : 5))
+    zb_batch(BatchArgs b) {
     extern __shared__ __align__(16) float dyn[];  // matching tile, or the Wiener coefficient buffer
     __shared__ float tbuf[PHASE == 1 ? 1 : kFilterWarps * 2 * kGroupBuf];
     __shared__ long long s_item;
     __shared__ int s_ok;
+    static_assert(PHASE == 1 || PHASE == 2, "match phase or filter phase");
     const long long first = PHASE == 2 ? b.match_total : 0;
     const long long last = PHASE == 1 ? b.match_total : b.items_total;
     for (;;) {
@@ -1029,8 +1036,7 @@ __global__ void __launch_bounds__(128) zb_batch(BatchArgs b) {
         __syncthreads();
         const long long item = s_item;
         if (item >= last) break;
-        if constexpr (PHASE == 2) {
-        } else if (item < b.match_total) {
+        if constexpr (PHASE == 1) {
             const int e = batch_entry_of(b, item, false);
             const BatchEntry &E = b.entries[e];
             const int local = (int)(item - E.first_match);
@@ -1042,9 +1048,7 @@ __global__ void __launch_bounds__(128) zb_batch(BatchArgs b) {
             __threadfence();  // each thread's list stores before the tile's count
             __syncthreads();
             if (threadIdx.x == 0) atomicAdd(&b.match_done[e], 1u);
-            continue;
-        }
-        if constexpr (PHASE != 1) {
+        } else {
             const int e = batch_entry_of(b, item, true);
             const BatchEntry &E = b.entries[e];
             if (threadIdx.x == 0) {
@@ -1065,6 +1069,7 @@ __global__ void __launch_bounds__(128) zb_batch(BatchArgs b) {
             if (!s_ok) continue;  // this chunk is left out; the status tells the host
             __threadfence();      // the count before the lists, for every reading thread
             const long long g0 = (item - E.first_filter) * kBatchGroups;
+#pragma unroll 1
             for (int g = 0; g < kBatchGroups; g += 128 / 16)
                 filter16_groups<FINAL, T2D, T1D>(E.f, g0 + g, tbuf, dyn);
         }
@@ -1270,38 +1275,36 @@ cudaError_t launch_clamped_column(MatchArgs a, cudaStream_t st) {
 
 size_t match_tile2_bytes_rows(const MatchArgs &a, int rows_per_cta) { return match_tile2_bytes(a, rows_per_cta); }
 
-// Bytes of dynamic shared memory a batch entry needs: its matching tile (4 block rows),
-// and the Wiener coefficient buffer of its filter chunks.
-size_t batch_match_smem(const MatchArgs &m) { return match_tile2_bytes(m, 4); }
+// Bytes of dynamic shared memory a batch entry needs: its matching tile (kBatchMatchRows
+// block rows), and the Wiener coefficient buffer of its filter chunks.
+size_t batch_match_smem(const MatchArgs &m) { return match_tile2_bytes(m, kBatchMatchRows); }
 size_t batch_filter_smem(bool final_) { return final_ ? (size_t)(128 / 16) * kCoeffBuf * sizeof(float) : 0; }
 
 template <class K>
-static cudaError_t launch_batch_k(K k, const BatchArgs &b, size_t smem, cudaStream_t st) {
+static cudaError_t launch_batch_k(K k, const BatchArgs &b, int threads, size_t smem, cudaStream_t st) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148, per = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, 128, smem) != cudaSuccess || per < 1) per = 1;
-    k<<<sms * per, 128, smem, st>>>(b);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, threads, smem) != cudaSuccess || per < 1) per = 1;
+    k<<<sms * per, threads, smem, st>>>(b);
     return cudaGetLastError();
 }
 
 // The batch kernels for the filter kind (final, t2d, t1d); only the DCT in both dimensions
-// is built in (other kinds run entry by entry).  split: the match items and the filter
-// items as two launches (b.next must point at two counters), else the whole list in one.
+// is built in (other kinds run entry by entry).  The match items and the filter items run as
+// two stream-ordered persistent launches (b.next must point at two counters); the filter
+// chunks still check, bounded, that their entry's matching is complete.
 // match_smem / filter_smem: dynamic shared memory of each kind of item.
 cudaError_t launch_batch(BatchArgs b, bool final_, int t2d, int t1d, size_t match_smem, size_t filter_smem,
-                         bool split, cudaStream_t st) {
+                         cudaStream_t st) {
     if (t2d != T_DCT || t1d != T_DCT) return cudaErrorNotSupported;
-    if (!split)
-        return launch_batch_k(final_ ? zb_batch<true, T_DCT, T_DCT, 0> : zb_batch<false, T_DCT, T_DCT, 0>, b,
-                              std::max(match_smem, filter_smem), st);
     cudaError_t e = launch_batch_k(final_ ? zb_batch<true, T_DCT, T_DCT, 1> : zb_batch<false, T_DCT, T_DCT, 1>, b,
-                                   match_smem, st);
+                                   kBatchMatchRows * 32, match_smem, st);
     if (e != cudaSuccess) return e;
     b.next += 1;
-    return launch_batch_k(final_ ? zb_batch<true, T_DCT, T_DCT, 2> : zb_batch<false, T_DCT, T_DCT, 2>, b,
+    return launch_batch_k(final_ ? zb_batch<true, T_DCT, T_DCT, 2> : zb_batch<false, T_DCT, T_DCT, 2>, b, 128,
                           filter_smem > 0 ? filter_smem : 16, st);
 }
 

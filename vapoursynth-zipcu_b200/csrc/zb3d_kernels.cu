@@ -531,6 +531,60 @@ __device__ __forceinline__ void scan_window(const float *__restrict__ plane, int
     }
 }
 
+// The same scan for SSD on packed FP32x2 arithmetic: the ring holds rows (2k, 2k+1) of
+// each of its 4 columns as a float2, nc the negated reference half in the same pairs, and
+// one __ffma2_rn advances the even-row and the odd-row chain of a column together (each
+// with its own rounding), so every distance is half_distance<M_SSD>'s; n + (-c) is
+// exactly -(c - n), so the squares are the same.
+__device__ __forceinline__ void scan_window_ssd2(const float *__restrict__ plane, int pitch, int left, int right,
+                                                 int top, int bottom, const float2 (&nc)[4][4], unsigned pm,
+                                                 float (&e)[8], int (&q)[8]) {
+    for (int row = top; row <= bottom; ++row) {
+        const float *rp = plane + (long long)row * pitch;
+        float2 w[4][4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                w[k][j] = make_float2(__ldg(rp + 2 * k * pitch + left + j), __ldg(rp + (2 * k + 1) * pitch + left + j));
+        for (int col = left; col <= right; col += 4) {
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const int cc = col + s;
+                if (cc > right) break;
+                float sj[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float2 d = __fadd2_rn(w[0][(s + j) & 3], nc[0][j]);
+                    float2 acc = __fmul2_rn(d, d);
+#pragma unroll
+                    for (int k = 1; k < 4; ++k) {
+                        d = __fadd2_rn(w[k][(s + j) & 3], nc[k][j]);
+                        acc = __ffma2_rn(d, d, acc);
+                    }
+                    sj[j] = acc.x + acc.y;
+                }
+                const float hd = (sj[0] + sj[1]) + (sj[2] + sj[3]);
+                const float err = hd + __shfl_xor_sync(pm, hd, 1);
+                if (err < e[7]) top8_insert(e, q, err, pack_pos(cc, row));
+                if (cc + 1 <= right) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        w[k][s] = make_float2(__ldg(rp + 2 * k * pitch + cc + 4), __ldg(rp + (2 * k + 1) * pitch + cc + 4));
+                }
+            }
+        }
+    }
+}
+
+// The negated reference half as row pairs (2k, 2k+1) of each of its 4 columns.
+__device__ __forceinline__ void neg_pairs(const float (&c)[8][4], float2 (&nc)[4][4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) nc[k][j] = make_float2(-c[2 * k][j], -c[2 * k + 1][j]);
+}
+
 // Spatial matching for any block_step (and for the clamped last block column of
 // the tiled kernel), reading candidates through the L1/L2 path.  Lane pair per block.
 template <int M>
@@ -570,7 +624,15 @@ __global__ void __launch_bounds__(128) zb_match_global(MatchArgs a) {
         e[i] = ZB_FLT_MAX;
         q[i] = 0;
     }
-    scan_window<M>(plane, a.pitch, max(x - R, 0), min(x + R, W - 8), max(y - R, 0), min(y + R, H - 8), c, st, pm, e, q);
+    if constexpr (M == M_SSD) {
+        float2 nc[4][4];
+        neg_pairs(c, nc);
+        scan_window_ssd2(plane, a.pitch, max(x - R, 0), min(x + R, W - 8), max(y - R, 0), min(y + R, H - 8), nc, pm,
+                         e, q);
+    } else {
+        scan_window<M>(plane, a.pitch, max(x - R, 0), min(x + R, W - 8), max(y - R, 0), min(y + R, H - 8), c, st, pm,
+                       e, q);
+    }
     if (hh) return;
     const long long bi = (long long)by * a.nbx + kx;
     const int self = pack_pos(x, y);
@@ -605,7 +667,7 @@ __global__ void __launch_bounds__(128) zb_match_global(MatchArgs a) {
 // ps_num entries are merged into the block's list.
 // ---------------------------------------------------------------------------
 template <int M>
-__global__ void __launch_bounds__(128) zb_match_temporal(MatchArgs a) {
+__global__ void __launch_bounds__(128, M == M_SSD ? 4 : 3) zb_match_temporal(MatchArgs a) {
     const int lane = threadIdx.x & 31;
     const long long pair = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 1;
     const int hh = lane & 1;
@@ -623,22 +685,27 @@ __global__ void __launch_bounds__(128) zb_match_temporal(MatchArgs a) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) c[i][j] = __ldg(centre + (long long)(y + i) * a.pitch + x + j);
     const float st = ref_stat<M>(c, pm);
+    float2 nc[4][4];
+    if constexpr (M == M_SSD) neg_pairs(c, nc);
 
     float ge[8];
-    int gq[8], gz[8], sq[8];
+    int gq[8], gz[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const int2 v = a.list[pair * 8 + i];
         ge[i] = a.errs[pair * 8 + i];
         gq[i] = pack_pos(v.x, v.y & 0xffffff);
         gz[i] = r;
-        sq[i] = gq[i];
     }
 #pragma unroll 1
     for (int dir = -1; dir <= 1; dir += 2) {
+        // each direction starts from the spatial list (still unchanged in memory)
         int lq[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) lq[i] = sq[i];
+        for (int i = 0; i < 8; ++i) {
+            const int2 v = a.list[pair * 8 + i];
+            lq[i] = pack_pos(v.x, v.y & 0xffffff);
+        }
 #pragma unroll 1
         for (int t = 1; t <= r; ++t) {
             const int zt = r + dir * t;
@@ -654,8 +721,12 @@ __global__ void __launch_bounds__(128) zb_match_temporal(MatchArgs a) {
             for (int i = 0; i < 8; ++i) {
                 if (i < a.ps_num) {
                     const int xx = pos_x(lq[i]), yy = pos_y(lq[i]);
-                    scan_window<M>(fp, a.pitch, max(xx - P, 0), min(xx + P, W - 8), max(yy - P, 0),
-                                   min(yy + P, H - 8), c, st, pm, fe, fq);
+                    if constexpr (M == M_SSD)
+                        scan_window_ssd2(fp, a.pitch, max(xx - P, 0), min(xx + P, W - 8), max(yy - P, 0),
+                                         min(yy + P, H - 8), nc, pm, fe, fq);
+                    else
+                        scan_window<M>(fp, a.pitch, max(xx - P, 0), min(xx + P, W - 8), max(yy - P, 0),
+                                       min(yy + P, H - 8), c, st, pm, fe, fq);
                 }
             }
 #pragma unroll

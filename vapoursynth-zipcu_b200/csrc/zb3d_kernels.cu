@@ -1023,21 +1023,29 @@ struct FinishArgs {
     int mode;
 };
 
+// One CTA per 32 x 32 output pixels of one plane (and frame slot): the 39 x 39 tile of
+// origin weights that their 8x8 boxes cover is read once into shared memory, summed along
+// rows (8 wide), then each thread slides an 8-row sum down its column for 4 pixels.  The
+// sums are int64, exact in any order.
+constexpr int kFinishRows = 32;
+
 __global__ void __launch_bounds__(256) zb_finish(FinishArgs a) {
-    __shared__ long long t[15][40];
-    __shared__ long long hs[15][32];
+    constexpr int TR = kFinishRows + 7, TC = 32 + 7;
+    __shared__ long long t[TR][TC + 1];
+    __shared__ long long hs[TR][32];
     const int plane = blockIdx.z / a.tw, slot = blockIdx.z - plane * a.tw;
     if (!((a.proc_mask >> plane) & 1)) return;
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * kFinishRows;
     const long long base = plane * a.acc_plane_stride + slot * a.acc_frame_stride;
     const unsigned long long *den = a.den + base;
-    for (int i = threadIdx.y * 32 + threadIdx.x; i < 15 * 39; i += 256) {
-        const int r = i / 39, c = i - r * 39;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int i = tid; i < TR * TC; i += 256) {
+        const int r = i / TC, c = i - r * TC;
         const int gy = y0 - 7 + r, gx = x0 - 7 + c;
         t[r][c] = (gy >= 0 && gy < a.h && gx >= 0 && gx < a.w) ? (long long)den[(long long)gy * a.pitch + gx] : 0;
     }
     __syncthreads();
-    for (int i = threadIdx.y * 32 + threadIdx.x; i < 15 * 32; i += 256) {
+    for (int i = tid; i < TR * 32; i += 256) {
         const int r = i >> 5, c = i & 31;
         long long s = 0;
 #pragma unroll
@@ -1045,20 +1053,28 @@ __global__ void __launch_bounds__(256) zb_finish(FinishArgs a) {
         hs[r][c] = s;
     }
     __syncthreads();
-    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-    if (x >= a.w || y >= a.h) return;
+    const int x = x0 + threadIdx.x;
+    if (x >= a.w) return;
+    constexpr int PER = kFinishRows / 8;  // output rows per thread
+    const int ry = threadIdx.y * PER;     // first tile row of this thread's pixels
     long long ds = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) ds += hs[threadIdx.y + k][threadIdx.x];
-    const long long ns = (long long)a.num[base + (long long)y * a.pitch + x];
-    const float nf = __ll2float_rn(ns) * kFixInv;
-    const float df = __ll2float_rn(ds) * kFixInv;
-    if (a.mode == 0) {
-        a.dst[plane * a.dst_plane_stride + (long long)y * a.dst_pitch + x] = __fdiv_rn(nf, df);
-    } else {
-        float *o = a.dst + plane * a.dst_plane_stride + (long long)slot * 2 * a.h * a.dst_pitch;
-        o[(long long)y * a.dst_pitch + x] = nf;
-        o[(long long)(a.h + y) * a.dst_pitch + x] = df;
+    for (int k = 0; k < 8; ++k) ds += hs[ry + k][threadIdx.x];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int y = y0 + ry + i;
+        if (y >= a.h) return;
+        if (i > 0) ds += hs[ry + i + 7][threadIdx.x] - hs[ry + i - 1][threadIdx.x];
+        const long long ns = (long long)a.num[base + (long long)y * a.pitch + x];
+        const float nf = __ll2float_rn(ns) * kFixInv;
+        const float df = __ll2float_rn(ds) * kFixInv;
+        if (a.mode == 0) {
+            a.dst[plane * a.dst_plane_stride + (long long)y * a.dst_pitch + x] = __fdiv_rn(nf, df);
+        } else {
+            float *o = a.dst + plane * a.dst_plane_stride + (long long)slot * 2 * a.h * a.dst_pitch;
+            o[(long long)y * a.dst_pitch + x] = nf;
+            o[(long long)(a.h + y) * a.dst_pitch + x] = df;
+        }
     }
 }
 
@@ -1332,7 +1348,7 @@ cudaError_t launch_finish(const unsigned long long *num, const unsigned long lon
     a.dst_pitch = dst_pitch;
     a.dst_plane_stride = dst_plane_stride;
     a.mode = mode;
-    dim3 grid((w + 31) / 32, (h + 7) / 8, nplanes * a.tw);
+    dim3 grid((w + 31) / 32, (h + kFinishRows - 1) / kFinishRows, nplanes * a.tw);
     zb_finish<<<grid, dim3(32, 8), 0, st>>>(a);
     return cudaGetLastError();
 }

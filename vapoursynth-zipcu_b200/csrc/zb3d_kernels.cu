@@ -1103,13 +1103,9 @@ __device__ __forceinline__ int batch_entry_of(const BatchArgs &b, long long item
 // items of the other kind are skipped, so two stream-ordered launches cover the list, each
 // kernel with the register budget of its own kind of work).
 // PHASE 1: the match tiles (kBatchMatchRows warps per CTA); PHASE 2: the filter chunks
-// (4 warps per CTA).  Each phase is one persistent launch with its own register budget;
-// the filter phase's occupancy hint (5 CTAs per SM hard, 6 Wiener, as shared memory
-// allows) gives it the registers of the per-window filter kernels (96 / 80), where the
-// compiler's own choice (72 / 64 with a spill) ran its chunks about 1.4x slower.
+// (4 warps per CTA).  Each phase is one persistent launch with its own register budget.
 template <bool FINAL, int T2D, int T1D, int PHASE>
-__global__ void __launch_bounds__(PHASE == 1 ? kBatchMatchRows * 32 : 128, PHASE == 1 ? 2 : (FINAL ? 6 : 5))
-    zb_batch(BatchArgs b) {
+__global__ void __launch_bounds__(PHASE == 1 ? kBatchMatchRows * 32 : 128) zb_batch(BatchArgs b) {
     extern __shared__ __align__(16) float dyn[];  // matching tile, or the Wiener coefficient buffer
     __shared__ float tbuf[PHASE == 1 ? 1 : kFilterWarps * 2 * kGroupBuf];
     __shared__ long long s_item;

@@ -498,10 +498,10 @@ __global__ void __launch_bounds__(256, 2) zb_match_tiled2(MatchArgs a) {
 // (row-major, the reference's order).  `plane` is already offset by this
 // lane's half (4*hh columns).  A 4-column ring holds the sliding window.
 // ---------------------------------------------------------------------------
-template <int M>
+template <int M, int K = 8>
 __device__ __forceinline__ void scan_window(const float *__restrict__ plane, int pitch, int left, int right, int top,
                                             int bottom, const float (&c)[8][4], float st, unsigned pm,
-                                            float (&e)[8], int (&q)[8]) {
+                                            float (&e)[K], int (&q)[K]) {
     for (int row = top; row <= bottom; ++row) {
         const float *rp = plane + (long long)row * pitch;
         float w[8][4];
@@ -521,7 +521,7 @@ __device__ __forceinline__ void scan_window(const float *__restrict__ plane, int
                     for (int j = 0; j < 4; ++j) n[i][j] = w[i][(s + j) & 3];
                 const float hd = half_distance<M>(c, n, st, pm);
                 const float err = join_pair<M>(hd, pm);
-                if (err < e[7]) top8_insert(e, q, err, pack_pos(cc, row));
+                if (err < e[K - 1]) topk_insert<K>(e, q, err, pack_pos(cc, row));
                 if (cc + 1 <= right) {
 #pragma unroll
                     for (int i = 0; i < 8; ++i) w[i][s] = __ldg(rp + i * pitch + cc + 4);
@@ -536,9 +536,10 @@ __device__ __forceinline__ void scan_window(const float *__restrict__ plane, int
 // one __ffma2_rn advances the even-row and the odd-row chain of a column together (each
 // with its own rounding), so every distance is half_distance<M_SSD>'s; n + (-c) is
 // exactly -(c - n), so the squares are the same.
+template <int K = 8>
 __device__ __forceinline__ void scan_window_ssd2(const float *__restrict__ plane, int pitch, int left, int right,
                                                  int top, int bottom, const float2 (&nc)[4][4], unsigned pm,
-                                                 float (&e)[8], int (&q)[8]) {
+                                                 float (&e)[K], int (&q)[K]) {
     for (int row = top; row <= bottom; ++row) {
         const float *rp = plane + (long long)row * pitch;
         float2 w[4][4];
@@ -566,7 +567,7 @@ __device__ __forceinline__ void scan_window_ssd2(const float *__restrict__ plane
                 }
                 const float hd = (sj[0] + sj[1]) + (sj[2] + sj[3]);
                 const float err = hd + __shfl_xor_sync(pm, hd, 1);
-                if (err < e[7]) top8_insert(e, q, err, pack_pos(cc, row));
+                if (err < e[K - 1]) topk_insert<K>(e, q, err, pack_pos(cc, row));
                 if (cc + 1 <= right) {
 #pragma unroll
                     for (int k = 0; k < 4; ++k)
@@ -664,9 +665,11 @@ __global__ void __launch_bounds__(128) zb_match_global(MatchArgs a) {
 // (:758-788).  Starts from the spatial list; for direction -1 then +1 and
 // t = 1..r a per-frame list is built from ps_range windows around the first
 // ps_num entries of the previous list (t = 1: the spatial list), and its first
-// ps_num entries are merged into the block's list.
+// ps_num entries are merged into the block's list.  Only those first ps_num entries of a
+// per-frame list are ever read, so the per-frame list holds K >= ps_num entries: the
+// first K of the reference's 8-entry list (K = 2 covers the default ps_num).
 // ---------------------------------------------------------------------------
-template <int M>
+template <int M, int K>
 __global__ void __launch_bounds__(128, M == M_SSD ? 4 : 3) zb_match_temporal(MatchArgs a) {
     const int lane = threadIdx.x & 31;
     const long long pair = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 1;
@@ -710,30 +713,30 @@ __global__ void __launch_bounds__(128, M == M_SSD ? 4 : 3) zb_match_temporal(Mat
         for (int t = 1; t <= r; ++t) {
             const int zt = r + dir * t;
             const float *fp = a.frames + (long long)zt * a.fstride + 4 * hh;
-            float fe[8];
-            int fq[8];
+            float fe[K];
+            int fq[K];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
+            for (int i = 0; i < K; ++i) {
                 fe[i] = ZB_FLT_MAX;
                 fq[i] = 0;
             }
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
+            for (int i = 0; i < K; ++i) {
                 if (i < a.ps_num) {
                     const int xx = pos_x(lq[i]), yy = pos_y(lq[i]);
                     if constexpr (M == M_SSD)
-                        scan_window_ssd2(fp, a.pitch, max(xx - P, 0), min(xx + P, W - 8), max(yy - P, 0),
-                                         min(yy + P, H - 8), nc, pm, fe, fq);
+                        scan_window_ssd2<K>(fp, a.pitch, max(xx - P, 0), min(xx + P, W - 8), max(yy - P, 0),
+                                            min(yy + P, H - 8), nc, pm, fe, fq);
                     else
-                        scan_window<M>(fp, a.pitch, max(xx - P, 0), min(xx + P, W - 8), max(yy - P, 0),
-                                       min(yy + P, H - 8), c, st, pm, fe, fq);
+                        scan_window<M, K>(fp, a.pitch, max(xx - P, 0), min(xx + P, W - 8), max(yy - P, 0),
+                                          min(yy + P, H - 8), c, st, pm, fe, fq);
                 }
             }
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
+            for (int i = 0; i < K; ++i)
                 if (i < a.ps_num && fe[i] < ge[7]) top8_insert_z(ge, gq, gz, fe[i], fq[i], zt);
 #pragma unroll
-            for (int i = 0; i < 8; ++i) lq[i] = fq[i];
+            for (int i = 0; i < K; ++i) lq[i] = fq[i];
         }
     }
     if (hh) return;
@@ -1221,7 +1224,10 @@ static cudaError_t launch_global_m(const MatchArgs &a, cudaStream_t st) {
 template <int M>
 static cudaError_t launch_temporal_m(const MatchArgs &a, cudaStream_t st) {
     const long long threads = (long long)a.nby * a.nbx * 2;
-    zb_match_temporal<M><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a);
+    if (a.ps_num <= 2)
+        zb_match_temporal<M, 2><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a);
+    else
+        zb_match_temporal<M, 8><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a);
     return cudaGetLastError();
 }
 

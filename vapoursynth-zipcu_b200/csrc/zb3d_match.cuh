@@ -27,6 +27,23 @@ __device__ __forceinline__ void top8_insert(float (&e)[8], int (&q)[8], float er
     }
 }
 
+// The same strict-less insertion into a list of K entries.  Its entries are the first K
+// of the 8-entry list that the same candidates would build (stable in scan order).
+template <int K>
+__device__ __forceinline__ void topk_insert(float (&e)[K], int (&q)[K], float err, int pos) {
+#pragma unroll
+    for (int i = K - 1; i > 0; --i) {
+        const bool ci = err < e[i];
+        const bool cp = err < e[i - 1];
+        e[i] = cp ? e[i - 1] : (ci ? err : e[i]);
+        q[i] = cp ? q[i - 1] : (ci ? pos : q[i]);
+    }
+    if (err < e[0]) {
+        e[0] = err;
+        q[0] = pos;
+    }
+}
+
 __device__ __forceinline__ void top8_insert_z(float (&e)[8], int (&q)[8], int (&z)[8], float err, int pos, int zz) {
 #pragma unroll
     for (int i = 7; i > 0; --i) {

@@ -65,6 +65,21 @@ def synth_frames(clip: int, count: int, first: int = 0):
     return out
 
 
+def warm_until(torch, step, warmup: int, min_s: float = 0.3) -> int:
+    """Untimed warm-up: `step` at least `warmup` times, then until `min_s` seconds of
+    synchronised wall time have passed, so that the SM clocks have left their idle level
+    (they take a few hundred ms to rise) before a short timed region starts.  Returns the
+    number of steps run."""
+    t0 = time.perf_counter()
+    n = 0
+    while n < warmup or time.perf_counter() - t0 < min_s:
+        step()
+        n += 1
+        if n >= warmup:
+            torch.cuda.synchronize()
+    return n
+
+
 def match_flops(w, h, bs, rng):
     """Algorithmic FLOPs of one block-matching launch: 192 per candidate (64 sub,
     64 mul, 64 add per 8x8 distance) over every reference block's clipped window."""
@@ -520,7 +535,8 @@ def run_vbm3d(torch, steps: int, warmup: int, filter_form: int = 0):
     from zb3d import _native as N
     from zb3d import synth
     from zb3d.device import DeviceFilter
-    r, nf, sigma = 2, 120, 15.0
+    # 120 frames, or more so that every timed output frame (8 .. 8 * (steps + 1) - 1) is in the clip
+    r, nf, sigma = 2, max(120, BATCH * (steps + 2)), 15.0
     tw = 2 * r + 1
     f = DeviceFilter(W, H, num_frames=nf, sigma=[sigma], radius=r, extractor_exp=EXTRACTOR_EXP, num_streams=1,
                      filter_form=filter_form)
@@ -567,18 +583,17 @@ def run_vbm3d(torch, steps: int, warmup: int, filter_form: int = 0):
             aggregate(n)
 
     with torch.cuda.stream(st):
-        run(0, warmup * BATCH)
-        torch.cuda.synchronize()
+        nw = warm_until(torch, lambda: run(0, BATCH), warmup)
         a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(st)
-        run(warmup * BATCH, steps * BATCH)
+        run(BATCH, steps * BATCH)
         z.record(st)
         z.synchronize()
     ms = a.elapsed_time(z)
     res = {"metric": "VBM3D 1080p Mpix/s (BM3Dv2 radius 2, fused)", "value": W * H * steps * BATCH / ms * 1e3 / 1e6,
-           "unit": "Mpix/s", "ms_per_step": ms / steps, "steps": steps, "warmup": warmup,
+           "unit": "Mpix/s", "ms_per_step": ms / steps, "steps": steps, "warmup": warmup, "warmup_steps_run": nw,
            "config": {"workload": "GRAYS 1920x1080, radius 2, sigma 15, block_step 8, bm_range 9, ps_num 2, "
-                                  "ps_range 4, extractor_exp 3, moving scene, 120 frames, one window + one "
+                                  f"ps_range 4, extractor_exp 3, moving scene, {nf} frames, one window + one "
                                   "temporal aggregation per output frame", "batch_frames_per_step": BATCH,
                       "filter": "precision: 2D transforms on tcgen05, split TF32" if filter_form else
                                 "plain: FP32 transforms, bit for bit the reference's"}}
@@ -742,8 +757,7 @@ def run_gray640(torch, steps: int, warmup: int):
         for i in range(8):
             f.run_entry(0, src[i].data_ptr(), out[i].data_ptr(), st.cuda_stream)
 
-    for _ in range(warmup):
-        step()
+    nw = warm_until(torch, step, warmup)
     a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(st)
     for _ in range(steps):
@@ -752,7 +766,7 @@ def run_gray640(torch, steps: int, warmup: int):
     z.synchronize()
     ms = a.elapsed_time(z)
     f.close()
-    return {"metric": "BM3D 640x480 Mpix/s (sigma 3, block_step 8)", "value": w * h * 8 * steps / ms * 1e3 / 1e6,
+    return {"warmup_steps_run": nw, "metric": "BM3D 640x480 Mpix/s (sigma 3, block_step 8)", "value": w * h * 8 * steps / ms * 1e3 / 1e6,
             "unit": "Mpix/s", "ms_per_step": ms / steps, "steps": steps, "warmup": warmup,
             "config": {"workload": "GRAYS 640x480 x 8 frames, sigma 3, block_step 8, bm_range 9, dct/dct, "
                                    "extractor_exp 3, single pass"}}
@@ -790,8 +804,7 @@ def run_dct_tf32(torch, steps: int, warmup: int):
             rc = lib.zb3d_dct2d_tf32(x.data_ptr(), y.data_ptr(), npat, split, status.data_ptr(), st.cuda_stream)
             if rc:
                 raise RuntimeError(f"zb3d_dct2d_tf32 returned {rc}")
-        for _ in range(warmup):
-            call()
+        warm_until(torch, call, warmup)
         a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(st)
         for _ in range(steps):
@@ -854,9 +867,7 @@ def run_match1080(torch, steps: int, warmup: int):
             if rec is not None:
                 rec.append((e, a, z))
 
-    for _ in range(warmup):
-        step()
-    torch.cuda.synchronize()
+    nw = warm_until(torch, step, warmup)
     rec = []
     g0 = torch.cuda.Event(enable_timing=True)
     g0.record(st)
@@ -880,7 +891,7 @@ def run_match1080(torch, steps: int, warmup: int):
     f.close()
     return {"metric": "block matching of one 1920x1080 YUV420 frame (Y, U, V), luma Mpix/s", "unit": "Mpix/s",
             "value": W * H / (ms / 1e3) / 1e6, "ms_per_step": ms, "steps": steps, "warmup": warmup,
-            "planes": planes,
+            "warmup_steps_run": nw, "planes": planes,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": None,
                          "how": "192 FLOP per candidate over every block's clipped window, 3 launches per step "

@@ -660,6 +660,89 @@ __global__ void __launch_bounds__(128) zb_match_global(MatchArgs a) {
     }
 }
 
+// The clamped last block column (x = W - 8) that the tiled kernels leave out: one warp per
+// block.  Its candidate rows are split into 16 consecutive ranges in order, one per lane
+// pair, each scanned in the reference's order into a list of its own; the lists are then
+// merged in row order, a later range's entries inserted (strict less) after the earlier
+// ranges', which is the list of one scan over all the rows.
+template <int M>
+__global__ void __launch_bounds__(128) zb_match_column(MatchArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int by = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (by >= a.nby) return;  // whole warps
+    const int hh = lane & 1, pr = lane >> 1;
+    const int W = a.w, H = a.h, R = a.range;
+    const int kx = a.nbx - 1;
+    const int x = min(a.bs * kx, W - 8), y = min(a.bs * by, H - 8);
+    const unsigned pm = 3u << (lane & 30);
+    const float *plane = a.frames + (long long)a.radius * a.fstride + 4 * hh;
+
+    float c[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) c[i][j] = __ldg(plane + (long long)(y + i) * a.pitch + x + j);
+    const float st = ref_stat<M>(c, pm);
+    float e[8];
+    int q[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        e[i] = ZB_FLT_MAX;
+        q[i] = 0;
+    }
+    const int top = max(y - R, 0), bottom = min(y + R, H - 8);
+    const int per = (bottom - top + 16) / 16;
+    const int r0 = top + pr * per, r1 = min(r0 + per - 1, bottom);
+    if (r0 <= r1) {
+        if constexpr (M == M_SSD) {
+            float2 nc[4][4];
+            neg_pairs(c, nc);
+            scan_window_ssd2(plane, a.pitch, max(x - R, 0), min(x + R, W - 8), r0, r1, nc, pm, e, q);
+        } else {
+            scan_window<M>(plane, a.pitch, max(x - R, 0), min(x + R, W - 8), r0, r1, c, st, pm, e, q);
+        }
+    }
+#pragma unroll
+    for (int k = 1; k < 16; k <<= 1) {
+        float oe[8];
+        int oq[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            oe[i] = __shfl_down_sync(kFull, e[i], 2 * k);
+            oq[i] = __shfl_down_sync(kFull, q[i], 2 * k);
+        }
+        if ((pr & (2 * k - 1)) == 0) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if (oe[i] < e[7]) top8_insert(e, q, oe[i], oq[i]);
+        }
+    }
+    if (lane != 0) return;
+    const long long bi = (long long)by * a.nbx + kx;
+    const int self = pack_pos(x, y);
+    if (a.self_incl) {
+        bool found = false;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) found |= (q[i] == self);
+        if (!found) {
+#pragma unroll
+            for (int i = 7; i > 0; --i) {
+                e[i] = e[i - 1];
+                q[i] = q[i - 1];
+            }
+            e[0] = 0.0f;
+            q[0] = self;
+        }
+    }
+    const int zr = a.radius << 24;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a.list[bi * 8 + i] = make_int2(pos_x(q[i]), pos_y(q[i]) | zr);
+    if (a.errs) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a.errs[bi * 8 + i] = e[i];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Temporal predictive search (vszipcu src/bm3d.cu:663-756) and self inclusion
 // (:758-788).  Starts from the spatial list; for direction -1 then +1 and
@@ -1222,6 +1305,12 @@ static cudaError_t launch_global_m(const MatchArgs &a, cudaStream_t st) {
 }
 
 template <int M>
+static cudaError_t launch_column_m(const MatchArgs &a, cudaStream_t st) {
+    zb_match_column<M><<<(unsigned)((a.nby + 3) / 4), 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int M>
 static cudaError_t launch_temporal_m(const MatchArgs &a, cudaStream_t st) {
     const long long threads = (long long)a.nby * a.nbx * 2;
     if (a.ps_num <= 2)
@@ -1269,10 +1358,17 @@ cudaError_t launch_match(MatchArgs a, int metric, int rows_per_cta, bool use_til
         }
         if (e != cudaSuccess) return e;
         if (a.nbx_al == a.nbx) goto temporal;
-        a.gen_mode = 1;  // clamped last column
-    } else {
-        a.gen_mode = 0;
+        switch (metric) {  // the clamped last column
+        case M_SSD: e = launch_column_m<M_SSD>(a, st); break;
+        case M_SAD: e = launch_column_m<M_SAD>(a, st); break;
+        case M_ZSSD: e = launch_column_m<M_ZSSD>(a, st); break;
+        case M_ZSAD: e = launch_column_m<M_ZSAD>(a, st); break;
+        default: e = launch_column_m<M_SSD_NORM>(a, st); break;
+        }
+        if (e != cudaSuccess) return e;
+        goto temporal;
     }
+    a.gen_mode = 0;
     switch (metric) {
     case M_SSD: e = launch_global_m<M_SSD>(a, st); break;
     case M_SAD: e = launch_global_m<M_SAD>(a, st); break;
@@ -1358,8 +1454,7 @@ cudaError_t launch_finish(const unsigned long long *num, const unsigned long lon
 // The clamped last block column of an entry (x = w - 8), which the tiled kernels leave out.
 cudaError_t launch_clamped_column(MatchArgs a, cudaStream_t st) {
     a.self_incl = a.radius == 0;
-    a.gen_mode = 1;
-    return launch_global_m<M_SSD>(a, st);
+    return launch_column_m<M_SSD>(a, st);
 }
 
 size_t match_tile2_bytes_rows(const MatchArgs &a, int rows_per_cta) { return match_tile2_bytes(a, rows_per_cta); }

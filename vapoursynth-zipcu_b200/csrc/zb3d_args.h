@@ -21,8 +21,8 @@ struct MatchArgs {
     int2 *list;            // [nby*nbx][8]: (x, y | z << 24)
     float *errs;           // [nby*nbx][8]: distances of the spatial list (radius > 0)
     int self_incl;         // 1: insert the block itself here (radius 0)
-    int gen_mode;          // generic kernel: 0 = every block, 1 = clamped last column only,
-                           // 2 = the blocks listed in tc_ws (fallbacks of the tensor-core form)
+    int gen_mode;          // generic kernel: 0 = every block, 2 = the blocks listed in tc_ws
+                           // (fallbacks of the tensor-core form)
     // Tensor-core form (zb3d_match_tc.cu).  tc_ws: [0] number of listed fallback
     // blocks, [kTcWsList..] their block indices.  tc_stats (optional, accumulated):
     // [0] tiles, [1] blocks, [2] re-ranked candidates, [3] fallback blocks.

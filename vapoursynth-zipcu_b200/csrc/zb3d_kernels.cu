@@ -586,23 +586,20 @@ __device__ __forceinline__ void neg_pairs(const float (&c)[8][4], float2 (&nc)[4
         for (int j = 0; j < 4; ++j) nc[k][j] = make_float2(-c[2 * k][j], -c[2 * k + 1][j]);
 }
 
-// Spatial matching for any block_step (and for the clamped last block column of
-// the tiled kernel), reading candidates through the L1/L2 path.  Lane pair per block.
+// Spatial matching for block steps the tiled kernels do not take (and the blocks the
+// tensor-core form lists), reading candidates through the L1/L2 path.  Lane pair per block.
 template <int M>
 __global__ void __launch_bounds__(128) zb_match_global(MatchArgs a) {
     const int lane = threadIdx.x & 31;
     const long long pair = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 1;
     const int hh = lane & 1;
-    const long long nb = a.gen_mode == 2 ? (long long)a.tc_ws[0] : a.gen_mode ? a.nby : (long long)a.nby * a.nbx;
+    const long long nb = a.gen_mode == 2 ? (long long)a.tc_ws[0] : (long long)a.nby * a.nbx;
     if (pair >= nb) return;
     int kx, by;
     if (a.gen_mode == 2) {
         const int bi = a.tc_ws[kTcWsList + pair];
         by = bi / a.nbx;
         kx = bi - by * a.nbx;
-    } else if (a.gen_mode) {
-        kx = a.nbx - 1;
-        by = (int)pair;
     } else {
         by = (int)(pair / a.nbx);
         kx = (int)(pair - (long long)by * a.nbx);
@@ -1298,8 +1295,7 @@ static cudaError_t launch_tiled_m(const MatchArgs &a, int rows_per_cta, cudaStre
 template <int M>
 static cudaError_t launch_global_m(const MatchArgs &a, cudaStream_t st) {
     // listed blocks (gen_mode 2): the count is on the device, so size for every block
-    const long long nb = a.gen_mode == 1 ? a.nby : (long long)a.nby * a.nbx;
-    const long long threads = nb * 2;
+    const long long threads = (long long)a.nby * a.nbx * 2;
     zb_match_global<M><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a);
     return cudaGetLastError();
 }

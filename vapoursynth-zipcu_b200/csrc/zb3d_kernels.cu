@@ -1122,6 +1122,15 @@ __global__ void __launch_bounds__(256) zb_finish(FinishArgs a) {
     const long long base = plane * a.acc_plane_stride + slot * a.acc_frame_stride;
     const unsigned long long *den = a.den + base;
     const int tid = threadIdx.y * 32 + threadIdx.x;
+    constexpr int PER = kFinishRows / 8;  // output rows per thread
+    const int x = x0 + threadIdx.x;
+    const int ry = threadIdx.y * PER;     // first tile row of this thread's pixels
+    long long ns[PER];                    // this thread's numerators, loaded before the tile
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int y = y0 + ry + i;
+        ns[i] = (x < a.w && y < a.h) ? (long long)a.num[base + (long long)y * a.pitch + x] : 0;
+    }
     for (int i = tid; i < TR * TC; i += 256) {
         const int r = i / TC, c = i - r * TC;
         const int gy = y0 - 7 + r, gx = x0 - 7 + c;
@@ -1136,10 +1145,7 @@ __global__ void __launch_bounds__(256) zb_finish(FinishArgs a) {
         hs[r][c] = s;
     }
     __syncthreads();
-    const int x = x0 + threadIdx.x;
     if (x >= a.w) return;
-    constexpr int PER = kFinishRows / 8;  // output rows per thread
-    const int ry = threadIdx.y * PER;     // first tile row of this thread's pixels
     long long ds = 0;
 #pragma unroll
     for (int k = 0; k < 8; ++k) ds += hs[ry + k][threadIdx.x];
@@ -1148,8 +1154,7 @@ __global__ void __launch_bounds__(256) zb_finish(FinishArgs a) {
         const int y = y0 + ry + i;
         if (y >= a.h) return;
         if (i > 0) ds += hs[ry + i + 7][threadIdx.x] - hs[ry + i - 1][threadIdx.x];
-        const long long ns = (long long)a.num[base + (long long)y * a.pitch + x];
-        const float nf = __ll2float_rn(ns) * kFixInv;
+        const float nf = __ll2float_rn(ns[i]) * kFixInv;
         const float df = __ll2float_rn(ds) * kFixInv;
         if (a.mode == 0) {
             a.dst[plane * a.dst_plane_stride + (long long)y * a.dst_pitch + x] = __fdiv_rn(nf, df);

@@ -342,7 +342,7 @@ __device__ __forceinline__ float2 f4hi(const float4 &v) { return make_float2(v.z
 // the pitch and half-plane size).  The columns are loaded one column pair at a time, just
 // before the sums that use them: column col feeds the (s, j = col - s) chains, each
 // of which runs over its pair rows k = 0..3 in order, so every sum is the reference's.
-// Keeping no window in registers holds the kernel at 116 registers.  The four distances
+// Keeping no window in registers holds the kernel at 112-116 registers.  The four distances
 // come first (no branch between their FMA chains), then the insertions in scan order;
 // a displacement past R is computed from the tile's padding columns and discarded.
 template <bool SHARED, int GF>
@@ -747,7 +747,9 @@ __global__ void __launch_bounds__(128) zb_match_column(MatchArgs a) {
 // ps_num entries of the previous list (t = 1: the spatial list), and its first
 // ps_num entries are merged into the block's list.  Only those first ps_num entries of a
 // per-frame list are ever read, so the per-frame list holds K >= ps_num entries: the
-// first K of the reference's 8-entry list (K = 2 covers the default ps_num).
+// first K of the reference's 8-entry list (K = 2 covers the default ps_num).  For SSD the
+// kernel is held at 128 registers, 4 CTAs per SM, so that a 1080p plane at block_step 8
+// (507 CTAs) runs in one wave; the other metrics keep their 3 CTAs per SM.
 // ---------------------------------------------------------------------------
 template <int M, int K>
 __global__ void __launch_bounds__(128, M == M_SSD ? 4 : 3) zb_match_temporal(MatchArgs a) {

@@ -990,10 +990,11 @@ __device__ __forceinline__ void filter16_groups(const FilterArgs &a, long long g
         float k = 0.0f;
         if constexpr (FINAL) {
             // Wiener coefficients r^2 / (r^2 + sigma^2) of the basic estimate's spectrum (the
-            // reference rounds r^2 once and adds sigma^2 without FMA), then the weight's sum of
-            // squared coefficients, accumulated by FMA over spectrum and row for column j in
-            // the reference's order: every lane runs the full chain of its column.  The basic
-            // estimate and the noisy patches share one copy of the forward transform's code.
+            // reference rounds r^2 once and adds sigma^2 without FMA); the weight's sum of
+            // squared coefficients (after the shrinkage below) is accumulated by FMA over
+            // spectrum and row for column j in the reference's order: every lane runs the full
+            // chain of its column.  The basic estimate and the noisy patches share one copy of
+            // the forward transform's code.
             const float s2 = sigma * sigma;
 #pragma unroll 1
             for (int pass = 0; pass < 2; ++pass) {
@@ -1011,16 +1012,6 @@ __device__ __forceinline__ void filter16_groups(const FilterArgs &a, long long g
                         cb[p * 72 + (2 * t + h) * 8 + j] = coeff;
                     }
                 __syncwarp(gm);
-#pragma unroll 8
-                for (int p = 0; p < 8; ++p)
-#pragma unroll
-                    for (int r = 0; r < 8; ++r) {
-                        const float c = cb[p * 72 + r * 8 + j];
-                        k = __fmaf_rn(c, c, k);
-                    }
-                k += __shfl_xor_sync(gm, k, 1, 8);
-                k += __shfl_xor_sync(gm, k, 2, 8);
-                k += __shfl_xor_sync(gm, k, 4, 8);
             }
         } else {
             gather16(d, a.src + pl * a.plane_stride, a, grp, h, j);
@@ -1054,6 +1045,18 @@ __device__ __forceinline__ void filter16_groups(const FilterArgs &a, long long g
                     val *= cb[(2 * q + h) * 72 + i * 8 + j];
                     d[q * 8 + i] = val * (1.0f / 4096.0f);
                 }
+            // the weight's chain, here so that it can overlap the vertical inverse transforms
+            // (it only reads the coefficient buffer)
+#pragma unroll 8
+            for (int p = 0; p < 8; ++p)
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    const float c = cb[p * 72 + r * 8 + j];
+                    k = __fmaf_rn(c, c, k);
+                }
+            k += __shfl_xor_sync(gm, k, 1, 8);
+            k += __shfl_xor_sync(gm, k, 2, 8);
+            k += __shfl_xor_sync(gm, k, 4, 8);
         }
         const float w = 1.0f / k;
         inverse3_16<T2, T1>(d, gb, h, j, gm);
